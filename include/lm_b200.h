@@ -1,0 +1,157 @@
+/*
+ * lm_b200.h — C ABI of the B200 (sm_100a) dense-solve library.
+ *
+ * This is the drop-in boundary for linear-massiv's dense solve path.  Every
+ * entry point is `extern "C"`, takes plain pointers and sizes, and returns an
+ * int status:
+ *     0            success
+ *     > 0          LAPACK-style info: k + 1 where k is the first zero pivot
+ *                  (LU) or first non-positive diagonal (Cholesky).  The
+ *                  outputs are still written, with the Inf/NaN the reference's
+ *                  own arithmetic produces in that case.
+ *     < 0          LM_ERR_* below (argument, CUDA or device-wait error).
+ * Errors never cross the ABI as exceptions.
+ *
+ * Layout convention (the reference's massiv `Array P Ix2 Double`): row-major,
+ * element (i, j) at ptr[i * ld + j], ld >= number of columns.
+ *
+ * Device-pointer entry points (lm_d*) leave matrices resident in HBM and run
+ * asynchronously on the context's stream unless an `info` host pointer is
+ * passed (then they synchronise to report it).  Host-buffer entry points
+ * (lm_*_host) are what a pure binding of the reference's functions calls:
+ * they copy in, compute, copy out and synchronise.
+ *
+ * References in comments are to linear-massiv source files:
+ *   L3.hs  src/Numeric/LinearAlgebra/Massiv/BLAS/Level3.hs
+ *   L2.hs  src/Numeric/LinearAlgebra/Massiv/BLAS/Level2.hs
+ *   LU.hs  src/Numeric/LinearAlgebra/Massiv/Solve/LU.hs
+ *   Chol.hs src/Numeric/LinearAlgebra/Massiv/Solve/Cholesky.hs
+ *   K.hs   src/Numeric/LinearAlgebra/Massiv/Internal/Kernel.hs
+ */
+#ifndef LM_B200_H
+#define LM_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LM_OK 0
+#define LM_ERR_ARG (-1)           /* invalid argument (size, stride, null)      */
+#define LM_ERR_CUDA (-2)          /* CUDA runtime/driver error                  */
+#define LM_ERR_UNSUPPORTED (-3)   /* configuration not supported                */
+#define LM_ERR_TIMEOUT (-4)       /* a bounded device-side wait gave up         */
+#define LM_ERR_NOMEM (-5)         /* device or pinned allocation failed         */
+#define LM_ERR_NOT_CONVERGED (-6) /* iterative refinement did not converge      */
+
+typedef struct lm_ctx lm_ctx;
+
+/* ---- context ------------------------------------------------------------
+ * One context per device and calling thread (Haskell capability).  A context
+ * owns a CUDA stream, a grow-only device workspace and a pinned staging
+ * buffer.  Calls on one context are serialised by an internal lock. */
+int lm_ctx_create(lm_ctx** ctx, int device);
+int lm_ctx_destroy(lm_ctx* ctx);
+/* Use an external cudaStream_t (passed as void*) instead of the own stream. */
+int lm_ctx_set_stream(lm_ctx* ctx, void* stream);
+void* lm_ctx_get_stream(lm_ctx* ctx);
+int lm_ctx_synchronize(lm_ctx* ctx);
+/* Device status of the last call on this context (checks the device error
+ * flag, e.g. a bounded wait that timed out); synchronises. */
+int lm_ctx_check(lm_ctx* ctx);
+const char* lm_status_string(int status);
+/* Thread-local text of the last error raised by this library. */
+const char* lm_last_error(void);
+/* Number of kernel launches this library has issued in this process. */
+long long lm_launch_count(void);
+
+/* ---- memory (device buffers stay resident between calls) -------------- */
+int lm_dmalloc(lm_ctx* ctx, void** ptr, size_t bytes);
+int lm_dfree(lm_ctx* ctx, void* ptr);
+int lm_h2d(lm_ctx* ctx, void* dst_device, const void* src_host, size_t bytes);
+int lm_d2h(lm_ctx* ctx, void* dst_host, const void* src_device, size_t bytes);
+
+/* ---- BLAS-3 ---------------------------------------------------------------
+ * gemm alpha A B beta C (L3.hs:102-131); with alpha = 1, beta = 0 this is
+ * matMul / matMulP (L3.hs:144-147, 183-207) and matMulPPar (L3.hs:214-294),
+ * whose work rawGemmKernel (K.hs:145-806) does on the CPU.
+ * C (m x n) = alpha * A (m x k) * B (k x n) + beta * C, device pointers. */
+int lm_dgemm(lm_ctx* ctx, int m, int n, int k, double alpha, const double* A, int lda,
+             const double* B, int ldb, double beta, double* C, int ldc);
+
+/* ---- LU with partial pivoting ---------------------------------------------
+ * lm_dgetrf: in-place PA = LU of the n x n matrix A (device).  Replaces the
+ * factor phase of luSolveP, panelLUFactor (LU.hs:265-357) with its kernels
+ * rawPivotSearch / rawSwapRows / rawLUEliminateColumnTo (K.hs:1414-1556),
+ * rawTriSolvePanelTrail (LU.hs:364-407) and the trailing GEMM; also the
+ * factor of `lu` (LU.hs:121-167).  Pivot rule: largest |a_ik|, first
+ * (lowest) row on ties (K.hs:1541-1556).  Rows are swapped across all n
+ * columns, as the reference does.
+ * ipiv (device, n ints): swap list, 0-based — step k swapped rows k and
+ * ipiv[k] (the reference's [(k, pivRow)] list, LU.hs:283,326).
+ * info (host, may be NULL): if given, the call synchronises and stores the
+ * LAPACK-style info there; the return value carries the same. */
+int lm_dgetrf(lm_ctx* ctx, int n, double* A, int lda, int* ipiv, int* info);
+
+/* lm_dgetrs: solve A X = B with the output of lm_dgetrf, B (n x nrhs, ldb)
+ * overwritten by X.  Replaces applyPivotsForward, rawForwardSubUnitPackedSIMD
+ * and rawBackSubPackedSIMD (LU.hs:493-507, K.hs:2205-2314); nrhs > 1 solves
+ * each column as luSolveP would. */
+int lm_dgetrs(lm_ctx* ctx, int n, int nrhs, const double* LU, int lda, const int* ipiv, double* B,
+              int ldb);
+
+/* lm_dgesv: luSolveP (LU.hs:265-304) on device buffers: A is overwritten by
+ * its LU factors, B by the solution. */
+int lm_dgesv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, double* B, int ldb,
+             int* info);
+
+/* ---- Cholesky ---------------------------------------------------------------
+ * lm_dpotrf: A = G G^T from the lower triangle of A (device), G written to
+ * the lower triangle and the strict upper triangle zeroed, as `cholesky`
+ * returns it (Chol.hs:114-147).  Replaces panelCholFactor with
+ * rawCholColumnSIMD(From) (Chol.hs:279-321, K.hs:2071-2195). */
+int lm_dpotrf(lm_ctx* ctx, int n, double* A, int lda, int* info);
+
+/* lm_dpotrs: solve with G from lm_dpotrf; B (n x nrhs) overwritten by X.
+ * Replaces rawForwardSubCholPackedSIMD and rawBackSubCholTPackedSIMD
+ * (K.hs:2319-2430). */
+int lm_dpotrs(lm_ctx* ctx, int n, int nrhs, const double* G, int lda, double* B, int ldb);
+
+/* lm_dposv: choleskySolveP (Chol.hs:241-273) on device buffers. */
+int lm_dposv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, double* B, int ldb, int* info);
+
+/* ---- host-buffer entry points (pure functions of the reference) ------------
+ * Inputs are read-only host arrays (row-major, dense: lda = n, ldb = nrhs);
+ * outputs are written to host arrays.  These are the calls a Haskell
+ * `foreign import ccall safe` binding of luSolve / choleskySolve / matMul /
+ * lu / cholesky makes. */
+int lm_lu_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X,
+                     int* info);
+int lm_chol_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X,
+                       int* info);
+int lm_matmul_host(lm_ctx* ctx, int m, int n, int k, const double* A, const double* B, double* C);
+int lm_gemm_host(lm_ctx* ctx, int m, int n, int k, double alpha, const double* A, const double* B,
+                 double beta, const double* C0, double* C);
+/* lu (LU.hs:121-122): packed LU (n x n) and the permutation vector form of
+ * the pivots, perm[i] = original row of A that ends up at row i. */
+int lm_lu_host(lm_ctx* ctx, int n, const double* A, double* LU, int* perm, int* info);
+/* cholesky (Chol.hs:114-115): G with zeros above the diagonal. */
+int lm_cholesky_host(lm_ctx* ctx, int n, const double* A, double* G, int* info);
+/* det (LU.hs:534-545): product of U's diagonal times the pivot sign. */
+int lm_det_host(lm_ctx* ctx, int n, const double* A, double* det);
+
+/* Host helper: swap list -> permutation vector (the reference's `lu` form). */
+int lm_ipiv_to_perm(int n, const int* ipiv, int* perm);
+
+/* ---- residual (IR and the reference's scaled residual) ---------------------
+ * R = B - A X in FP64 (device), n x nrhs; replaces matvec / rawGemv
+ * (L2.hs:123-144, K.hs:119-134) on the refinement path. */
+int lm_dresidual(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* X, int ldx,
+                 const double* B, int ldb, double* R, int ldr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LM_B200_H */

@@ -1,0 +1,604 @@
+// Context, memory and the extern "C" entry points of lm_b200.h.
+#include <algorithm>
+#include <atomic>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cudaTypedefs.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+struct lm_ctx;
+
+namespace lm {
+
+struct Ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int* d_status = nullptr;  // int[4], see common.cuh
+  void* ws[kWsSlots] = {};
+  size_t ws_bytes[kWsSlots] = {};
+  std::mutex mu;
+};
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+int load_encode() {
+  std::call_once(g_encode_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!g_encode) {
+    set_last_error("cuTensorMapEncodeTiled is not available from the driver");
+    return LM_ERR_CUDA;
+  }
+  return LM_OK;
+}
+}  // namespace
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+int* ctx_status(Ctx& c) { return c.d_status; }
+int ctx_num_sms(Ctx& c) { return c.num_sms; }
+int ctx_device(Ctx& c) { return c.device; }
+
+int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr) {
+  if (slot < 0 || slot >= kWsSlots) return LM_ERR_ARG;
+  if (c.ws_bytes[slot] < bytes) {
+    if (c.ws[slot]) {
+      // the old buffer may still be in use by queued work on this stream
+      LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+      LM_CUDA_TRY(cudaFree(c.ws[slot]));
+      c.ws[slot] = nullptr;
+      c.ws_bytes[slot] = 0;
+    }
+    size_t want = std::max(bytes, (size_t)1 << 20);
+    if (cudaMalloc(&c.ws[slot], want) != cudaSuccess) {
+      cudaGetLastError();
+      set_last_error("workspace allocation failed");
+      return LM_ERR_NOMEM;
+    }
+    c.ws_bytes[slot] = want;
+  }
+  *ptr = c.ws[slot];
+  return LM_OK;
+}
+
+int make_tmap_2d(CUtensorMap* tm, CUtensorMapDataType dt, int elem_bytes, const void* base,
+                 long long inner, long long outer, long long ld, int box_inner, int box_outer,
+                 CUtensorMapSwizzle swz) {
+  LM_TRY(load_encode());
+  if (inner <= 0 || outer <= 0) return LM_ERR_ARG;
+  cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  cuuint64_t strides[1] = {(cuuint64_t)(ld * elem_bytes)};
+  cuuint32_t box[2] = {(cuuint32_t)box_inner, (cuuint32_t)box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(tm, dt, 2, const_cast<void*>(base), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_last_error("cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
+    return LM_ERR_CUDA;
+  }
+  return LM_OK;
+}
+
+// Reset the device info word before a factorisation.
+int reset_info(Ctx& c) {
+  LM_CUDA_TRY(cudaMemsetAsync(c.d_status + 1, 0, sizeof(int), c.stream));
+  return LM_OK;
+}
+
+// Read back {error, info}; returns the status the ABI reports.
+int read_status(Ctx& c, int* info_out) {
+  int h[2] = {0, 0};
+  LM_CUDA_TRY(cudaMemcpyAsync(h, c.d_status, 2 * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+  if (h[0] != LM_DEVERR_NONE) {
+    set_last_error(h[0] == LM_DEVERR_TIMEOUT ? "a bounded device-side wait timed out"
+                                              : "a device-side self-check failed");
+    int z = 0;
+    cudaMemcpy(c.d_status, &z, sizeof(int), cudaMemcpyHostToDevice);
+    return LM_ERR_TIMEOUT;
+  }
+  if (info_out) *info_out = h[1];
+  return h[1];
+}
+
+}  // namespace lm
+
+struct lm_ctx {
+  lm::Ctx c;
+};
+
+using lm::Ctx;
+
+namespace {
+
+template <typename F>
+int guarded(lm_ctx* ctx, F&& f) {
+  if (!ctx) return LM_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->c.mu);
+  if (cudaSetDevice(ctx->c.device) != cudaSuccess) {
+    lm::set_last_error("cudaSetDevice failed");
+    return LM_ERR_CUDA;
+  }
+  return f(ctx->c);
+}
+
+inline long long rup(long long a, long long b) { return (a + b - 1) / b * b; }
+
+}  // namespace
+
+extern "C" {
+
+int lm_ctx_create(lm_ctx** out, int device) {
+  if (!out) return LM_ERR_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  LM_CUDA_TRY(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev || device >= lm::kMaxDevices) return LM_ERR_ARG;
+  LM_CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  LM_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10) {
+    lm::set_last_error("this library is built for sm_100a (B200); device is sm_" +
+                       std::to_string(prop.major) + std::to_string(prop.minor));
+    return LM_ERR_UNSUPPORTED;
+  }
+  auto* ctx = new lm_ctx();
+  ctx->c.device = device;
+  ctx->c.num_sms = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaMalloc(&ctx->c.d_status, 4 * sizeof(int)) != cudaSuccess) {
+    lm::set_last_error("context allocation failed");
+    delete ctx;
+    return LM_ERR_CUDA;
+  }
+  ctx->c.own_stream = true;
+  cudaMemset(ctx->c.d_status, 0, 4 * sizeof(int));
+  *out = ctx;
+  return LM_OK;
+}
+
+int lm_ctx_destroy(lm_ctx* ctx) {
+  if (!ctx) return LM_OK;
+  {
+    std::lock_guard<std::mutex> lock(ctx->c.mu);
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    for (int s = 0; s < lm::kWsSlots; ++s)
+      if (ctx->c.ws[s]) cudaFree(ctx->c.ws[s]);
+    if (ctx->c.d_status) cudaFree(ctx->c.d_status);
+    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+  }
+  delete ctx;
+  return LM_OK;
+}
+
+int lm_ctx_set_stream(lm_ctx* ctx, void* stream) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (c.own_stream) {
+      cudaStreamSynchronize(c.stream);
+      cudaStreamDestroy(c.stream);
+      c.own_stream = false;
+    }
+    c.stream = static_cast<cudaStream_t>(stream);
+    return LM_OK;
+  });
+}
+
+void* lm_ctx_get_stream(lm_ctx* ctx) { return ctx ? (void*)ctx->c.stream : nullptr; }
+
+int lm_ctx_synchronize(lm_ctx* ctx) {
+  return guarded(ctx, [&](Ctx& c) {
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return LM_OK;
+  });
+}
+
+int lm_ctx_check(lm_ctx* ctx) {
+  return guarded(ctx, [&](Ctx& c) {
+    int r = lm::read_status(c, nullptr);
+    return r < 0 ? r : LM_OK;
+  });
+}
+
+const char* lm_status_string(int s) {
+  switch (s) {
+    case LM_OK: return "ok";
+    case LM_ERR_ARG: return "invalid argument";
+    case LM_ERR_CUDA: return "CUDA error";
+    case LM_ERR_UNSUPPORTED: return "unsupported configuration";
+    case LM_ERR_TIMEOUT: return "device-side wait timed out";
+    case LM_ERR_NOMEM: return "out of memory";
+    case LM_ERR_NOT_CONVERGED: return "iterative refinement did not converge";
+    default: return s > 0 ? "numerical breakdown (info > 0)" : "unknown error";
+  }
+}
+
+const char* lm_last_error(void) { return lm::g_last_error.c_str(); }
+long long lm_launch_count(void) { return lm::g_launches.load(); }
+
+int lm_dmalloc(lm_ctx* ctx, void** ptr, size_t bytes) {
+  return guarded(ctx, [&](Ctx&) {
+    if (!ptr) return LM_ERR_ARG;
+    if (cudaMalloc(ptr, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return LM_ERR_NOMEM;
+    }
+    return LM_OK;
+  });
+}
+
+int lm_dfree(lm_ctx* ctx, void* ptr) {
+  return guarded(ctx, [&](Ctx& c) {
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    LM_CUDA_TRY(cudaFree(ptr));
+    return LM_OK;
+  });
+}
+
+int lm_h2d(lm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  return guarded(ctx, [&](Ctx& c) {
+    LM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream));
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return LM_OK;
+  });
+}
+
+int lm_d2h(lm_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  return guarded(ctx, [&](Ctx& c) {
+    LM_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c.stream));
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return LM_OK;
+  });
+}
+
+int lm_dgemm(lm_ctx* ctx, int m, int n, int k, double alpha, const double* A, int lda,
+             const double* B, int ldb, double beta, double* C, int ldc) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (m < 0 || n < 0 || k < 0 || (m > 0 && n > 0 && !C)) return LM_ERR_ARG;
+    if ((k > 0 && m > 0 && (!A || lda < k)) || (k > 0 && n > 0 && (!B || ldb < n)) ||
+        (m > 0 && n > 0 && ldc < n))
+      return LM_ERR_ARG;
+    lm::GemmDesc d;
+    d.m = m; d.n = n; d.k = k;
+    d.alpha = alpha; d.beta = beta;
+    d.A = A; d.lda = lda; d.B = B; d.ldb = ldb; d.C = C; d.ldc = ldc;
+    const bool aligned = !((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15) &&
+                         !(lda & 1) && !(ldb & 1);
+    if (aligned || k == 0 || alpha == 0.0) return lm::dgemm(c, d, c.stream);
+    // TMA needs 16-byte aligned rows: stage A and B with even strides.
+    const long long lda2 = rup(k, 2), ldb2 = rup(n, 2);
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 0, sizeof(double) * ((size_t)m * lda2 + (size_t)k * ldb2), &ws));
+    double* A2 = static_cast<double*>(ws);
+    double* B2 = A2 + (size_t)m * lda2;
+    LM_TRY(lm::copy2d<double>(A2, lda2, A, lda, m, k, c.stream));
+    LM_TRY(lm::copy2d<double>(B2, ldb2, B, ldb, k, n, c.stream));
+    d.A = A2; d.lda = lda2; d.B = B2; d.ldb = ldb2;
+    return lm::dgemm(c, d, c.stream);
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Run `fn(A2, lda2)` on an even-stride copy of A when lda is odd or A is
+// misaligned (TMA rows must start on 16 bytes), copying the result back.
+template <typename F>
+int with_aligned(Ctx& c, int n, double* A, long long lda, F&& fn) {
+  if (!((reinterpret_cast<uintptr_t>(A) & 15) || (lda & 1))) return fn(A, lda);
+  const long long lda2 = rup(n, 8);
+  void* ws = nullptr;
+  LM_TRY(lm::ctx_workspace(c, 0, sizeof(double) * (size_t)n * lda2, &ws));
+  double* A2 = static_cast<double*>(ws);
+  LM_TRY(lm::copy2d<double>(A2, lda2, A, lda, n, n, c.stream));
+  int r = fn(A2, lda2);
+  if (r < 0) return r;
+  LM_TRY(lm::copy2d<double>(A, lda, A2, lda2, n, n, c.stream));
+  return r;
+}
+
+int finish_info(Ctx& c, int* info) {
+  if (!info) return LM_OK;
+  int r = lm::read_status(c, info);
+  return r;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lm_dgetrf(lm_ctx* ctx, int n, double* A, int lda, int* ipiv, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!A || !ipiv || lda < n))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(with_aligned(c, n, A, lda, [&](double* A2, long long l2) { return lm::dgetrf(c, n, A2, l2, ipiv, c.stream); }));
+    return finish_info(c, info);
+  });
+}
+
+int lm_dgetrs(lm_ctx* ctx, int n, int nrhs, const double* LU, int lda, const int* ipiv, double* B,
+              int ldb) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || (n > 0 && nrhs > 0 && (!LU || !ipiv || !B || lda < n || ldb < nrhs)))
+      return LM_ERR_ARG;
+    if (n == 0 || nrhs == 0) return LM_OK;
+    return lm::dgetrs(c, n, nrhs, LU, lda, ipiv, B, ldb, c.stream);
+  });
+}
+
+int lm_dgesv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, double* B, int ldb,
+             int* info) {
+  int r = lm_dgetrf(ctx, n, A, lda, ipiv, nullptr);
+  if (r < 0) return r;
+  r = lm_dgetrs(ctx, n, nrhs, A, lda, ipiv, B, ldb);
+  if (r < 0) return r;
+  return guarded(ctx, [&](Ctx& c) { return finish_info(c, info); });
+}
+
+int lm_dpotrf(lm_ctx* ctx, int n, double* A, int lda, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!A || lda < n))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(with_aligned(c, n, A, lda, [&](double* A2, long long l2) { return lm::dpotrf(c, n, A2, l2, c.stream); }));
+    return finish_info(c, info);
+  });
+}
+
+int lm_dpotrs(lm_ctx* ctx, int n, int nrhs, const double* G, int lda, double* B, int ldb) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || (n > 0 && nrhs > 0 && (!G || !B || lda < n || ldb < nrhs)))
+      return LM_ERR_ARG;
+    if (n == 0 || nrhs == 0) return LM_OK;
+    return lm::dpotrs(c, n, nrhs, G, lda, B, ldb, c.stream);
+  });
+}
+
+int lm_dposv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, double* B, int ldb, int* info) {
+  int r = lm_dpotrf(ctx, n, A, lda, nullptr);
+  if (r < 0) return r;
+  r = lm_dpotrs(ctx, n, nrhs, A, lda, B, ldb);
+  if (r < 0) return r;
+  return guarded(ctx, [&](Ctx& c) { return finish_info(c, info); });
+}
+
+int lm_dresidual(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* X, int ldx,
+                 const double* B, int ldb, double* R, int ldr) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0) return LM_ERR_ARG;
+    if (n == 0 || nrhs == 0) return LM_OK;
+    if (!A || !X || !B || !R || lda < n || ldx < nrhs || ldb < nrhs || ldr < nrhs) return LM_ERR_ARG;
+    return lm::dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, c.stream);
+  });
+}
+
+int lm_ipiv_to_perm(int n, const int* ipiv, int* perm) {
+  if (n < 0 || (n > 0 && (!ipiv || !perm))) return LM_ERR_ARG;
+  for (int i = 0; i < n; ++i) perm[i] = i;
+  for (int k = 0; k < n; ++k) {
+    const int p = ipiv[k];
+    if (p < 0 || p >= n) return LM_ERR_ARG;
+    std::swap(perm[k], perm[p]);
+  }
+  return LM_OK;
+}
+
+// ---- host-buffer entry points ----------------------------------------------
+}  // extern "C"
+
+namespace {
+
+struct HostBufs {
+  double* A = nullptr;
+  double* B = nullptr;
+  int* ipiv = nullptr;
+  long long lda = 0, ldb = 0;
+};
+
+int host_bufs(Ctx& c, int n, int nrhs, HostBufs& hb) {
+  hb.lda = rup(std::max(n, 1), 8);
+  hb.ldb = rup(std::max(nrhs, 1), 8);
+  const size_t a = sizeof(double) * (size_t)n * hb.lda;
+  const size_t b = sizeof(double) * (size_t)n * hb.ldb;
+  const size_t p = sizeof(int) * (size_t)rup(std::max(n, 1), 64);
+  void* ws = nullptr;
+  LM_TRY(lm::ctx_workspace(c, 3, a + b + p, &ws));
+  hb.A = static_cast<double*>(ws);
+  hb.B = reinterpret_cast<double*>(static_cast<char*>(ws) + a);
+  hb.ipiv = reinterpret_cast<int*>(static_cast<char*>(ws) + a + b);
+  return LM_OK;
+}
+
+int h2d_2d(Ctx& c, double* dst, long long ldd, const double* src, long long lds, int rows, int cols) {
+  if (rows == 0 || cols == 0) return LM_OK;
+  LM_CUDA_TRY(cudaMemcpy2DAsync(dst, ldd * sizeof(double), src, lds * sizeof(double), cols * sizeof(double),
+                                rows, cudaMemcpyHostToDevice, c.stream));
+  return LM_OK;
+}
+
+int d2h_2d(Ctx& c, double* dst, long long ldd, const double* src, long long lds, int rows, int cols) {
+  if (rows == 0 || cols == 0) return LM_OK;
+  LM_CUDA_TRY(cudaMemcpy2DAsync(dst, ldd * sizeof(double), src, lds * sizeof(double), cols * sizeof(double),
+                                rows, cudaMemcpyDeviceToHost, c.stream));
+  return LM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lm_lu_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X,
+                     int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || (n > 0 && (!A || (nrhs > 0 && (!B || !X))))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    HostBufs hb;
+    LM_TRY(host_bufs(c, n, nrhs, hb));
+    LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
+    LM_TRY(h2d_2d(c, hb.B, hb.ldb, B, nrhs, n, nrhs));
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::dgetrf(c, n, hb.A, hb.lda, hb.ipiv, c.stream));
+    if (nrhs > 0) LM_TRY(lm::dgetrs(c, n, nrhs, hb.A, hb.lda, hb.ipiv, hb.B, hb.ldb, c.stream));
+    LM_TRY(d2h_2d(c, X, nrhs, hb.B, hb.ldb, n, nrhs));
+    int inf = 0;
+    int r = lm::read_status(c, &inf);
+    if (info) *info = inf;
+    return r;
+  });
+}
+
+int lm_chol_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X,
+                       int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || (n > 0 && (!A || (nrhs > 0 && (!B || !X))))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    HostBufs hb;
+    LM_TRY(host_bufs(c, n, nrhs, hb));
+    LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
+    LM_TRY(h2d_2d(c, hb.B, hb.ldb, B, nrhs, n, nrhs));
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::dpotrf(c, n, hb.A, hb.lda, c.stream));
+    if (nrhs > 0) LM_TRY(lm::dpotrs(c, n, nrhs, hb.A, hb.lda, hb.B, hb.ldb, c.stream));
+    LM_TRY(d2h_2d(c, X, nrhs, hb.B, hb.ldb, n, nrhs));
+    int inf = 0;
+    int r = lm::read_status(c, &inf);
+    if (info) *info = inf;
+    return r;
+  });
+}
+
+int lm_gemm_host(lm_ctx* ctx, int m, int n, int k, double alpha, const double* A, const double* B,
+                 double beta, const double* C0, double* C) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (m < 0 || n < 0 || k < 0) return LM_ERR_ARG;
+    if (m == 0 || n == 0) return LM_OK;
+    if (!C || (k > 0 && (!A || !B)) || (beta != 0.0 && !C0)) return LM_ERR_ARG;
+    const long long lda = rup(std::max(k, 1), 8), ldb = rup(n, 8), ldc = rup(n, 8);
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 3, sizeof(double) * ((size_t)m * lda + (size_t)k * ldb + (size_t)m * ldc), &ws));
+    double* dA = static_cast<double*>(ws);
+    double* dB = dA + (size_t)m * lda;
+    double* dC = dB + (size_t)k * ldb;
+    LM_TRY(h2d_2d(c, dA, lda, A, k, m, k));
+    LM_TRY(h2d_2d(c, dB, ldb, B, n, k, n));
+    if (beta != 0.0) LM_TRY(h2d_2d(c, dC, ldc, C0, n, m, n));
+    lm::GemmDesc d;
+    d.m = m; d.n = n; d.k = k; d.alpha = alpha; d.beta = beta;
+    d.A = dA; d.lda = lda; d.B = dB; d.ldb = ldb; d.C = dC; d.ldc = ldc;
+    LM_TRY(lm::dgemm(c, d, c.stream));
+    LM_TRY(d2h_2d(c, C, n, dC, ldc, m, n));
+    int r = lm::read_status(c, nullptr);
+    return r < 0 ? r : LM_OK;
+  });
+}
+
+int lm_matmul_host(lm_ctx* ctx, int m, int n, int k, const double* A, const double* B, double* C) {
+  return lm_gemm_host(ctx, m, n, k, 1.0, A, B, 0.0, nullptr, C);
+}
+
+int lm_lu_host(lm_ctx* ctx, int n, const double* A, double* LU, int* perm, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!A || !LU || !perm))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    HostBufs hb;
+    LM_TRY(host_bufs(c, n, 0, hb));
+    LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::dgetrf(c, n, hb.A, hb.lda, hb.ipiv, c.stream));
+    LM_TRY(d2h_2d(c, LU, n, hb.A, hb.lda, n, n));
+    std::vector<int> ip(n);
+    LM_CUDA_TRY(cudaMemcpyAsync(ip.data(), hb.ipiv, sizeof(int) * n, cudaMemcpyDeviceToHost, c.stream));
+    int inf = 0;
+    int r = lm::read_status(c, &inf);
+    if (r < 0) return r;
+    LM_TRY(lm_ipiv_to_perm(n, ip.data(), perm));
+    if (info) *info = inf;
+    return r;
+  });
+}
+
+int lm_cholesky_host(lm_ctx* ctx, int n, const double* A, double* G, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!A || !G))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    HostBufs hb;
+    LM_TRY(host_bufs(c, n, 0, hb));
+    LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::dpotrf(c, n, hb.A, hb.lda, c.stream));
+    LM_TRY(d2h_2d(c, G, n, hb.A, hb.lda, n, n));
+    int inf = 0;
+    int r = lm::read_status(c, &inf);
+    if (info) *info = inf;
+    return r;
+  });
+}
+
+int lm_det_host(lm_ctx* ctx, int n, const double* A, double* det) {
+  if (!det || n < 0) return LM_ERR_ARG;
+  if (n == 0) {
+    *det = 1.0;
+    return LM_OK;
+  }
+  std::vector<double> lu((size_t)n * n);
+  std::vector<int> perm(n);
+  int info = 0;
+  int r = lm_lu_host(ctx, n, A, lu.data(), perm.data(), &info);
+  if (r < 0) return r;
+  // det (LU.hs:534-545): left fold of the diagonal from 1, then the sign of
+  // the permutation counted as in countSwaps (LU.hs:548-557).
+  double prod = 1.0;
+  for (int i = 0; i < n; ++i) prod = prod * lu[(size_t)i * n + i];
+  int swaps = 0;
+  for (int i = 0; i < n; ++i) {
+    if (perm[i] == i) continue;
+    for (int j = i + 1; j < n; ++j)
+      if (perm[j] == i) {
+        perm[j] = perm[i];
+        break;
+      }
+    ++swaps;
+  }
+  *det = (swaps % 2 == 0) ? prod : -prod;
+  return LM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,217 @@
+// Host-side drivers of the FP64 factorisations and triangular solves.
+//
+// dgetrf — right-looking blocked LU, outer panels of kNB = 128 columns so the
+//   trailing update is a k = 128 DMMA GEMM (compute-bound on B200, unlike the
+//   reference's k = 32 update, LU.hs:311-357).  Each 128-wide panel is
+//   factored recursively (halves down to a cluster leaf of <= 32 columns):
+//     left half -> swap right half -> U12 = L11^-1 A12 -> A22 -= L21 U12 ->
+//     right half -> swap left half.
+//   Row interchanges are applied to every column of A, matching the
+//   reference's full-row rawSwapRows (fromCol = 0, LU.hs:324-325).
+// dpotrf — right-looking blocked Cholesky, kNB = 128: diagonal block in SMEM,
+//   L21 = A21 L11^-T (inverse block times the panel, on the tensor cores), then
+//   A22 -= L21 L21^T as a lower-triangle-only GEMM (SYRK tile skip).  Same
+//   mathematics as the reference's left-looking panelCholFactor
+//   (Chol.hs:279-321), different association.
+// dgetrs / dpotrs — blocked substitutions: a 128 x 128 triangular block
+//   solve, then the rest of the right-hand side updated by GEMM.
+#include <algorithm>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace lm {
+
+namespace {
+
+constexpr int kNB = 128;
+
+int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int* ipiv, cudaStream_t st) {
+  const int R = n - c0;
+  const int wmax = panel_leaf_max_width_for(c, R);
+  if (wmax <= 0) return LM_ERR_UNSUPPORTED;
+  if (w <= wmax) return panel_leaf<double>(c, A, lda, n, c0, w, ipiv, st);
+  // Split so that column offsets stay multiples of 4 (16-byte TMA alignment).
+  int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
+  if (w1 >= w) w1 = w - 4;
+  const int w2 = w - w1;
+  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, ipiv, st));
+  LM_TRY(laswp<double>(A, lda, n, ipiv, c0, c0 + w1, c0 + w1, c0 + w, 0, 0, ctx_status(c), st));
+  double* A11 = A + (long long)c0 * lda + c0;
+  LM_TRY(trsm_left<double>(A11, lda, w1, true, true, false, A11 + w1, lda, w2, st));
+  GemmDesc d;
+  d.m = R - w1; d.n = w2; d.k = w1;
+  d.alpha = -1.0; d.beta = 1.0;
+  d.A = A11 + (long long)w1 * lda; d.lda = lda;
+  d.B = A11 + w1; d.ldb = lda;
+  d.C = A11 + (long long)w1 * lda + w1; d.ldc = lda;
+  LM_TRY(dgemm(c, d, st));
+  LM_TRY(getrf_panel_rec(c, A, lda, n, c0 + w1, w2, ipiv, st));
+  LM_TRY(laswp<double>(A, lda, n, ipiv, c0 + w1, c0 + w, c0, c0 + w1, 0, 0, ctx_status(c), st));
+  return LM_OK;
+}
+
+}  // namespace
+
+int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) {
+  for (int k0 = 0; k0 < n; k0 += kNB) {
+    const int w = std::min(kNB, n - k0);
+    LM_TRY(getrf_panel_rec(c, A, lda, n, k0, w, ipiv, st));
+    // this panel's interchanges on the columns left and right of it
+    LM_TRY(laswp<double>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st));
+    if (k0 + w < n) {
+      double* A11 = A + (long long)k0 * lda + k0;
+      LM_TRY(trsm_left<double>(A11, lda, w, true, true, false, A11 + w, lda, n - k0 - w, st));
+      GemmDesc d;
+      d.m = n - k0 - w; d.n = n - k0 - w; d.k = w;
+      d.alpha = -1.0; d.beta = 1.0;
+      d.A = A11 + (long long)w * lda; d.lda = lda;
+      d.B = A11 + w; d.ldb = lda;
+      d.C = A11 + (long long)w * lda + w; d.ldc = lda;
+      LM_TRY(dgemm(c, d, st));
+    }
+  }
+  return LM_OK;
+}
+
+int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st) {
+  for (int j0 = 0; j0 < n; j0 += kNB) {
+    const int w = std::min(kNB, n - j0);
+    const int R = n - j0 - w;
+    double* A11 = A + (long long)j0 * lda + j0;
+    LM_TRY(potrf_block<double>(c, A11, lda, w, j0, st));
+    if (R > 0) {
+      void* ws = nullptr;
+      LM_TRY(ctx_workspace(c, 1, sizeof(double) * ((size_t)kNB * kNB + (size_t)R * kNB), &ws));
+      double* Linv = static_cast<double*>(ws);
+      double* W21 = Linv + (size_t)kNB * kNB;
+      double* A21 = A11 + (long long)w * lda;
+      LM_TRY(set_identity<double>(Linv, kNB, w, w, st));
+      LM_TRY(trsm_left<double>(A11, lda, w, true, false, false, Linv, kNB, w, st));
+      LM_TRY(copy2d<double>(W21, kNB, A21, lda, R, w, st));
+      GemmDesc t;  // L21 = A21 * L11^-T
+      t.m = R; t.n = w; t.k = w; t.alpha = 1.0; t.beta = 0.0;
+      t.A = W21; t.lda = kNB; t.B = Linv; t.ldb = kNB; t.b_trans = true;
+      t.C = A21; t.ldc = lda;
+      LM_TRY(dgemm(c, t, st));
+      GemmDesc s;  // A22 -= L21 L21^T (lower triangle)
+      s.m = R; s.n = R; s.k = w; s.alpha = -1.0; s.beta = 1.0;
+      s.A = A21; s.lda = lda; s.B = A21; s.ldb = lda; s.b_trans = true; s.lower_only = true;
+      s.C = A21 + w; s.ldc = lda;
+      LM_TRY(dgemm(c, s, st));
+    }
+  }
+  return zero_upper<double>(A, lda, n, st);
+}
+
+namespace {
+
+// Copy to even-stride, 16-byte aligned buffers when the caller's are not
+// (TMA row alignment); returns the buffers to use.
+struct SolveBufs {
+  const double* M;
+  long long ldm;
+  double* X;
+  long long ldx;
+  bool copied_x;
+};
+
+int solve_bufs(Ctx& c, int n, int nrhs, const double* M, long long ldm, double* B, long long ldb,
+               SolveBufs& sb, cudaStream_t st) {
+  sb.M = M; sb.ldm = ldm; sb.X = B; sb.ldx = ldb; sb.copied_x = false;
+  const bool m_ok = !(reinterpret_cast<uintptr_t>(M) & 15) && !(ldm & 1);
+  const bool x_ok = !(reinterpret_cast<uintptr_t>(B) & 15) && !(ldb & 1);
+  const long long ldm2 = m_ok ? 0 : (n + 7) / 8 * 8;
+  const long long ldx2 = x_ok ? 0 : (nrhs + 7) / 8 * 8;
+  const size_t bytes = sizeof(double) * ((size_t)n * ldm2 + (size_t)n * ldx2);
+  if (bytes == 0) return LM_OK;
+  void* ws = nullptr;
+  LM_TRY(ctx_workspace(c, 2, bytes, &ws));
+  double* p = static_cast<double*>(ws);
+  if (!m_ok) {
+    LM_TRY(copy2d<double>(p, ldm2, M, ldm, n, n, st));
+    sb.M = p; sb.ldm = ldm2;
+    p += (size_t)n * ldm2;
+  }
+  if (!x_ok) {
+    LM_TRY(copy2d<double>(p, ldx2, B, ldb, n, nrhs, st));
+    sb.X = p; sb.ldx = ldx2; sb.copied_x = true;
+  }
+  return LM_OK;
+}
+
+// Forward substitution with the lower triangle of M (unit or not), blocked.
+int forward_blocked(Ctx& c, int n, int nrhs, const double* M, long long ldm, bool unit, double* X,
+                    long long ldx, cudaStream_t st) {
+  for (int i0 = 0; i0 < n; i0 += kNB) {
+    const int w = std::min(kNB, n - i0);
+    const double* Mii = M + (long long)i0 * ldm + i0;
+    LM_TRY(trsm_left<double>(Mii, ldm, w, true, unit, false, X + (long long)i0 * ldx, ldx, nrhs, st));
+    if (i0 + w < n) {
+      GemmDesc d;
+      d.m = n - i0 - w; d.n = nrhs; d.k = w; d.alpha = -1.0; d.beta = 1.0;
+      d.A = Mii + (long long)w * ldm; d.lda = ldm;
+      d.B = X + (long long)i0 * ldx; d.ldb = ldx;
+      d.C = X + (long long)(i0 + w) * ldx; d.ldc = ldx;
+      LM_TRY(dgemm(c, d, st));
+    }
+  }
+  return LM_OK;
+}
+
+}  // namespace
+
+int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* ipiv, double* B,
+           long long ldb, cudaStream_t st) {
+  SolveBufs sb;
+  LM_TRY(solve_bufs(c, n, nrhs, LU, lda, B, ldb, sb, st));
+  // P b (applyPivotsForward, LU.hs:493-507)
+  LM_TRY(laswp<double>(sb.X, sb.ldx, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+  LM_TRY(forward_blocked(c, n, nrhs, sb.M, sb.ldm, true, sb.X, sb.ldx, st));
+  const int nblk = (n + kNB - 1) / kNB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int i0 = b * kNB;
+    const int w = std::min(kNB, n - i0);
+    const double* Uii = sb.M + (long long)i0 * sb.ldm + i0;
+    LM_TRY(trsm_left<double>(Uii, sb.ldm, w, false, false, false, sb.X + (long long)i0 * sb.ldx, sb.ldx, nrhs,
+                             st));
+    if (i0 > 0) {
+      GemmDesc d;
+      d.m = i0; d.n = nrhs; d.k = w; d.alpha = -1.0; d.beta = 1.0;
+      d.A = sb.M + i0; d.lda = sb.ldm;
+      d.B = sb.X + (long long)i0 * sb.ldx; d.ldb = sb.ldx;
+      d.C = sb.X; d.ldc = sb.ldx;
+      LM_TRY(dgemm(c, d, st));
+    }
+  }
+  if (sb.copied_x) LM_TRY(copy2d<double>(B, ldb, sb.X, sb.ldx, n, nrhs, st));
+  return LM_OK;
+}
+
+int dpotrs(Ctx& c, int n, int nrhs, const double* G, long long lda, double* B, long long ldb,
+           cudaStream_t st) {
+  SolveBufs sb;
+  LM_TRY(solve_bufs(c, n, nrhs, G, lda, B, ldb, sb, st));
+  LM_TRY(forward_blocked(c, n, nrhs, sb.M, sb.ldm, false, sb.X, sb.ldx, st));
+  // G^T x = y, bottom-up; the off-diagonal update uses G's row block transposed.
+  const int nblk = (n + kNB - 1) / kNB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int i0 = b * kNB;
+    const int w = std::min(kNB, n - i0);
+    const double* Gii = sb.M + (long long)i0 * sb.ldm + i0;
+    LM_TRY(trsm_left<double>(Gii, sb.ldm, w, true, false, true, sb.X + (long long)i0 * sb.ldx, sb.ldx, nrhs,
+                             st));
+    if (i0 > 0) {
+      GemmDesc d;
+      d.m = i0; d.n = nrhs; d.k = w; d.alpha = -1.0; d.beta = 1.0;
+      d.A = sb.M + (long long)i0 * sb.ldm; d.lda = sb.ldm; d.a_trans = true;
+      d.B = sb.X + (long long)i0 * sb.ldx; d.ldb = sb.ldx;
+      d.C = sb.X; d.ldc = sb.ldx;
+      LM_TRY(dgemm(c, d, st));
+    }
+  }
+  if (sb.copied_x) LM_TRY(copy2d<double>(B, ldb, sb.X, sb.ldx, n, nrhs, st));
+  return LM_OK;
+}
+
+}  // namespace lm

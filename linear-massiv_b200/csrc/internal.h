@@ -1,0 +1,100 @@
+// Internal (non-ABI) interfaces shared by the library's translation units.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstddef>
+
+namespace lm {
+
+constexpr int kMaxDevices = 64;
+
+struct Ctx;
+
+// --- context accessors (api.cu) ---------------------------------------------
+void count_launch(int n);  // process-wide kernel launch counter
+int* ctx_status(Ctx& c);        // device int[4]: error code, info, ticket, spare
+int ctx_num_sms(Ctx& c);
+int ctx_device(Ctx& c);
+// Grow-only device workspace owned by the context (slot 0..kWsSlots-1).
+constexpr int kWsSlots = 4;
+int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr);
+
+// TMA descriptor for a row-major 2D view: `inner` elements per row (contiguous),
+// `outer` rows, row stride `ld` elements; box of box_inner x box_outer.
+int make_tmap_2d(CUtensorMap* tm, CUtensorMapDataType dt, int elem_bytes, const void* base,
+                 long long inner, long long outer, long long ld, int box_inner, int box_outer,
+                 CUtensorMapSwizzle swz);
+
+// --- FP64 GEMM (dgemm.cu) ----------------------------------------------------
+// C = alpha * op(A) * op(B) + beta * C, row-major.
+//   a_trans = false: A is m x k (lda)  | true: A^T is stored, k x m (lda)
+//   b_trans = false: B is k x n (ldb)  | true: B^T is stored, n x k (ldb)
+// lower_only: only C(i,j) with j <= i is read or written (requires m == n).
+// max_ctas: cap on the persistent grid (0 = one CTA per SM).
+struct GemmDesc {
+  int m = 0, n = 0, k = 0;
+  double alpha = 1.0, beta = 0.0;
+  const double* A = nullptr;
+  long long lda = 0;
+  const double* B = nullptr;
+  long long ldb = 0;
+  double* C = nullptr;
+  long long ldc = 0;
+  bool a_trans = false, b_trans = false, lower_only = false;
+  int max_ctas = 0;
+};
+int dgemm(Ctx& c, const GemmDesc& d, cudaStream_t st);
+
+// --- shared kernels (blas_aux.cu) --------------------------------------------
+// Apply row interchanges ipiv[k0..k1) in order (row s <-> row ipiv[s]) to the
+// columns [ca0, ca1) and [cb0, cb1) of A (nrows rows).  A pivot row outside
+// [0, nrows) is skipped and recorded as LM_DEVERR_BOUNDS in status[0].
+template <typename T>
+int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int ca0, int ca1, int cb0, int cb1,
+          int* status, cudaStream_t st);
+
+// In-place triangular solve with a w x w block (w <= 128) of Tri (ldt) on the
+// w x ncols block B (ldb):  op(Tri) X = B.
+//   lower/unit describe Tri as stored; trans solves with Tri^T.
+template <typename T>
+int trsm_left(const T* Tri, long long ldt, int w, bool lower, bool unit, bool trans, T* B,
+              long long ldb, int ncols, cudaStream_t st);
+
+// 2D copy (rows x cols) between strided buffers on the device.
+template <typename T>
+int copy2d(T* dst, long long ldd, const T* src, long long lds, int rows, int cols, cudaStream_t st);
+
+// Set a rows x cols block to the identity (1 on the diagonal, 0 elsewhere).
+template <typename T>
+int set_identity(T* A, long long lda, int rows, int cols, cudaStream_t st);
+
+// Zero the strict upper triangle of an n x n matrix.
+template <typename T>
+int zero_upper(T* A, long long lda, int n, cudaStream_t st);
+
+// --- factorisations and solves ---------------------------------------------
+int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st);
+int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* ipiv, double* B,
+           long long ldb, cudaStream_t st);
+int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st);
+int dpotrs(Ctx& c, int n, int nrhs, const double* G, long long lda, double* B, long long ldb,
+           cudaStream_t st);
+
+// Panel factorisation kernels (panel.cu): LU of rows [c0, n) x columns
+// [c0, c0 + w) in place, w <= 32, recording ipiv[c0 .. c0 + w) (global rows)
+// and the first zero pivot in status[1].
+template <typename T>
+int panel_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int* ipiv, cudaStream_t st);
+int panel_leaf_max_width_for(Ctx& c, int rows);  // widest leaf one cluster holds for `rows`
+
+// Cholesky of a w x w diagonal block (w <= 128) in place, lower triangle;
+// records the first non-positive pivot (global index base + j + 1) in status[1].
+template <typename T>
+int potrf_block(Ctx& c, T* A, long long lda, int w, int base, cudaStream_t st);
+
+// r = b - A x for nrhs columns (FP64), and max-norm helpers (resid.cu).
+int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* X, long long ldx,
+              const double* B, long long ldb, double* R, long long ldr, cudaStream_t st);
+
+}  // namespace lm

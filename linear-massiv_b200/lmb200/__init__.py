@@ -1,0 +1,395 @@
+"""Python binding of liblm_b200.so (the C ABI in include/lm_b200.h).
+
+Function names mirror linear-massiv's public API for the dense-solve path
+(gemm, matMul, lu, luSolve, cholesky, choleskySolve, det): each takes
+device-resident torch float64 tensors, leaves its inputs untouched and returns
+fresh results, the way the reference's pure functions return fresh massiv
+arrays.  The raw in-place routines (dgetrf, dgetrs, dpotrf, dpotrs, dgemm)
+are exposed too.
+
+There is no fallback: if the CUDA library is missing or no GPU is visible,
+every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.dirname(_HERE)
+LIB_PATH = os.path.join(PKG_DIR, "liblm_b200.so")
+
+LM_OK = 0
+LM_ERR_ARG = -1
+LM_ERR_CUDA = -2
+LM_ERR_UNSUPPORTED = -3
+LM_ERR_TIMEOUT = -4
+LM_ERR_NOMEM = -5
+LM_ERR_NOT_CONVERGED = -6
+
+# Every symbol include/lm_b200.h declares (checked by the CPU test suite).
+EXPORTS = [
+    "lm_ctx_create", "lm_ctx_destroy", "lm_ctx_set_stream", "lm_ctx_get_stream",
+    "lm_ctx_synchronize", "lm_ctx_check", "lm_status_string", "lm_last_error",
+    "lm_launch_count", "lm_dmalloc", "lm_dfree", "lm_h2d", "lm_d2h", "lm_dgemm",
+    "lm_dgetrf", "lm_dgetrs", "lm_dgesv", "lm_dpotrf", "lm_dpotrs", "lm_dposv",
+    "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
+    "lm_lu_host", "lm_cholesky_host", "lm_det_host", "lm_ipiv_to_perm", "lm_dresidual",
+]
+
+
+class LMError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        msg = _lib().lm_status_string(status).decode()
+        last = _lib().lm_last_error().decode()
+        super().__init__(f"{what}: {msg} ({status}){': ' + last if last else ''}")
+
+
+def build(verbose: bool = False) -> str:
+    """Compile liblm_b200.so in-tree with the package Makefile (sm_100a)."""
+    out = None if verbose else subprocess.DEVNULL
+    subprocess.run(["make", "-s", "-j8", "-C", PKG_DIR], check=True, stdout=out)
+    return LIB_PATH
+
+
+_L = None
+_LOCK = threading.Lock()
+
+
+def _lib():
+    global _L
+    with _LOCK:
+        if _L is None:
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"liblm_b200.so is not built ({LIB_PATH}); run __graft_entry__.build()")
+            L = ctypes.CDLL(LIB_PATH)
+            vp, i, d, sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_size_t
+            ip = ctypes.POINTER(ctypes.c_int)
+            dp = ctypes.POINTER(ctypes.c_double)
+            sigs = {
+                "lm_ctx_create": ([ctypes.POINTER(vp), i], i),
+                "lm_ctx_destroy": ([vp], i),
+                "lm_ctx_set_stream": ([vp, vp], i),
+                "lm_ctx_get_stream": ([vp], vp),
+                "lm_ctx_synchronize": ([vp], i),
+                "lm_ctx_check": ([vp], i),
+                "lm_status_string": ([i], ctypes.c_char_p),
+                "lm_last_error": ([], ctypes.c_char_p),
+                "lm_launch_count": ([], ctypes.c_longlong),
+                "lm_dmalloc": ([vp, ctypes.POINTER(vp), sz], i),
+                "lm_dfree": ([vp, vp], i),
+                "lm_h2d": ([vp, vp, vp, sz], i),
+                "lm_d2h": ([vp, vp, vp, sz], i),
+                "lm_dgemm": ([vp, i, i, i, d, vp, i, vp, i, d, vp, i], i),
+                "lm_dgetrf": ([vp, i, vp, i, vp, ip], i),
+                "lm_dgetrs": ([vp, i, i, vp, i, vp, vp, i], i),
+                "lm_dgesv": ([vp, i, i, vp, i, vp, vp, i, ip], i),
+                "lm_dpotrf": ([vp, i, vp, i, ip], i),
+                "lm_dpotrs": ([vp, i, i, vp, i, vp, i], i),
+                "lm_dposv": ([vp, i, i, vp, i, vp, i, ip], i),
+                "lm_lu_solve_host": ([vp, i, i, dp, dp, dp, ip], i),
+                "lm_chol_solve_host": ([vp, i, i, dp, dp, dp, ip], i),
+                "lm_matmul_host": ([vp, i, i, i, dp, dp, dp], i),
+                "lm_gemm_host": ([vp, i, i, i, d, dp, dp, d, dp, dp], i),
+                "lm_lu_host": ([vp, i, dp, dp, ip, ip], i),
+                "lm_cholesky_host": ([vp, i, dp, dp, ip], i),
+                "lm_det_host": ([vp, i, dp, dp], i),
+                "lm_ipiv_to_perm": ([i, ip, ip], i),
+                "lm_dresidual": ([vp, i, i, vp, i, vp, i, vp, i, vp, i], i),
+            }
+            for name, (args, res) in sigs.items():
+                fn = getattr(L, name)
+                fn.argtypes = args
+                fn.restype = res
+            _L = L
+    return _L
+
+
+def lib():
+    return _lib()
+
+
+def launch_count() -> int:
+    return int(_lib().lm_launch_count())
+
+
+def _check(status: int, what: str) -> int:
+    if status < 0:
+        raise LMError(status, what)
+    return status
+
+
+class Context:
+    """An lm_ctx bound to one device.  By default its kernels run on torch's
+    current stream so torch events and synchronisation see them."""
+
+    def __init__(self, device: int = 0, use_torch_stream: bool = True):
+        import torch
+
+        if not torch.cuda.is_available():
+            raise RuntimeError("lmb200 needs a CUDA device; none is visible")
+        self.device = device
+        h = ctypes.c_void_p()
+        _check(_lib().lm_ctx_create(ctypes.byref(h), device), "lm_ctx_create")
+        self.h = h
+        if use_torch_stream:
+            with torch.cuda.device(device):
+                s = torch.cuda.current_stream(device).cuda_stream
+            _check(_lib().lm_ctx_set_stream(self.h, ctypes.c_void_p(s)), "lm_ctx_set_stream")
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().lm_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        _check(_lib().lm_ctx_synchronize(self.h), "lm_ctx_synchronize")
+
+    def check(self):
+        _check(_lib().lm_ctx_check(self.h), "device status")
+
+
+_DEFAULT = {}
+
+
+def default_context(device: int = 0) -> Context:
+    c = _DEFAULT.get(device)
+    if c is None:
+        c = Context(device)
+        _DEFAULT[device] = c
+    return c
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _mat(t, name):
+    import torch
+
+    if not (t.is_cuda and t.dtype == torch.float64 and t.dim() == 2 and t.stride(1) == 1):
+        raise ValueError(f"{name} must be a row-major (stride(1) == 1) float64 CUDA matrix")
+    return t
+
+
+# ---- raw in-place routines ---------------------------------------------------
+
+def dgemm(alpha, A, B, beta, C, ctx: Context | None = None):
+    """C <- alpha*A*B + beta*C in place."""
+    ctx = ctx or default_context(C.device.index or 0)
+    _mat(A, "A"), _mat(B, "B"), _mat(C, "C")
+    m, k = A.shape
+    n = B.shape[1]
+    if B.shape[0] != k or C.shape != (m, n):
+        raise ValueError("dimension mismatch")
+    _check(_lib().lm_dgemm(ctx.h, m, n, k, float(alpha), _ptr(A), A.stride(0), _ptr(B), B.stride(0),
+                           float(beta), _ptr(C), C.stride(0)), "lm_dgemm")
+    return C
+
+
+def dgetrf(A, ipiv, ctx: Context | None = None, sync_info: bool = True) -> int:
+    """In-place LU of A; ipiv is an int32 CUDA tensor of length n.  Returns info."""
+    ctx = ctx or default_context(A.device.index or 0)
+    _mat(A, "A")
+    n = A.shape[0]
+    info = ctypes.c_int(0)
+    st = _lib().lm_dgetrf(ctx.h, n, _ptr(A), A.stride(0), _ptr(ipiv), ctypes.byref(info) if sync_info else None)
+    _check(st, "lm_dgetrf")
+    return info.value
+
+
+def dgetrs(LU, ipiv, B, ctx: Context | None = None):
+    ctx = ctx or default_context(LU.device.index or 0)
+    _mat(LU, "LU"), _mat(B, "B")
+    n, nrhs = B.shape
+    _check(_lib().lm_dgetrs(ctx.h, n, nrhs, _ptr(LU), LU.stride(0), _ptr(ipiv), _ptr(B), B.stride(0)), "lm_dgetrs")
+    return B
+
+
+def dpotrf(A, ctx: Context | None = None, sync_info: bool = True) -> int:
+    ctx = ctx or default_context(A.device.index or 0)
+    _mat(A, "A")
+    info = ctypes.c_int(0)
+    st = _lib().lm_dpotrf(ctx.h, A.shape[0], _ptr(A), A.stride(0), ctypes.byref(info) if sync_info else None)
+    _check(st, "lm_dpotrf")
+    return info.value
+
+
+def dpotrs(G, B, ctx: Context | None = None):
+    ctx = ctx or default_context(G.device.index or 0)
+    _mat(G, "G"), _mat(B, "B")
+    n, nrhs = B.shape
+    _check(_lib().lm_dpotrs(ctx.h, n, nrhs, _ptr(G), G.stride(0), _ptr(B), B.stride(0)), "lm_dpotrs")
+    return B
+
+
+def dresidual(A, X, B, R, ctx: Context | None = None):
+    ctx = ctx or default_context(A.device.index or 0)
+    n, nrhs = B.shape
+    _check(_lib().lm_dresidual(ctx.h, n, nrhs, _ptr(A), A.stride(0), _ptr(X), X.stride(0), _ptr(B), B.stride(0),
+                               _ptr(R), R.stride(0)), "lm_dresidual")
+    return R
+
+
+# ---- the reference's pure API (fresh outputs, inputs untouched) ---------------
+
+def _as_cols(b):
+    return (b.unsqueeze(1), True) if b.dim() == 1 else (b, False)
+
+
+def gemm(alpha, A, B, beta, C, ctx: Context | None = None):
+    """gemm alpha A B beta C (Level3.hs:102-131)."""
+    out = C.clone()
+    return dgemm(alpha, A, B, beta, out, ctx)
+
+
+def matMul(A, B, ctx: Context | None = None):
+    """matMul / matMulP (Level3.hs:144-147, 183-207)."""
+    import torch
+
+    C = torch.empty((A.shape[0], B.shape[1]), dtype=torch.float64, device=A.device)
+    return dgemm(1.0, A, B, 0.0, C, ctx)
+
+
+def lu_factor(A, ctx: Context | None = None):
+    """Device LU: (packed LU, swap list ipiv, info)."""
+    import torch
+
+    LU = A.clone()
+    ipiv = torch.empty(A.shape[0], dtype=torch.int32, device=A.device)
+    info = dgetrf(LU, ipiv, ctx)
+    return LU, ipiv, info
+
+
+def lu(A, ctx: Context | None = None):
+    """lu (LU.hs:121-122): (packed LU, permutation vector perm)."""
+    LU, ipiv, _ = lu_factor(A, ctx)
+    return LU, ipiv_to_perm(ipiv.cpu().tolist())
+
+
+def luSolve(A, b, ctx: Context | None = None):
+    """luSolve / luSolveP (LU.hs:240-304) for a vector or an n x nrhs matrix."""
+    B, vec = _as_cols(b)
+    LU, ipiv, _ = lu_factor(A, ctx)
+    X = B.clone().contiguous()
+    dgetrs(LU, ipiv, X, ctx)
+    return X[:, 0] if vec else X
+
+
+def cholesky(A, ctx: Context | None = None):
+    """cholesky (Chol.hs:114-147): G, zeros above the diagonal."""
+    G = A.clone()
+    dpotrf(G, ctx)
+    return G
+
+
+def choleskySolve(A, b, ctx: Context | None = None):
+    """choleskySolve / choleskySolveP (Chol.hs:229-273)."""
+    B, vec = _as_cols(b)
+    G = cholesky(A, ctx)
+    X = B.clone().contiguous()
+    dpotrs(G, X, ctx)
+    return X[:, 0] if vec else X
+
+
+def det(A, ctx: Context | None = None) -> float:
+    """det (LU.hs:534-545)."""
+    import numpy as np
+
+    ctx = ctx or default_context(A.device.index or 0)
+    a = np.ascontiguousarray(A.detach().cpu().numpy(), dtype=np.float64)
+    out = ctypes.c_double(0.0)
+    _check(_lib().lm_det_host(ctx.h, a.shape[0], a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                              ctypes.byref(out)), "lm_det_host")
+    return out.value
+
+
+def ipiv_to_perm(ipiv):
+    n = len(ipiv)
+    perm = list(range(n))
+    for k, p in enumerate(ipiv):
+        perm[k], perm[p] = perm[p], perm[k]
+    return perm
+
+
+# ---- host-buffer entry points (what a pure FFI binding calls) -----------------
+
+def _np_ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def lu_solve_host(A, B, ctx: Context | None = None):
+    """lm_lu_solve_host on host numpy arrays: returns (X, info)."""
+    import numpy as np
+
+    ctx = ctx or default_context(0)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    vec = B.ndim == 1
+    B2 = np.ascontiguousarray(B.reshape(A.shape[0], -1), dtype=np.float64)
+    X = np.empty_like(B2)
+    info = ctypes.c_int(0)
+    _check(_lib().lm_lu_solve_host(ctx.h, A.shape[0], B2.shape[1], _np_ptr(A), _np_ptr(B2), _np_ptr(X),
+                                   ctypes.byref(info)), "lm_lu_solve_host")
+    return (X[:, 0] if vec else X), info.value
+
+
+def chol_solve_host(A, B, ctx: Context | None = None):
+    import numpy as np
+
+    ctx = ctx or default_context(0)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    vec = B.ndim == 1
+    B2 = np.ascontiguousarray(B.reshape(A.shape[0], -1), dtype=np.float64)
+    X = np.empty_like(B2)
+    info = ctypes.c_int(0)
+    _check(_lib().lm_chol_solve_host(ctx.h, A.shape[0], B2.shape[1], _np_ptr(A), _np_ptr(B2), _np_ptr(X),
+                                     ctypes.byref(info)), "lm_chol_solve_host")
+    return (X[:, 0] if vec else X), info.value
+
+
+def gemm_host(alpha, A, B, beta, C0, ctx: Context | None = None):
+    import numpy as np
+
+    ctx = ctx or default_context(0)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64)
+    C0 = np.ascontiguousarray(C0, dtype=np.float64)
+    C = np.empty((A.shape[0], B.shape[1]))
+    _check(_lib().lm_gemm_host(ctx.h, A.shape[0], B.shape[1], A.shape[1], float(alpha), _np_ptr(A), _np_ptr(B),
+                               float(beta), _np_ptr(C0), _np_ptr(C)), "lm_gemm_host")
+    return C
+
+
+def lu_host(A, ctx: Context | None = None):
+    import numpy as np
+
+    ctx = ctx or default_context(0)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n = A.shape[0]
+    LU = np.empty_like(A)
+    perm = np.zeros(n, dtype=np.int32)
+    info = ctypes.c_int(0)
+    _check(_lib().lm_lu_host(ctx.h, n, _np_ptr(A), _np_ptr(LU), perm.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                             ctypes.byref(info)), "lm_lu_host")
+    return LU, perm, info.value
+
+
+def cholesky_host(A, ctx: Context | None = None):
+    import numpy as np
+
+    ctx = ctx or default_context(0)
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    G = np.empty_like(A)
+    info = ctypes.c_int(0)
+    _check(_lib().lm_cholesky_host(ctx.h, A.shape[0], _np_ptr(A), _np_ptr(G), ctypes.byref(info)),
+           "lm_cholesky_host")
+    return G, info.value
