@@ -1,0 +1,423 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 dense-solve path (one JSON line on rank 0).
+
+Workloads (--workload):
+  lu    (default) luSolve, A n x n i.i.d. uniform[-1,1] (numpy Philox, seeded),
+        b uniform[-1,1], nrhs right-hand sides; one step = copy A into the
+        work buffer (luSolveP's thaw), LU with partial pivoting, solve.
+  chol  choleskySolve with A = B B^T + n I, B uniform[-1,1].
+  gemm  C = A B, m = n = k.
+Metric: FP64-accurate solves per second (GEMMs per second for gemm), whole
+job.  Multi-GPU: replicas only — every rank solves its own system, no
+collective on the data path; value = all solves / max-over-ranks time.
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle restatement of luSolveP / choleskySolveP / matMulP; linear-massiv is
+Haskell and no GHC exists here) on the host cores, as independent solves on
+every hardware thread, on a bounded-size sample scaled to the workload's n by
+the n^3 flop count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "linear-massiv_b200"))
+
+FLOPS = {
+    "lu": lambda n, r: 2.0 / 3.0 * n ** 3 + 2.0 * n * n * r,
+    "chol": lambda n, r: 1.0 / 3.0 * n ** 3 + 2.0 * n * n * r,
+    "gemm": lambda n, r: 2.0 * n ** 3,
+}
+
+
+def gemm_k(a):
+    return a.k if a.k > 0 else a.n
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--workload", choices=["lu", "chol", "gemm"], default="lu")
+    p.add_argument("--n", type=int, default=16384)
+    p.add_argument("--nrhs", type=int, default=1)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS DGEMM peak measurement")
+    p.add_argument("--k", type=int, default=0, help="gemm inner dimension (default n); k < n adds beta = 1")
+    p.add_argument("--no-profile", action="store_true", help="time without the per-phase event tracing")
+    return p.parse_args()
+
+
+def workload_name(a):
+    if a.workload == "lu":
+        return f"luSolve FP64 n={a.n} nrhs={a.nrhs}, A uniform[-1,1]"
+    if a.workload == "chol":
+        return f"choleskySolve FP64 n={a.n} nrhs={a.nrhs}, A = B B^T + n I"
+    if gemm_k(a) != a.n:
+        return f"gemm FP64 m=n={a.n} k={gemm_k(a)} C += A B, uniform[-1,1]"
+    return f"gemm FP64 m=n=k={a.n}, uniform[-1,1]"
+
+
+def metric_name(a):
+    return "FP64 GEMMs/s" if a.workload == "gemm" else "FP64-accurate solves/s"
+
+
+# ---- clocks sampled during the timed region ----------------------------------------
+
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200", "-i", str(gpu_index)], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None,
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit()),
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---- distributed plumbing ------------------------------------------------------------
+
+def dist_init(a):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        if a.impl == "ours":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- inputs ---------------------------------------------------------------------------
+
+def make_inputs(a, rank, torch, np):
+    g = np.random.Generator(np.random.Philox(a.seed + 7919 * rank))
+    n = a.n
+    A = torch.from_numpy(g.uniform(-1.0, 1.0, (n, n)))
+    if a.workload == "chol":
+        Bd = A.cuda()
+        S = Bd @ Bd.T  # input preparation only (not timed)
+        S.diagonal().add_(float(n))
+        S = 0.5 * (S + S.T)
+        A = S.cpu()
+        del Bd, S
+    if a.workload == "gemm" and gemm_k(a) != n:
+        A = A[:, :gemm_k(a)].contiguous()
+    B = torch.from_numpy(g.uniform(-1.0, 1.0, (gemm_k(a) if a.workload == "gemm" else n,
+                                               a.nrhs if a.workload != "gemm" else n)))
+    return A.pin_memory(), B.pin_memory()
+
+
+def measure_fp64_peak(torch):
+    """cuBLAS DGEMM 8192^3 throughput on this GPU (the FP64 roofline denominator)."""
+    n = 8192
+    x = torch.rand((n, n), dtype=torch.float64, device="cuda")
+    y = torch.rand((n, n), dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(x, y)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(x, y)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3))
+    del x, y
+    torch.cuda.empty_cache()
+    return best / 1e12
+
+
+def cpu_baseline(a):
+    """Oracle luSolveP/choleskySolveP/matMulP single-threaded on a bounded sample."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    ns = min(a.n, 2048)
+    g = np.random.Generator(np.random.Philox(a.seed + 1))
+    A = g.uniform(-1.0, 1.0, (ns, ns))
+    b = g.uniform(-1.0, 1.0, ns)
+    if a.workload == "chol":
+        A = A @ A.T + ns * np.eye(ns)
+    fn = {"lu": lambda: O.lu_solve_p(A, b), "chol": lambda: O.chol_solve_p(A, b),
+          "gemm": lambda: O.matmul_p(A, A)}[a.workload]
+    fn()
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        fn()
+        reps += 1
+        if time.perf_counter() - t0 > 8.0 or reps >= 20:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    scale = FLOPS[a.workload](ns, 1) / FLOPS[a.workload](a.n, a.nrhs)
+    return {"value": scale / dt, "unit": metric_name(a), "cores": 1, "kind": "port",
+            "sample": f"{reps} single-threaded oracle solves at n={ns} ({dt:.3f} s each), scaled to n={a.n} "
+                      f"by the flop count"}
+
+
+# ---- the reference arm ------------------------------------------------------------------
+
+def run_reference(a, world, rank):
+    if rank != 0:
+        return
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = os.cpu_count() or 1
+    ns = min(a.n, 1024)
+    g = np.random.Generator(np.random.Philox(a.seed + 1))
+    A = g.uniform(-1.0, 1.0, (ns, ns))
+    b = g.uniform(-1.0, 1.0, ns)
+    if a.workload == "chol":
+        A = A @ A.T + ns * np.eye(ns)
+
+    def step():
+        if a.workload == "lu":
+            O.lu_solve_p_many(A, b, threads, threads)
+        elif a.workload == "chol":
+            O.chol_solve_p_many(A, b, threads, threads)
+        else:
+            O.matmul_par(A, A, threads)
+
+    for _ in range(a.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        step()
+    dt = time.perf_counter() - t0
+    per_step = threads if a.workload != "gemm" else 1
+    scale = FLOPS[a.workload](ns, 1) / FLOPS[a.workload](a.n, a.nrhs)
+    value = per_step * a.steps / dt * scale
+    sample = (f"each step: {per_step} independent oracle {'solves' if per_step > 1 else 'GEMM (matMulPPar tiling)'} "
+              f"at n={ns} on {threads} host threads; scaled to n={a.n} by the flop count")
+    line = {"impl": "reference", "metric": metric_name(a), "value": value, "unit": metric_name(a),
+            "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded numpy Philox)", "config": {"workload": workload_name(a), "sample_n": ns},
+            "cpu_baseline": {"value": value, "unit": metric_name(a), "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": metric_name(a), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---- our arm ------------------------------------------------------------------------------
+
+def run_ours(a, world, rank, local):
+    import numpy as np
+    import torch
+
+    import lmb200
+
+    torch.cuda.set_device(local)
+    ctx = lmb200.Context(local)
+    lib = lmb200.lib()
+    n, nrhs = a.n, a.nrhs
+    A_h, B_h = make_inputs(a, rank, torch, np)
+    A_d = A_h.cuda()
+    B_d = B_h.cuda()
+    work = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    X = torch.empty_like(B_d)
+    ipiv = torch.empty(n, dtype=torch.int32, device="cuda")
+    P = lmb200._ptr
+
+    kk = gemm_k(a)
+
+    def step():
+        if a.workload == "gemm":
+            st = lib.lm_dgemm(ctx.h, n, n, kk, 1.0, P(A_d), kk, P(B_d), n, 1.0 if kk != n else 0.0, P(work), n)
+        else:
+            work.copy_(A_d)
+            X.copy_(B_d)
+            fn = lib.lm_dgesv if a.workload == "lu" else None
+            if a.workload == "lu":
+                st = fn(ctx.h, n, nrhs, P(work), n, P(ipiv), P(X), nrhs, None)
+            else:
+                st = lib.lm_dposv(ctx.h, n, nrhs, P(work), n, P(X), nrhs, None)
+        if st < 0:
+            raise lmb200.LMError(st, "bench step")
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    ctx.check()
+    # accuracy of the last warm-up result (FP64 backward error, checked on the GPU)
+    accuracy = {}
+    if a.workload != "gemm":
+        R = B_d - A_d @ X
+        num = R.abs().max().item()
+        den = A_d.abs().sum(dim=1).max().item() * X.abs().max().item() + B_d.abs().max().item()
+        accuracy = {"backward_error": num / den, "bound": 1e-15 * n}
+        del R
+    peak = measure_fp64_peak(torch) if (rank == 0 and not a.no_peak) else None
+
+    ctx.profile(not a.no_profile)
+    ctx.profile_read()
+    launches0 = lmb200.launch_count()
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    th0 = time.perf_counter()
+    for _ in range(a.steps):
+        step()
+    host_enqueue_ms = (time.perf_counter() - th0) * 1e3 / a.steps
+    e1.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    t_local = e0.elapsed_time(e1) * 1e-3
+    launches = lmb200.launch_count() - launches0
+    phases = ctx.profile_read()
+    ctx.profile(False)
+    t = max_over_ranks(t_local, world)
+    value = world * a.steps / t
+
+    # e2e through the host-buffer entry point: H2D of A and B, solve, D2H of X
+    Xh = torch.empty((n, n) if a.workload == "gemm" else tuple(B_h.shape), dtype=torch.float64).pin_memory()
+    dp = lmb200._np_ptr
+
+    def e2e_step():
+        if a.workload == "lu":
+            st = lib.lm_lu_solve_host(ctx.h, n, nrhs, dp(A_h.numpy()), dp(B_h.numpy()), dp(Xh.numpy()), None)
+        elif a.workload == "chol":
+            st = lib.lm_chol_solve_host(ctx.h, n, nrhs, dp(A_h.numpy()), dp(B_h.numpy()), dp(Xh.numpy()), None)
+        else:
+            st = lib.lm_matmul_host(ctx.h, n, n, kk, dp(A_h.numpy()), dp(B_h.numpy()), dp(Xh.numpy()))
+        if st < 0:
+            raise lmb200.LMError(st, "e2e step")
+
+    e2e_val = None
+    if a.e2e_steps > 0:
+        e2e_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+        e2e_val = world * a.e2e_steps / t_e2e
+    h2d = A_h.numel() * 8 + B_h.numel() * 8
+    d2h = Xh.numel() * 8
+
+    if rank != 0:
+        return
+    gp = phases["gemm"]
+    achieved = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
+    total_ms = sum(p["ms"] for p in phases.values())
+    line = {
+        "metric": metric_name(a), "value": value, "unit": metric_name(a), "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded numpy Philox, uniform[-1,1])",
+        "config": {"workload": workload_name(a), "n": n, "nrhs": nrhs, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (8 n^2 bytes per matrix)"},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_val, "unit": metric_name(a), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": a.e2e_steps, "api": "lm_lu_solve_host / lm_chol_solve_host / lm_matmul_host"},
+        "roofline": {"bound": "tensor", "kernel": "dgemm_dmma_kernel (FP64 DMMA trailing updates)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)",
+                     "gemm_launches_per_step": gp["launches"] / a.steps},
+        "phases_ms_per_step": {k: v["ms"] / a.steps for k, v in phases.items()},
+        "phase_share": {k: (v["ms"] / total_ms if total_ms else None) for k, v in phases.items()},
+        "tflops_whole_step": (2.0 * n * n * kk if a.workload == "gemm" else FLOPS[a.workload](n, nrhs)) * a.steps / t / 1e12,
+        "host_enqueue_ms_per_step": host_enqueue_ms,
+        "profiled": not a.no_profile,
+        "accuracy": accuracy,
+        "clocks": clk,
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(a)
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    world, rank, local = dist_init(a)
+    try:
+        if a.impl == "reference":
+            run_reference(a, world, rank)
+        else:
+            run_ours(a, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -66,6 +66,19 @@ const char* lm_last_error(void);
 /* Number of kernel launches this library has issued in this process. */
 long long lm_launch_count(void);
 
+/* ---- per-phase tracing ----------------------------------------------------
+ * When enabled, every kernel of the named phases is bracketed by CUDA events
+ * on the context's stream; lm_ctx_profile_read aggregates them per phase:
+ * launches, device milliseconds, algorithmic FLOPs and bytes.
+ * Phases: 0 GEMM (trailing updates, solve updates), 1 panel (LU leaf,
+ * Cholesky diagonal block), 2 row interchanges, 3 triangular block solves,
+ * 4 other (copies, residuals). */
+#define LM_PHASES 5
+int lm_ctx_profile(lm_ctx* ctx, int enable);
+/* Synchronises; fills arrays of LM_PHASES entries (any may be NULL) and
+ * clears the records. */
+int lm_ctx_profile_read(lm_ctx* ctx, long long* launches, double* ms, double* flops, double* bytes);
+
 /* ---- memory (device buffers stay resident between calls) -------------- */
 int lm_dmalloc(lm_ctx* ctx, void** ptr, size_t bytes);
 int lm_dfree(lm_ctx* ctx, void* ptr);

@@ -15,7 +15,28 @@ struct lm_ctx;
 
 namespace lm {
 
+struct ProfRec {
+  int phase;
+  cudaEvent_t a, b;
+  double flops, bytes;
+};
+
+struct GraphEntry {
+  std::string key;
+  int stage = 0;  // 1: seen once (eager), 2: captured
+  cudaGraphExec_t exec = nullptr;
+  long long nlaunch = 0;  // kernels in the graph (for the launch counter)
+};
+
 struct Ctx {
+  bool graphs = true;         // capture repeated call sequences into CUDA graphs
+  std::vector<GraphEntry> gcache;
+  long long ws_generation = 0;
+  cudaStream_t side = nullptr;  // capture stream when the caller's stream is the legacy default
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  bool prof = false;
+  std::vector<ProfRec> recs;
+  std::vector<cudaEvent_t> pool;
   int device = 0;
   int num_sms = 0;
   cudaStream_t stream = nullptr;
@@ -52,6 +73,34 @@ int load_encode() {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+namespace {
+cudaEvent_t take_event(Ctx& c) {
+  if (!c.pool.empty()) {
+    cudaEvent_t e = c.pool.back();
+    c.pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+Prof::Prof(Ctx& cc, int ph, double f, double b, cudaStream_t s) : c(cc), phase(ph), flops(f), bytes(b), st(s) {
+  if (c.prof) {
+    a = take_event(c);
+    cudaEventRecord(a, st);
+  }
+}
+
+Prof::~Prof() {
+  if (a) {
+    cudaEvent_t b = take_event(c);
+    cudaEventRecord(b, st);
+    c.recs.push_back({phase, a, b, flops, bytes});
+  }
+}
+
 int* ctx_status(Ctx& c) { return c.d_status; }
 int ctx_num_sms(Ctx& c) { return c.num_sms; }
 int ctx_device(Ctx& c) { return c.device; }
@@ -67,6 +116,7 @@ int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr) {
       c.ws_bytes[slot] = 0;
     }
     size_t want = std::max(bytes, (size_t)1 << 20);
+    ++c.ws_generation;  // captured graphs that baked in the old buffer are stale
     if (cudaMalloc(&c.ws[slot], want) != cudaSuccess) {
       cudaGetLastError();
       set_last_error("workspace allocation failed");
@@ -117,6 +167,88 @@ int read_status(Ctx& c, int* info_out) {
   }
   if (info_out) *info_out = h[1];
   return h[1];
+}
+
+// Run `body(stream)` — a fixed sequence of launches — through a cached CUDA
+// graph: the first call with a key runs eagerly (sizing workspaces, setting
+// kernel attributes), the second is captured and replayed, later calls only
+// replay.  Disabled while tracing is on (event timings need eager launches).
+template <typename F>
+int run_graphed(Ctx& c, const std::string& key0, F&& body) {
+  if (!c.graphs || c.prof) return body(c.stream);
+  const std::string key = key0 + "|g" + std::to_string(c.ws_generation);
+  GraphEntry* e = nullptr;
+  for (auto& g : c.gcache)
+    if (g.key == key) e = &g;
+  if (!e) {
+    if (c.gcache.size() >= 16) {
+      if (c.gcache.front().exec) cudaGraphExecDestroy(c.gcache.front().exec);
+      c.gcache.erase(c.gcache.begin());
+    }
+    c.gcache.push_back(GraphEntry{key, 1, nullptr});
+    return body(c.stream);
+  }
+  // The legacy default stream cannot be captured: use a side stream joined
+  // to the caller's stream by events.
+  cudaStream_t cs = c.stream;
+  const bool via_side = (c.stream == nullptr || c.stream == cudaStreamLegacy || c.stream == cudaStreamPerThread);
+  if (via_side) {
+    if (!c.side) {
+      LM_CUDA_TRY(cudaStreamCreateWithFlags(&c.side, cudaStreamNonBlocking));
+      LM_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_in, cudaEventDisableTiming));
+      LM_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_out, cudaEventDisableTiming));
+    }
+    cs = c.side;
+  }
+  if (e->stage == 1) {
+    if (via_side) {
+      LM_CUDA_TRY(cudaEventRecord(c.ev_in, c.stream));
+      LM_CUDA_TRY(cudaStreamWaitEvent(cs, c.ev_in, 0));
+    }
+    LM_CUDA_TRY(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const long long l0 = g_launches.load();
+    int r = body(cs);
+    e->nlaunch = g_launches.load() - l0;
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    if (r != LM_OK) {
+      if (g) cudaGraphDestroy(g);
+      return r;
+    }
+    if (ce != cudaSuccess) {
+      cudaGetLastError();
+      set_last_error(std::string("graph capture failed: ") + cudaGetErrorString(ce));
+      return LM_ERR_CUDA;
+    }
+    cudaGraphExec_t ex = nullptr;
+    ce = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      set_last_error(std::string("graph instantiate failed: ") + cudaGetErrorString(ce));
+      return LM_ERR_CUDA;
+    }
+    e->exec = ex;
+    e->stage = 2;
+    LM_CUDA_TRY(cudaGraphLaunch(ex, cs));
+  } else {
+    if (via_side) {
+      LM_CUDA_TRY(cudaEventRecord(c.ev_in, c.stream));
+      LM_CUDA_TRY(cudaStreamWaitEvent(cs, c.ev_in, 0));
+    }
+    LM_CUDA_TRY(cudaGraphLaunch(e->exec, cs));
+    count_launch((int)e->nlaunch);
+  }
+  if (via_side) {
+    LM_CUDA_TRY(cudaEventRecord(c.ev_out, cs));
+    LM_CUDA_TRY(cudaStreamWaitEvent(c.stream, c.ev_out, 0));
+  }
+  return LM_OK;
+}
+
+std::string gkey(const char* op, std::initializer_list<long long> v) {
+  std::string k(op);
+  for (long long x : v) k += "," + std::to_string(x);
+  return k;
 }
 
 }  // namespace lm
@@ -183,6 +315,16 @@ int lm_ctx_destroy(lm_ctx* ctx) {
     cudaStreamSynchronize(ctx->c.stream);
     for (int s = 0; s < lm::kWsSlots; ++s)
       if (ctx->c.ws[s]) cudaFree(ctx->c.ws[s]);
+    for (auto& r : ctx->c.recs) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    for (auto e : ctx->c.pool) cudaEventDestroy(e);
+    for (auto& g : ctx->c.gcache)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (ctx->c.side) cudaStreamDestroy(ctx->c.side);
+    if (ctx->c.ev_in) cudaEventDestroy(ctx->c.ev_in);
+    if (ctx->c.ev_out) cudaEventDestroy(ctx->c.ev_out);
     if (ctx->c.d_status) cudaFree(ctx->c.d_status);
     if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
   }
@@ -215,6 +357,39 @@ int lm_ctx_check(lm_ctx* ctx) {
   return guarded(ctx, [&](Ctx& c) {
     int r = lm::read_status(c, nullptr);
     return r < 0 ? r : LM_OK;
+  });
+}
+
+int lm_ctx_profile(lm_ctx* ctx, int enable) {
+  return guarded(ctx, [&](Ctx& c) {
+    c.prof = enable != 0;
+    return LM_OK;
+  });
+}
+
+int lm_ctx_profile_read(lm_ctx* ctx, long long* launches, double* ms, double* flops, double* bytes) {
+  return guarded(ctx, [&](Ctx& c) {
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    long long L[lm::kNumPhases] = {};
+    double M[lm::kNumPhases] = {}, F[lm::kNumPhases] = {}, B[lm::kNumPhases] = {};
+    for (auto& r : c.recs) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, r.a, r.b);
+      L[r.phase] += 1;
+      M[r.phase] += t;
+      F[r.phase] += r.flops;
+      B[r.phase] += r.bytes;
+      c.pool.push_back(r.a);
+      c.pool.push_back(r.b);
+    }
+    c.recs.clear();
+    for (int i = 0; i < lm::kNumPhases; ++i) {
+      if (launches) launches[i] = L[i];
+      if (ms) ms[i] = M[i];
+      if (flops) flops[i] = F[i];
+      if (bytes) bytes[i] = B[i];
+    }
+    return LM_OK;
   });
 }
 
@@ -303,16 +478,16 @@ namespace {
 // Run `fn(A2, lda2)` on an even-stride copy of A when lda is odd or A is
 // misaligned (TMA rows must start on 16 bytes), copying the result back.
 template <typename F>
-int with_aligned(Ctx& c, int n, double* A, long long lda, F&& fn) {
+int with_aligned(Ctx& c, int n, double* A, long long lda, cudaStream_t st, F&& fn) {
   if (!((reinterpret_cast<uintptr_t>(A) & 15) || (lda & 1))) return fn(A, lda);
   const long long lda2 = rup(n, 8);
   void* ws = nullptr;
   LM_TRY(lm::ctx_workspace(c, 0, sizeof(double) * (size_t)n * lda2, &ws));
   double* A2 = static_cast<double*>(ws);
-  LM_TRY(lm::copy2d<double>(A2, lda2, A, lda, n, n, c.stream));
+  LM_TRY(lm::copy2d<double>(A2, lda2, A, lda, n, n, st));
   int r = fn(A2, lda2);
   if (r < 0) return r;
-  LM_TRY(lm::copy2d<double>(A, lda, A2, lda2, n, n, c.stream));
+  LM_TRY(lm::copy2d<double>(A, lda, A2, lda2, n, n, st));
   return r;
 }
 
@@ -334,7 +509,9 @@ int lm_dgetrf(lm_ctx* ctx, int n, double* A, int lda, int* ipiv, int* info) {
       return LM_OK;
     }
     LM_TRY(lm::reset_info(c));
-    LM_TRY(with_aligned(c, n, A, lda, [&](double* A2, long long l2) { return lm::dgetrf(c, n, A2, l2, ipiv, c.stream); }));
+    LM_TRY(lm::run_graphed(c, lm::gkey("getrf", {n, (long long)A, lda, (long long)ipiv}), [&](cudaStream_t s) {
+      return with_aligned(c, n, A, lda, s, [&](double* A2, long long l2) { return lm::dgetrf(c, n, A2, l2, ipiv, s); });
+    }));
     return finish_info(c, info);
   });
 }
@@ -345,17 +522,30 @@ int lm_dgetrs(lm_ctx* ctx, int n, int nrhs, const double* LU, int lda, const int
     if (n < 0 || nrhs < 0 || (n > 0 && nrhs > 0 && (!LU || !ipiv || !B || lda < n || ldb < nrhs)))
       return LM_ERR_ARG;
     if (n == 0 || nrhs == 0) return LM_OK;
-    return lm::dgetrs(c, n, nrhs, LU, lda, ipiv, B, ldb, c.stream);
+    return lm::run_graphed(c, lm::gkey("getrs", {n, nrhs, (long long)LU, lda, (long long)ipiv, (long long)B, ldb}),
+                           [&](cudaStream_t s) { return lm::dgetrs(c, n, nrhs, LU, lda, ipiv, B, ldb, s); });
   });
 }
 
 int lm_dgesv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, double* B, int ldb,
              int* info) {
-  int r = lm_dgetrf(ctx, n, A, lda, ipiv, nullptr);
-  if (r < 0) return r;
-  r = lm_dgetrs(ctx, n, nrhs, A, lda, ipiv, B, ldb);
-  if (r < 0) return r;
-  return guarded(ctx, [&](Ctx& c) { return finish_info(c, info); });
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || (n > 0 && (!A || !ipiv || lda < n || (nrhs > 0 && (!B || ldb < nrhs)))))
+      return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::run_graphed(
+        c, lm::gkey("gesv", {n, nrhs, (long long)A, lda, (long long)ipiv, (long long)B, ldb}), [&](cudaStream_t s) {
+          LM_TRY(with_aligned(c, n, A, lda, s,
+                              [&](double* A2, long long l2) { return lm::dgetrf(c, n, A2, l2, ipiv, s); }));
+          if (nrhs == 0) return LM_OK;
+          return lm::dgetrs(c, n, nrhs, A, lda, ipiv, B, ldb, s);
+        }));
+    return finish_info(c, info);
+  });
 }
 
 int lm_dpotrf(lm_ctx* ctx, int n, double* A, int lda, int* info) {
@@ -366,7 +556,9 @@ int lm_dpotrf(lm_ctx* ctx, int n, double* A, int lda, int* info) {
       return LM_OK;
     }
     LM_TRY(lm::reset_info(c));
-    LM_TRY(with_aligned(c, n, A, lda, [&](double* A2, long long l2) { return lm::dpotrf(c, n, A2, l2, c.stream); }));
+    LM_TRY(lm::run_graphed(c, lm::gkey("potrf", {n, (long long)A, lda}), [&](cudaStream_t s) {
+      return with_aligned(c, n, A, lda, s, [&](double* A2, long long l2) { return lm::dpotrf(c, n, A2, l2, s); });
+    }));
     return finish_info(c, info);
   });
 }
@@ -376,16 +568,29 @@ int lm_dpotrs(lm_ctx* ctx, int n, int nrhs, const double* G, int lda, double* B,
     if (n < 0 || nrhs < 0 || (n > 0 && nrhs > 0 && (!G || !B || lda < n || ldb < nrhs)))
       return LM_ERR_ARG;
     if (n == 0 || nrhs == 0) return LM_OK;
-    return lm::dpotrs(c, n, nrhs, G, lda, B, ldb, c.stream);
+    return lm::run_graphed(c, lm::gkey("potrs", {n, nrhs, (long long)G, lda, (long long)B, ldb}),
+                           [&](cudaStream_t s) { return lm::dpotrs(c, n, nrhs, G, lda, B, ldb, s); });
   });
 }
 
 int lm_dposv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, double* B, int ldb, int* info) {
-  int r = lm_dpotrf(ctx, n, A, lda, nullptr);
-  if (r < 0) return r;
-  r = lm_dpotrs(ctx, n, nrhs, A, lda, B, ldb);
-  if (r < 0) return r;
-  return guarded(ctx, [&](Ctx& c) { return finish_info(c, info); });
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || (n > 0 && (!A || lda < n || (nrhs > 0 && (!B || ldb < nrhs))))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::run_graphed(c, lm::gkey("posv", {n, nrhs, (long long)A, lda, (long long)B, ldb}),
+                           [&](cudaStream_t s) {
+                             LM_TRY(with_aligned(c, n, A, lda, s, [&](double* A2, long long l2) {
+                               return lm::dpotrf(c, n, A2, l2, s);
+                             }));
+                             if (nrhs == 0) return LM_OK;
+                             return lm::dpotrs(c, n, nrhs, A, lda, B, ldb, s);
+                           }));
+    return finish_info(c, info);
+  });
 }
 
 int lm_dresidual(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* X, int ldx,
@@ -466,8 +671,12 @@ int lm_lu_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double
     LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
     LM_TRY(h2d_2d(c, hb.B, hb.ldb, B, nrhs, n, nrhs));
     LM_TRY(lm::reset_info(c));
-    LM_TRY(lm::dgetrf(c, n, hb.A, hb.lda, hb.ipiv, c.stream));
-    if (nrhs > 0) LM_TRY(lm::dgetrs(c, n, nrhs, hb.A, hb.lda, hb.ipiv, hb.B, hb.ldb, c.stream));
+    LM_TRY(lm::run_graphed(c, lm::gkey("lu_host", {n, nrhs, (long long)hb.A, hb.lda, (long long)hb.B, hb.ldb}),
+                           [&](cudaStream_t s) {
+                             LM_TRY(lm::dgetrf(c, n, hb.A, hb.lda, hb.ipiv, s));
+                             if (nrhs == 0) return LM_OK;
+                             return lm::dgetrs(c, n, nrhs, hb.A, hb.lda, hb.ipiv, hb.B, hb.ldb, s);
+                           }));
     LM_TRY(d2h_2d(c, X, nrhs, hb.B, hb.ldb, n, nrhs));
     int inf = 0;
     int r = lm::read_status(c, &inf);
@@ -489,8 +698,12 @@ int lm_chol_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const doub
     LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
     LM_TRY(h2d_2d(c, hb.B, hb.ldb, B, nrhs, n, nrhs));
     LM_TRY(lm::reset_info(c));
-    LM_TRY(lm::dpotrf(c, n, hb.A, hb.lda, c.stream));
-    if (nrhs > 0) LM_TRY(lm::dpotrs(c, n, nrhs, hb.A, hb.lda, hb.B, hb.ldb, c.stream));
+    LM_TRY(lm::run_graphed(c, lm::gkey("chol_host", {n, nrhs, (long long)hb.A, hb.lda, (long long)hb.B, hb.ldb}),
+                           [&](cudaStream_t s) {
+                             LM_TRY(lm::dpotrf(c, n, hb.A, hb.lda, s));
+                             if (nrhs == 0) return LM_OK;
+                             return lm::dpotrs(c, n, nrhs, hb.A, hb.lda, hb.B, hb.ldb, s);
+                           }));
     LM_TRY(d2h_2d(c, X, nrhs, hb.B, hb.ldb, n, nrhs));
     int inf = 0;
     int r = lm::read_status(c, &inf);

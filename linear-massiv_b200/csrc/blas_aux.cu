@@ -21,121 +21,178 @@ void count_launch(int n);
 
 namespace {
 
-// Each thread owns one column and applies the swaps in groups of 8: all rows a
-// group touches are loaded first (independent loads), the swaps are replayed
-// in order on registers, and the touched rows are stored once.
+// Row interchanges as one composed permutation.  The swaps ipiv[k0..k1)
+// (at most kSwapChunk of them) touch at most 2 * kSwapChunk rows.  Thread 0
+// replays them on row indices in shared memory (rows k0..k1-1 in fixed
+// slots, other pivot rows found through a small open-addressing table),
+// giving for every touched row r the row src(r) whose data ends up in it.
+// The CTA then gathers all sources of its 32-column block into shared memory
+// (coalesced along the columns, many independent loads per thread) and
+// scatters them to their rows.
+constexpr int kSwapChunk = 128;
+constexpr int kSwapThreads = 256;
+constexpr int kHash = 512;
+
 template <typename T>
-__global__ void laswp_kernel(T* A, long long lda, int nrows, const int* __restrict__ ipiv, int k0, int k1,
-                             int ca0, int ca1, int cb0, int cb1, int* status) {
-  const int na = ca1 - ca0, nb = cb1 - cb0;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= na + nb) return;
-  const int col = t < na ? ca0 + t : cb0 + (t - na);
-  T* base = A + col;
-  constexpr int G = 8;
-  for (int s0 = k0; s0 < k1; s0 += G) {
-    const int cnt = min(G, k1 - s0);
-    T v[2 * G];
-    int slot_of_piv[G];
-    int extra_row[G];
-    int nextra = 0;
-#pragma unroll
-    for (int q = 0; q < G; ++q)
-      if (q < cnt) v[q] = base[(long long)(s0 + q) * lda];
-#pragma unroll
-    for (int q = 0; q < G; ++q) {
-      if (q < cnt) {
-        int p = __ldg(ipiv + s0 + q);
-        if (p < 0 || p >= nrows) {  // a bad swap list: record it, treat as no swap
-          atomicCAS(status, 0, LM_DEVERR_BOUNDS);
-          p = s0 + q;
-        }
-        int slot = -1;
-        if (p >= s0 && p < s0 + cnt) {
-          slot = p - s0;
-        } else {
-          for (int e = 0; e < nextra; ++e)
-            if (extra_row[e] == p) slot = G + e;
-          if (slot < 0) {
-            extra_row[nextra] = p;
-            slot = G + nextra;
-            v[slot] = base[(long long)p * lda];
-            ++nextra;
-          }
-        }
-        slot_of_piv[q] = slot;
-      }
-    }
-    for (int q = 0; q < cnt; ++q) {
-      const int s = slot_of_piv[q];
-      const T tmp = v[q];
-      v[q] = v[s];
-      v[s] = tmp;
-    }
-#pragma unroll
-    for (int q = 0; q < G; ++q)
-      if (q < cnt) base[(long long)(s0 + q) * lda] = v[q];
-    for (int e = 0; e < nextra; ++e) base[(long long)extra_row[e] * lda] = v[G + e];
+__global__ void __launch_bounds__(kSwapThreads) laswp_kernel(T* A, long long lda, int nrows,
+                                                             const int* __restrict__ ipiv, int k0, int k1, int ca0,
+                                                             int ca1, int cb0, int cb1, int* status) {
+  __shared__ int rows[2 * kSwapChunk];
+  __shared__ int src[2 * kSwapChunk];
+  __shared__ int piv[kSwapChunk];
+  __shared__ int hkey[kHash];
+  __shared__ short hval[kHash];
+  __shared__ int list_r[2 * kSwapChunk];
+  __shared__ int list_s[2 * kSwapChunk];
+  __shared__ int m_sh, mm_sh;
+  extern __shared__ __align__(16) unsigned char sm[];
+  T* stage = reinterpret_cast<T*>(sm);  // [2 * kSwapChunk][32]
+  const int tid = threadIdx.x;
+  const int cnt = k1 - k0;
+  for (int i = tid; i < kHash; i += kSwapThreads) hkey[i] = -1;
+  for (int i = tid; i < cnt; i += kSwapThreads) {
+    rows[i] = k0 + i;
+    src[i] = k0 + i;
+    piv[i] = __ldg(ipiv + k0 + i);
   }
+  if (tid == 0) mm_sh = 0;
+  __syncthreads();
+  if (tid == 0) {
+    int m = cnt;
+    for (int q = 0; q < cnt; ++q) {
+      const int k = k0 + q;
+      const int p = piv[q];
+      if (p < 0 || p >= nrows) {  // a bad swap list: record it, treat as no swap
+        atomicCAS(status, 0, LM_DEVERR_BOUNDS);
+        continue;
+      }
+      if (p == k) continue;
+      int sp;
+      if (p >= k0 && p < k1) {
+        sp = p - k0;
+      } else {
+        unsigned h = ((unsigned)p * 2654435761u) & (kHash - 1);
+        while (hkey[h] != -1 && hkey[h] != p) h = (h + 1) & (kHash - 1);
+        if (hkey[h] == p) {
+          sp = hval[h];
+        } else {
+          hkey[h] = p;
+          hval[h] = (short)m;
+          rows[m] = p;
+          src[m] = p;
+          sp = m++;
+        }
+      }
+      const int t = src[q];
+      src[q] = src[sp];
+      src[sp] = t;
+    }
+    m_sh = m;
+  }
+  __syncthreads();
+  // compact to the rows that actually change
+  for (int i = tid; i < m_sh; i += kSwapThreads)
+    if (src[i] != rows[i]) {
+      const int at = atomicAdd(&mm_sh, 1);
+      list_r[at] = rows[i];
+      list_s[at] = src[i];
+    }
+  __syncthreads();
+  const int mm = mm_sh;
+  const int na = ca1 - ca0, ncols = na + (cb1 - cb0);
+  const int lane = tid & 31, warp = tid >> 5;
+  const int t = blockIdx.x * 32 + lane;
+  const bool active = t < ncols;
+  const int col = t < na ? ca0 + t : cb0 + (t - na);
+#pragma unroll 4
+  for (int i = warp; i < mm; i += kSwapThreads / 32)
+    if (active) stage[i * 32 + lane] = A[(long long)list_s[i] * lda + col];
+  __syncthreads();
+#pragma unroll 4
+  for (int i = warp; i < mm; i += kSwapThreads / 32)
+    if (active) A[(long long)list_r[i] * lda + col] = stage[i * 32 + lane];
 }
 
-// op(Tri) X = B for one w x 64 column block of B per CTA.  The w x w block of
-// Tri and the B block are staged in shared memory; step k finalises x_k and
-// applies it to the rows still to be solved (one barrier per step); the
-// divisions by the diagonal are applied once at the end.
+// op(Tri) X = B for one w x 32 column block of B per CTA (w <= 128).  The
+// triangle of op(Tri) is staged packed in shared memory (w(w+1)/2 entries,
+// so two CTAs fit per SM in FP64) together with the block.  Rows are solved
+// in 16-row blocks: warp 0 solves a diagonal block (lane = column,
+// sequential over its 16 rows), then all warps apply the block to the rows
+// still to be solved (a rank-16 update).  Two barriers per 16 rows.
+__device__ __forceinline__ int tri_idx(bool upper, int w, int i, int k) {
+  return upper ? i * w - (i * (i - 1)) / 2 + (k - i) : (i * (i + 1)) / 2 + k;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) trsm_left_kernel(const T* __restrict__ Tri, long long ldt, int w,
                                                        int lower, int unit, int trans, T* B, long long ldb,
                                                        int ncols) {
   extern __shared__ __align__(16) unsigned char sm[];
-  const int ldts = w + 1;
+  const bool upper_op = (lower == 0) != (trans != 0);
   T* Ts = reinterpret_cast<T*>(sm);
-  T* Bs = Ts + (size_t)w * ldts;  // w x 64, ld 65
-  const int c0 = blockIdx.x * 64;
-  const int nc = min(64, ncols - c0);
+  T* Bs = Ts + ((w * (w + 1) / 2 + 1) & ~1);  // w x 32, ld 33
+  const int c0 = blockIdx.x * 32;
+  const int nc = min(32, ncols - c0);
+#pragma unroll 8
   for (int i = threadIdx.x; i < w * w; i += blockDim.x) {
     const int r = i / w, c = i % w;
-    Ts[r * ldts + c] = Tri[(long long)r * ldt + c];
+    if (lower ? (c <= r) : (c >= r)) {
+      const int oi = trans ? c : r, ok = trans ? r : c;
+      Ts[tri_idx(upper_op, w, oi, ok)] = Tri[(long long)r * ldt + c];
+    }
   }
-  for (int i = threadIdx.x; i < w * 64; i += blockDim.x) {
-    const int r = i / 64, c = i % 64;
-    Bs[r * 65 + c] = (c < nc) ? B[(long long)r * ldb + c0 + c] : T(0);
+#pragma unroll 8
+  for (int i = threadIdx.x; i < w * 32; i += blockDim.x) {
+    const int r = i >> 5, c = i & 31;
+    Bs[r * 33 + c] = (c < nc) ? B[(long long)r * ldb + c0 + c] : T(0);
   }
   __syncthreads();
-  const bool upper_op = (lower == 0) != (trans != 0);
-  const int c = threadIdx.x & 63;
-  const int rg = threadIdx.x >> 6;
-  const int ng = blockDim.x >> 6;
-  for (int step = 0; step < w; ++step) {
-    const int k = upper_op ? (w - 1 - step) : step;
-    T xk = Bs[k * 65 + c];
-    if (!unit) xk = xk / Ts[k * ldts + k];
-    if (!upper_op) {
-      for (int i = k + 1 + ((rg - (k + 1)) % ng + ng) % ng; i < w; i += ng) {
-        const T tik = trans ? Ts[k * ldts + i] : Ts[i * ldts + k];
-        Bs[i * 65 + c] = fma(-tik, xk, Bs[i * 65 + c]);
-      }
-    } else {
-      for (int i = rg; i < k; i += ng) {
-        const T tik = trans ? Ts[k * ldts + i] : Ts[i * ldts + k];
-        Bs[i * 65 + c] = fma(-tik, xk, Bs[i * 65 + c]);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const int nb = (w + 15) / 16;
+  for (int bi = 0; bi < nb; ++bi) {
+    const int b = upper_op ? nb - 1 - bi : bi;
+    const int r0 = b * 16, r1 = min(r0 + 16, w);
+    if (warp == 0) {
+      if (!upper_op) {
+        for (int r = r0; r < r1; ++r) {
+          const T* trow = Ts + tri_idx(false, w, r, 0);
+          T x = Bs[r * 33 + lane];
+          for (int q = r0; q < r; ++q) x = fma(-trow[q], Bs[q * 33 + lane], x);
+          if (!unit) x = x / trow[r];
+          Bs[r * 33 + lane] = x;
+        }
+      } else {
+        for (int r = r1 - 1; r >= r0; --r) {
+          const T* trow = Ts + tri_idx(true, w, r, r) - r;  // trow[q] = op(T)(r, q), q >= r
+          T x = Bs[r * 33 + lane];
+          for (int q = r + 1; q < r1; ++q) x = fma(-trow[q], Bs[q * 33 + lane], x);
+          if (!unit) x = x / trow[r];
+          Bs[r * 33 + lane] = x;
+        }
       }
     }
     __syncthreads();
-  }
-  for (int i = threadIdx.x; i < w * 64; i += blockDim.x) {
-    const int r = i / 64, cc = i % 64;
-    if (cc < nc) {
-      T x = Bs[r * 65 + cc];
-      if (!unit) x = x / Ts[r * ldts + r];
-      B[(long long)r * ldb + c0 + cc] = x;
+    // rank-(r1-r0) update of the unsolved rows
+    const int u0 = upper_op ? 0 : r1, u1 = upper_op ? r0 : w;
+    for (int i = u0 + warp; i < u1; i += nwarps) {
+      const T* trow = upper_op ? Ts + tri_idx(true, w, i, i) - i : Ts + tri_idx(false, w, i, 0);
+      T acc = Bs[i * 33 + lane];
+      for (int q = r0; q < r1; ++q) acc = fma(-trow[q], Bs[q * 33 + lane], acc);
+      Bs[i * 33 + lane] = acc;
     }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < w * 32; i += blockDim.x) {
+    const int r = i >> 5, c = i & 31;
+    if (c < nc) B[(long long)r * ldb + c0 + c] = Bs[r * 33 + c];
   }
 }
 
 template <typename T>
 __global__ void copy2d_kernel(T* dst, long long ldd, const T* src, long long lds, int rows, int cols) {
   const long long total = (long long)rows * cols;
+#pragma unroll 4
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(i / cols), c = (int)(i % cols);
@@ -203,12 +260,25 @@ int grid_for(long long total, int threads, int sms) {
 template <typename T>
 int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int ca0, int ca1, int cb0, int cb1,
           int* status, cudaStream_t st) {
-  const int cols = std::max(0, ca1 - ca0) + std::max(0, cb1 - cb0);
+  ca1 = std::max(ca0, ca1);
+  cb1 = std::max(cb0, cb1);
+  const int cols = (ca1 - ca0) + (cb1 - cb0);
   if (cols == 0 || k1 <= k0) return LM_OK;
-  laswp_kernel<T><<<cdiv(cols, 128), 128, 0, st>>>(A, lda, nrows, ipiv, k0, k1, ca0, std::max(ca0, ca1), cb0,
-                                                   std::max(cb0, cb1), status);
-  count_launch(1);
-  LM_CUDA_TRY(cudaGetLastError());
+  const size_t smem = sizeof(T) * 2 * kSwapChunk * 32;
+  static bool attr_set[kMaxDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev]) {
+    LM_CUDA_TRY(cudaFuncSetAttribute(laswp_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev] = true;
+  }
+  for (int s0 = k0; s0 < k1; s0 += kSwapChunk) {
+    const int s1 = std::min(k1, s0 + kSwapChunk);
+    laswp_kernel<T><<<cdiv(cols, 32), kSwapThreads, smem, st>>>(A, lda, nrows, ipiv, s0, s1, ca0, ca1, cb0, cb1,
+                                                                status);
+    count_launch(1);
+    LM_CUDA_TRY(cudaGetLastError());
+  }
   return LM_OK;
 }
 
@@ -217,16 +287,16 @@ int trsm_left(const T* Tri, long long ldt, int w, bool lower, bool unit, bool tr
               int ncols, cudaStream_t st) {
   if (w <= 0 || ncols <= 0) return LM_OK;
   if (w > 128) return LM_ERR_ARG;
-  const size_t smem = sizeof(T) * ((size_t)w * (w + 1) + (size_t)w * 65);
+  const size_t smem = sizeof(T) * ((size_t)((w * (w + 1) / 2 + 1) & ~1) + (size_t)w * 33);
   static bool attr_set[kMaxDevices] = {};
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(trsm_left_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(T) * (128 * 129 + 128 * 65))));
+                                     (int)(sizeof(T) * (128 * 129 / 2 + 1 + 128 * 33))));
     attr_set[dev] = true;
   }
-  trsm_left_kernel<T><<<cdiv(ncols, 64), 256, smem, st>>>(Tri, ldt, w, lower ? 1 : 0, unit ? 1 : 0,
+  trsm_left_kernel<T><<<cdiv(ncols, 32), 256, smem, st>>>(Tri, ldt, w, lower ? 1 : 0, unit ? 1 : 0,
                                                           trans ? 1 : 0, B, ldb, ncols);
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());

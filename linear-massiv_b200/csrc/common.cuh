@@ -97,6 +97,27 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int* s
   return false;
 }
 
+// Non-suspending variant for latency-critical waits: polls with
+// mbarrier.test_wait (never parks the warp), still bounded by kSpinLimit.
+__device__ __forceinline__ bool mbar_test(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_spin(uint64_t* bar, uint32_t parity, int* status) {
+  for (uint32_t it = 0; it < 4 * kSpinLimit; ++it)
+    if (mbar_test(bar, parity)) return true;
+  atomicCAS(status, 0, LM_DEVERR_TIMEOUT);
+  return false;
+}
+
 // 2D tiled TMA load (no multicast) into this CTA's shared memory, completing
 // on an mbarrier of this CTA.
 __device__ __forceinline__ void tma_load_2d(void* smem_dst, const CUtensorMap* tmap, int x, int y,
@@ -159,6 +180,17 @@ template <>
 __device__ __forceinline__ double dsmem_ld<double>(uint32_t a) { return dsmem_ld_f64(a); }
 template <>
 __device__ __forceinline__ float dsmem_ld<float>(uint32_t a) { return dsmem_ld_f32(a); }
+
+// Asynchronous 16-byte store into (possibly another CTA's) shared memory that
+// completes tx bytes on the destination CTA's mbarrier (both addresses are
+// shared::cluster addresses from dsmem_map).
+__device__ __forceinline__ void st_async_16(uint32_t dst, uint32_t remote_bar, uint32_t a, uint32_t b, uint32_t c,
+                                            uint32_t d) {
+  asm volatile(
+      "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(dst),
+      "r"(a), "r"(b), "r"(c), "r"(d), "r"(remote_bar)
+      : "memory");
+}
 
 // FP64 tensor-core MMA, m16n8k4 (row.col): D = A*B + D.
 __device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {

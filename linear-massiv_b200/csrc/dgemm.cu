@@ -40,18 +40,30 @@ struct GemmArgs {
   double* C;
   long long ldc;
   int lower_only;
+  int prefetch_c;  // TMA-prefetch each C tile into L2 when its main loop starts
   int tiles_m, tiles_n, num_tiles;
   int* status;
 };
 
-template <int BM, int BN>
+__device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* tmap, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
+                   reinterpret_cast<uint64_t>(tmap)),
+               "r"(x), "r"(y)
+               : "memory");
+}
+
+// MINB CTAs share an SM: with two, one CTA's epilogue (C read-modify-write)
+// overlaps the other's DMMA main loop, which matters for the short-k
+// trailing updates of the factorisations.
+template <int BM, int BN, int MINB>
 struct GemmCfg {
   static constexpr int NC = (BM / 64) * (BN / 32);  // consumer warps
   static constexpr int THREADS = (NC + 1) * 32;
   static constexpr int A_BYTES = BM * kBK * 8;
   static constexpr int B_BYTES = BN * kBK * 8;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int STAGES = (200 * 1024) / STAGE_BYTES > 8 ? 8 : (200 * 1024) / STAGE_BYTES;
+  static constexpr int BUDGET = (200 * 1024) / MINB;
+  static constexpr int STAGES = BUDGET / STAGE_BYTES > 8 ? 8 : BUDGET / STAGE_BYTES;
   static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;  // + alignment slack
 };
 
@@ -75,11 +87,11 @@ __device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& tm, i
   }
 }
 
-template <int BM, int BN, bool AT, bool BT>
-__global__ void __launch_bounds__(GemmCfg<BM, BN>::THREADS, 1)
+template <int BM, int BN, bool AT, bool BT, int MINB>
+__global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
     dgemm_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-                      GemmArgs g) {
-  using Cfg = GemmCfg<BM, BN>;
+                      const __grid_constant__ CUtensorMap tmC, GemmArgs g) {
+  using Cfg = GemmCfg<BM, BN, MINB>;
   constexpr int STAGES = Cfg::STAGES;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
@@ -111,6 +123,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN>::THREADS, 1)
       for (int t = blockIdx.x; t < g.num_tiles; t += gridDim.x) {
         int tm, tn;
         tile_coords(g, t, tm, tn);
+        if (g.prefetch_c) tma_prefetch_l2_2d(&tmC, tn * BN, tm * BM);
         for (int kb = 0; kb < KT; ++kb, ++it) {
           const int s = it % STAGES;
           const uint32_t ph = (uint32_t)((it / STAGES) & 1) ^ 1u;
@@ -195,9 +208,35 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN>::THREADS, 1)
     }
 
     // ---------------- epilogue: C = alpha*acc + beta*C ----------------
+    // Per 16-row slice: issue all of its C loads first, then the FMAs and stores.
     const bool vec_ok = ((g.ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(g.C) & 15) == 0);
+    const bool use_beta = g.beta != 0.0;
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi) {
+      double old[2][4][2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int row = tm * BM + wm * 64 + mi * 16 + gq + h * 8;
+        const double* crow = g.C + (long long)row * g.ldc;
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+          const int col = tn * BN + wn * 32 + ni * 8 + 2 * tq;
+          old[h][ni][0] = 0.0;
+          old[h][ni][1] = 0.0;
+          if (use_beta && row < g.m) {
+            const bool in0 = col < g.n && (!g.lower_only || col <= row);
+            const bool in1 = col + 1 < g.n && (!g.lower_only || col + 1 <= row);
+            if (in0 && in1 && vec_ok) {
+              const double2 o = *reinterpret_cast<const double2*>(crow + col);
+              old[h][ni][0] = o.x;
+              old[h][ni][1] = o.y;
+            } else {
+              if (in0) old[h][ni][0] = crow[col];
+              if (in1) old[h][ni][1] = crow[col + 1];
+            }
+          }
+        }
+      }
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int row = tm * BM + wm * 64 + mi * 16 + gq + h * 8;
@@ -206,25 +245,15 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN>::THREADS, 1)
 #pragma unroll
         for (int ni = 0; ni < 4; ++ni) {
           const int col = tn * BN + wn * 32 + ni * 8 + 2 * tq;
-          const double v0 = acc[mi][ni][2 * h], v1 = acc[mi][ni][2 * h + 1];
           const bool in0 = col < g.n && (!g.lower_only || col <= row);
           const bool in1 = col + 1 < g.n && (!g.lower_only || col + 1 <= row);
+          const double r0 = fma(g.alpha, acc[mi][ni][2 * h], use_beta ? g.beta * old[h][ni][0] : 0.0);
+          const double r1 = fma(g.alpha, acc[mi][ni][2 * h + 1], use_beta ? g.beta * old[h][ni][1] : 0.0);
           if (in0 && in1 && vec_ok) {
-            double2* p = reinterpret_cast<double2*>(crow + col);
-            double2 o = make_double2(0.0, 0.0);
-            if (g.beta != 0.0) o = *p;
-            o.x = fma(g.alpha, v0, g.beta != 0.0 ? g.beta * o.x : 0.0);
-            o.y = fma(g.alpha, v1, g.beta != 0.0 ? g.beta * o.y : 0.0);
-            *p = o;
+            *reinterpret_cast<double2*>(crow + col) = make_double2(r0, r1);
           } else {
-            if (in0) {
-              const double old = (g.beta != 0.0) ? g.beta * crow[col] : 0.0;
-              crow[col] = fma(g.alpha, v0, old);
-            }
-            if (in1) {
-              const double old = (g.beta != 0.0) ? g.beta * crow[col + 1] : 0.0;
-              crow[col + 1] = fma(g.alpha, v1, old);
-            }
+            if (in0) crow[col] = r0;
+            if (in1) crow[col + 1] = r1;
           }
         }
       }
@@ -243,11 +272,11 @@ __global__ void scale_kernel(double* C, long long ldc, int m, int n, double beta
   }
 }
 
-template <int BM, int BN, bool AT, bool BT>
+template <int BM, int BN, bool AT, bool BT, int MINB>
 int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
-  using Cfg = GemmCfg<BM, BN>;
+  using Cfg = GemmCfg<BM, BN, MINB>;
   static bool attr_set[kMaxDevices] = {};  // per instantiation and device, set under the API lock
-  auto kern = dgemm_dmma_kernel<BM, BN, AT, BT>;
+  auto kern = dgemm_dmma_kernel<BM, BN, AT, BT, MINB>;
   const int dev = ctx_device(ctx);
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
@@ -266,7 +295,15 @@ int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
   else
     LM_TRY(make_tmap_2d(&tmB, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.B, d.n, d.k, d.ldb, 16, kBK,
                         CU_TENSOR_MAP_SWIZZLE_128B));
+  CUtensorMap tmC;
+  const bool c_ok = d.beta != 0.0 && !(reinterpret_cast<uintptr_t>(d.C) & 15) && !(d.ldc & 1);
+  if (c_ok)
+    LM_TRY(make_tmap_2d(&tmC, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.C, d.n, d.m, d.ldc, BN, BM,
+                        CU_TENSOR_MAP_SWIZZLE_NONE));
+  else
+    tmC = tmA;  // unused
   GemmArgs g;
+  g.prefetch_c = c_ok ? 1 : 0;
   g.m = d.m; g.n = d.n; g.k = d.k;
   g.alpha = d.alpha; g.beta = d.beta;
   g.C = d.C; g.ldc = d.ldc;
@@ -275,8 +312,8 @@ int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
   g.tiles_n = cdiv(d.n, BN);
   g.num_tiles = d.lower_only ? g.tiles_m * (g.tiles_m + 1) / 2 : g.tiles_m * g.tiles_n;
   g.status = ctx_status(ctx);
-  int grid = std::min(g.num_tiles, d.max_ctas > 0 ? d.max_ctas : ctx_num_sms(ctx));
-  kern<<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(tmA, tmB, g);
+  int grid = std::min(g.num_tiles, d.max_ctas > 0 ? d.max_ctas : MINB * ctx_num_sms(ctx));
+  kern<<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(tmA, tmB, tmC, g);
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;
@@ -302,15 +339,21 @@ int dgemm(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
       (d.lda & 1) || (d.ldb & 1))
     return LM_ERR_UNSUPPORTED;
   if (d.a_trans && d.b_trans) return LM_ERR_UNSUPPORTED;
-  const bool narrow = d.n <= 64 && !d.lower_only;
+  // Short k (the factorisations' trailing updates): 128 x 64 tiles, two CTAs
+  // per SM.  Long k: 128 x 128 tiles, one CTA per SM, deeper pipeline.
+  const double flops = d.lower_only ? (double)d.m * (d.m + 1) * d.k : 2.0 * d.m * d.n * d.k;
+  const double bytes = 8.0 * ((double)d.m * d.k + (double)d.k * d.n +
+                              (d.beta != 0.0 ? 2.0 : 1.0) * (d.lower_only ? 0.5 : 1.0) * d.m * d.n);
+  Prof prof(ctx, kPhaseGemm, flops, bytes, st);
+  const bool narrow = (d.n <= 64 || d.k <= 256) && !d.lower_only;
   if (d.a_trans)
-    return narrow ? launch_dmma<128, 64, true, false>(ctx, d, st)
-                  : launch_dmma<128, 128, true, false>(ctx, d, st);
+    return narrow ? launch_dmma<128, 64, true, false, 2>(ctx, d, st)
+                  : launch_dmma<128, 128, true, false, 1>(ctx, d, st);
   if (d.b_trans)
-    return narrow ? launch_dmma<128, 64, false, true>(ctx, d, st)
-                  : launch_dmma<128, 128, false, true>(ctx, d, st);
-  return narrow ? launch_dmma<128, 64, false, false>(ctx, d, st)
-                : launch_dmma<128, 128, false, false>(ctx, d, st);
+    return narrow ? launch_dmma<128, 64, false, true, 2>(ctx, d, st)
+                  : launch_dmma<128, 128, false, true, 1>(ctx, d, st);
+  return narrow ? launch_dmma<128, 64, false, false, 2>(ctx, d, st)
+                : launch_dmma<128, 128, false, false, 1>(ctx, d, st);
 }
 
 }  // namespace lm

@@ -26,19 +26,26 @@ namespace {
 
 constexpr int kNB = 128;
 
-int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int* ipiv, cudaStream_t st) {
+int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv,
+                    cudaStream_t st) {
   const int R = n - c0;
   const int wmax = panel_leaf_max_width_for(c, R);
   if (wmax <= 0) return LM_ERR_UNSUPPORTED;
-  if (w <= wmax) return panel_leaf<double>(c, A, lda, n, c0, w, ipiv, st);
+  if (w <= wmax) {
+    // the leaf also swaps the rest of the panel [pc0, pc0 + pw)
+    Prof p(c, kPhasePanel, (double)R * w * w, 16.0 * R * w, st);
+    return panel_leaf<double>(c, A, lda, n, c0, w, pc0, pw, ipiv, st);
+  }
   // Split so that column offsets stay multiples of 4 (16-byte TMA alignment).
   int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
   if (w1 >= w) w1 = w - 4;
   const int w2 = w - w1;
-  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, ipiv, st));
-  LM_TRY(laswp<double>(A, lda, n, ipiv, c0, c0 + w1, c0 + w1, c0 + w, 0, 0, ctx_status(c), st));
+  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, st));
   double* A11 = A + (long long)c0 * lda + c0;
-  LM_TRY(trsm_left<double>(A11, lda, w1, true, true, false, A11 + w1, lda, w2, st));
+  {
+    Prof p(c, kPhaseTrsm, (double)w1 * w1 * w2, 8.0 * ((double)w1 * w1 / 2 + 2.0 * w1 * w2), st);
+    LM_TRY(trsm_left<double>(A11, lda, w1, true, true, false, A11 + w1, lda, w2, st));
+  }
   GemmDesc d;
   d.m = R - w1; d.n = w2; d.k = w1;
   d.alpha = -1.0; d.beta = 1.0;
@@ -46,9 +53,7 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int*
   d.B = A11 + w1; d.ldb = lda;
   d.C = A11 + (long long)w1 * lda + w1; d.ldc = lda;
   LM_TRY(dgemm(c, d, st));
-  LM_TRY(getrf_panel_rec(c, A, lda, n, c0 + w1, w2, ipiv, st));
-  LM_TRY(laswp<double>(A, lda, n, ipiv, c0 + w1, c0 + w, c0, c0 + w1, 0, 0, ctx_status(c), st));
-  return LM_OK;
+  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, st);
 }
 
 }  // namespace
@@ -56,12 +61,19 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int*
 int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) {
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
-    LM_TRY(getrf_panel_rec(c, A, lda, n, k0, w, ipiv, st));
+    LM_TRY(getrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, st));
     // this panel's interchanges on the columns left and right of it
-    LM_TRY(laswp<double>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st));
+    {
+      Prof p(c, kPhaseSwap, 0.0, 32.0 * w * (n - w), st);
+      LM_TRY(laswp<double>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st));
+    }
     if (k0 + w < n) {
       double* A11 = A + (long long)k0 * lda + k0;
-      LM_TRY(trsm_left<double>(A11, lda, w, true, true, false, A11 + w, lda, n - k0 - w, st));
+      {
+        const double nc = n - k0 - w;
+        Prof p(c, kPhaseTrsm, (double)w * w * nc, 8.0 * ((double)w * w / 2 + 2.0 * w * nc), st);
+        LM_TRY(trsm_left<double>(A11, lda, w, true, true, false, A11 + w, lda, n - k0 - w, st));
+      }
       GemmDesc d;
       d.m = n - k0 - w; d.n = n - k0 - w; d.k = w;
       d.alpha = -1.0; d.beta = 1.0;
@@ -79,16 +91,25 @@ int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st) {
     const int w = std::min(kNB, n - j0);
     const int R = n - j0 - w;
     double* A11 = A + (long long)j0 * lda + j0;
-    LM_TRY(potrf_block<double>(c, A11, lda, w, j0, st));
+    {
+      Prof p(c, kPhasePanel, (double)w * w * w / 3.0, 8.0 * w * w, st);
+      LM_TRY(potrf_block<double>(c, A11, lda, w, j0, st));
+    }
     if (R > 0) {
       void* ws = nullptr;
       LM_TRY(ctx_workspace(c, 1, sizeof(double) * ((size_t)kNB * kNB + (size_t)R * kNB), &ws));
       double* Linv = static_cast<double*>(ws);
       double* W21 = Linv + (size_t)kNB * kNB;
       double* A21 = A11 + (long long)w * lda;
-      LM_TRY(set_identity<double>(Linv, kNB, w, w, st));
-      LM_TRY(trsm_left<double>(A11, lda, w, true, false, false, Linv, kNB, w, st));
-      LM_TRY(copy2d<double>(W21, kNB, A21, lda, R, w, st));
+      {
+        Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 24.0 * w * w, st);
+        LM_TRY(set_identity<double>(Linv, kNB, w, w, st));
+        LM_TRY(trsm_left<double>(A11, lda, w, true, false, false, Linv, kNB, w, st));
+      }
+      {
+        Prof p(c, kPhaseOther, 0.0, 16.0 * R * w, st);
+        LM_TRY(copy2d<double>(W21, kNB, A21, lda, R, w, st));
+      }
       GemmDesc t;  // L21 = A21 * L11^-T
       t.m = R; t.n = w; t.k = w; t.alpha = 1.0; t.beta = 0.0;
       t.A = W21; t.lda = kNB; t.B = Linv; t.ldb = kNB; t.b_trans = true;
@@ -146,7 +167,10 @@ int forward_blocked(Ctx& c, int n, int nrhs, const double* M, long long ldm, boo
   for (int i0 = 0; i0 < n; i0 += kNB) {
     const int w = std::min(kNB, n - i0);
     const double* Mii = M + (long long)i0 * ldm + i0;
-    LM_TRY(trsm_left<double>(Mii, ldm, w, true, unit, false, X + (long long)i0 * ldx, ldx, nrhs, st));
+    {
+      Prof p(c, kPhaseTrsm, (double)w * w * nrhs, 8.0 * ((double)w * w / 2 + 2.0 * w * nrhs), st);
+      LM_TRY(trsm_left<double>(Mii, ldm, w, true, unit, false, X + (long long)i0 * ldx, ldx, nrhs, st));
+    }
     if (i0 + w < n) {
       GemmDesc d;
       d.m = n - i0 - w; d.n = nrhs; d.k = w; d.alpha = -1.0; d.beta = 1.0;
@@ -166,15 +190,21 @@ int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* 
   SolveBufs sb;
   LM_TRY(solve_bufs(c, n, nrhs, LU, lda, B, ldb, sb, st));
   // P b (applyPivotsForward, LU.hs:493-507)
-  LM_TRY(laswp<double>(sb.X, sb.ldx, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+  {
+    Prof p(c, kPhaseSwap, 0.0, 32.0 * n * nrhs, st);
+    LM_TRY(laswp<double>(sb.X, sb.ldx, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+  }
   LM_TRY(forward_blocked(c, n, nrhs, sb.M, sb.ldm, true, sb.X, sb.ldx, st));
   const int nblk = (n + kNB - 1) / kNB;
   for (int b = nblk - 1; b >= 0; --b) {
     const int i0 = b * kNB;
     const int w = std::min(kNB, n - i0);
     const double* Uii = sb.M + (long long)i0 * sb.ldm + i0;
-    LM_TRY(trsm_left<double>(Uii, sb.ldm, w, false, false, false, sb.X + (long long)i0 * sb.ldx, sb.ldx, nrhs,
-                             st));
+    {
+      Prof p(c, kPhaseTrsm, (double)w * w * nrhs, 8.0 * ((double)w * w / 2 + 2.0 * w * nrhs), st);
+      LM_TRY(trsm_left<double>(Uii, sb.ldm, w, false, false, false, sb.X + (long long)i0 * sb.ldx, sb.ldx, nrhs,
+                               st));
+    }
     if (i0 > 0) {
       GemmDesc d;
       d.m = i0; d.n = nrhs; d.k = w; d.alpha = -1.0; d.beta = 1.0;
@@ -199,8 +229,11 @@ int dpotrs(Ctx& c, int n, int nrhs, const double* G, long long lda, double* B, l
     const int i0 = b * kNB;
     const int w = std::min(kNB, n - i0);
     const double* Gii = sb.M + (long long)i0 * sb.ldm + i0;
-    LM_TRY(trsm_left<double>(Gii, sb.ldm, w, true, false, true, sb.X + (long long)i0 * sb.ldx, sb.ldx, nrhs,
-                             st));
+    {
+      Prof p(c, kPhaseTrsm, (double)w * w * nrhs, 8.0 * ((double)w * w / 2 + 2.0 * w * nrhs), st);
+      LM_TRY(trsm_left<double>(Gii, sb.ldm, w, true, false, true, sb.X + (long long)i0 * sb.ldx, sb.ldx, nrhs,
+                               st));
+    }
     if (i0 > 0) {
       GemmDesc d;
       d.m = i0; d.n = nrhs; d.k = w; d.alpha = -1.0; d.beta = 1.0;

@@ -20,6 +20,19 @@ int ctx_device(Ctx& c);
 constexpr int kWsSlots = 4;
 int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr);
 
+// Per-phase CUDA-event tracing (enabled by lm_ctx_profile).  A Prof scope
+// brackets the kernels launched inside it with events on stream `st`.
+enum Phase { kPhaseGemm = 0, kPhasePanel = 1, kPhaseSwap = 2, kPhaseTrsm = 3, kPhaseOther = 4, kNumPhases = 5 };
+struct Prof {
+  Prof(Ctx& c, int phase, double flops, double bytes, cudaStream_t st);
+  ~Prof();
+  Ctx& c;
+  int phase;
+  double flops, bytes;
+  cudaStream_t st;
+  cudaEvent_t a = nullptr;
+};
+
 // TMA descriptor for a row-major 2D view: `inner` elements per row (contiguous),
 // `outer` rows, row stride `ld` elements; box of box_inner x box_outer.
 int make_tmap_2d(CUtensorMap* tm, CUtensorMapDataType dt, int elem_bytes, const void* base,
@@ -83,9 +96,11 @@ int dpotrs(Ctx& c, int n, int nrhs, const double* G, long long lda, double* B, l
 
 // Panel factorisation kernels (panel.cu): LU of rows [c0, n) x columns
 // [c0, c0 + w) in place, w <= 32, recording ipiv[c0 .. c0 + w) (global rows)
-// and the first zero pivot in status[1].
+// and the first zero pivot in status[1].  The leaf's row interchanges are
+// also applied to the other columns of the enclosing panel [pc0, pc0 + pw)
+// (pw <= 128); columns outside it are left to the caller.
 template <typename T>
-int panel_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int* ipiv, cudaStream_t st);
+int panel_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv, cudaStream_t st);
 int panel_leaf_max_width_for(Ctx& c, int rows);  // widest leaf one cluster holds for `rows`
 
 // Cholesky of a w x w diagonal block (w <= 128) in place, lower triangle;

@@ -31,15 +31,6 @@ namespace {
 constexpr int kLeafThreads = 512;
 constexpr int kLeafRowsTimesW = 16384;  // rows per CTA * leaf width (128 KB of FP64)
 
-template <typename T, int W>
-struct alignas(16) Mailbox {
-  T val;
-  int idx;
-  int jnan;
-  T cand[W];
-  T rowj[W];
-};
-
 template <typename T>
 __device__ __forceinline__ bool better(T v1, int i1, T v2, int i2) {
   return v1 > v2 || (v1 == v2 && i1 < i2);
@@ -51,34 +42,65 @@ __device__ __forceinline__ T absval(T x) {
   return (a != a) ? T(-1) : a;  // NaN never wins the scan
 }
 
+// One CTA's per-column message, pushed into every CTA of the cluster:
+//   [0] |a| of its best candidate (or -1), [1] that row (relative to c0, as T),
+//   [2] 1 if it owns row j and a_jj is NaN, [3] unused,
+//   [4, 4 + W) the candidate row, [4 + W, 4 + 2W) row j (from its owner).
 template <typename T, int W>
-struct LeafSmem {
-  static constexpr size_t mb_off = 0;
-  static constexpr size_t mb_bytes = 2 * sizeof(Mailbox<T, W>);
-  static constexpr size_t cand_off = (mb_off + mb_bytes + 15) / 16 * 16;
-  static constexpr size_t rowj_off = cand_off + 16 * W * sizeof(T);
-  static constexpr size_t cval_off = rowj_off + W * sizeof(T);
-  static constexpr size_t cidx_off = cval_off + 16 * sizeof(T);
-  static constexpr size_t misc_off = cidx_off + 16 * sizeof(int);
-  static constexpr size_t wval_off = (misc_off + 4 * sizeof(int) + 15) / 16 * 16;
-  static constexpr size_t widx_off = wval_off + 16 * sizeof(T);
-  static constexpr size_t p_off = (widx_off + 16 * sizeof(int) + 15) / 16 * 16;
-  static size_t bytes(int rpc) { return p_off + (size_t)W * (rpc + 1) * sizeof(T); }
+struct LeafMsg {
+  static constexpr int N = 4 + 2 * W;                      // elements
+  static constexpr int BYTES = N * (int)sizeof(T);         // multiple of 16
+  static constexpr int CHUNKS = BYTES / 16;                 // 16-byte st.async pieces
+  static constexpr int PER_CHUNK = 16 / (int)sizeof(T);
+  static_assert(BYTES % 16 == 0, "message must be a whole number of 16-byte chunks");
 };
 
 template <typename T, int W>
+struct LeafSmem {
+  using M = LeafMsg<T, W>;
+  static constexpr size_t recv_off = 0;                                   // T[2][16][M::N]
+  static constexpr size_t recv_bytes = 2 * 16 * (size_t)M::BYTES;
+  static constexpr size_t bar_off = recv_off + recv_bytes;                // uint64_t[2]
+  static constexpr size_t wval_off = bar_off + 16;                        // T[16]
+  static constexpr size_t widx_off = wval_off + 16 * sizeof(T);           // int[16]
+  static constexpr size_t hist_off = widx_off + 16 * sizeof(int);         // int[W] pivot rows
+  static constexpr size_t trow_off = hist_off + W * sizeof(int);          // int[2W] touched rows
+  static constexpr size_t tsrc_off = trow_off + 2 * W * sizeof(int);      // int[2W] their sources
+  static constexpr size_t tm_off = tsrc_off + 2 * W * sizeof(int);        // int touched count
+  static constexpr size_t p_off = (tm_off + sizeof(int) + 15) / 16 * 16;
+  // Swap staging for the other panel columns: 2W rows x up to 128 columns, split over the cluster.
+  static size_t stage_elems(int C) { return (size_t)(2 * W * 128 + C - 1) / C; }
+  static size_t bytes(int rpc, int C) {
+    return p_off + (size_t)W * (rpc + 1) * sizeof(T) + stage_elems(C) * sizeof(T);
+  }
+};
+
+template <typename T, int W>
+__device__ __forceinline__ T msg_elem(int e, const T* P, int ldp, int crow, int jrow, T val, int idx, int jnan) {
+  // element e of this CTA's message (crow/jrow: slab rows of the candidate / row j, -1 if none)
+  if (e == 0) return val;
+  if (e == 1) return T(idx);
+  if (e == 2) return T(jnan);
+  if (e == 3) return T(0);
+  if (e < 4 + W) return crow >= 0 ? P[(e - 4) * ldp + crow] : T(0);
+  return jrow >= 0 ? P[(e - 4 - W) * ldp + jrow] : T(0);
+}
+
+template <typename T, int W>
 __global__ void __launch_bounds__(kLeafThreads, 1)
-    panel_leaf_kernel(T* A, long long lda, int n, int c0, int w, int rpc, int* ipiv, int* status) {
+    panel_leaf_kernel(T* A, long long lda, int n, int c0, int w, int rpc, int pc0, int pw, int* ipiv,
+                      int* status) {
   using L = LeafSmem<T, W>;
+  using M = LeafMsg<T, W>;
   extern __shared__ __align__(16) unsigned char sm[];
-  Mailbox<T, W>* mb = reinterpret_cast<Mailbox<T, W>*>(sm + L::mb_off);
-  T* cand_all = reinterpret_cast<T*>(sm + L::cand_off);
-  T* rowj_st = reinterpret_cast<T*>(sm + L::rowj_off);
-  T* cval = reinterpret_cast<T*>(sm + L::cval_off);
-  int* cidx = reinterpret_cast<int*>(sm + L::cidx_off);
-  int* misc = reinterpret_cast<int*>(sm + L::misc_off);
+  T* recv = reinterpret_cast<T*>(sm + L::recv_off);
+  uint64_t* rbar = reinterpret_cast<uint64_t*>(sm + L::bar_off);
   T* wval = reinterpret_cast<T*>(sm + L::wval_off);
   int* widx = reinterpret_cast<int*>(sm + L::widx_off);
+  int* hist = reinterpret_cast<int*>(sm + L::hist_off);
+  int* trow = reinterpret_cast<int*>(sm + L::trow_off);
+  int* tsrc = reinterpret_cast<int*>(sm + L::tsrc_off);
+  int* tm = reinterpret_cast<int*>(sm + L::tm_off);
   T* P = reinterpret_cast<T*>(sm + L::p_off);
   const int ldp = rpc + 1;
 
@@ -91,12 +113,23 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   const int rcnt = max(0, min(rpc, R - rbeg));
   constexpr int RPT = (kLeafRowsTimesW / W + kLeafThreads - 1) / kLeafThreads;  // rows per thread
 
-  // Load this CTA's slab, column-major: P[c * ldp + r].
-  for (int i = tid; i < rcnt * W; i += kLeafThreads) {
-    const int r = i / W, c = i % W;
-    P[c * ldp + r] = (c < w) ? A[(long long)(c0 + rbeg + r) * lda + c0 + c] : T(0);
+  if (tid == 0) {
+    mbar_init(&rbar[0], 1);
+    mbar_init(&rbar[1], 1);
+    fence_barrier_init();
   }
-  __syncthreads();
+  // Load this CTA's slab, column-major: P[c * ldp + r].  Unrolled so each
+  // thread keeps several independent loads in flight.
+  {
+    const int total = rcnt * W;
+#pragma unroll 8
+    for (int i = tid; i < total; i += kLeafThreads) {
+      const int r = i / W, c = i % W;
+      P[c * ldp + r] = (c < w) ? A[(long long)(c0 + rbeg + r) * lda + c0 + c] : T(0);
+    }
+  }
+  // every CTA's barriers exist before anyone pushes into them
+  cluster_sync_all();
 
   // Local argmax of column 0.
   T bv = T(-1);
@@ -110,8 +143,11 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     }
   }
 
+  bool timed_out = false;
   for (int j = 0; j < w; ++j) {
-    // ---- CTA-level reduction of (bv, bi) ----
+    const int par = j & 1;
+    if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)(C * M::BYTES));
+    // ---- CTA-level argmax: warp shuffles, one barrier, every warp reduces ----
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -120,8 +156,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     }
     if (lane == 0) { wval[warp] = bv; widx[warp] = bi; }
     __syncthreads();
-    Mailbox<T, W>& m = mb[j & 1];
-    if (warp == 0) {
+    if (warp < C) {  // warp d pushes this CTA's message into CTA d
       T v = lane < kLeafThreads / 32 ? wval[lane] : T(-1);
       int i = lane < kLeafThreads / 32 ? widx[lane] : INT_MAX;
 #pragma unroll
@@ -130,52 +165,62 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
         const int oi = __shfl_xor_sync(0xffffffffu, i, o);
         if (better(ov, oi, v, i)) { v = ov; i = oi; }
       }
-      if (lane == 0) { m.val = v; m.idx = i; }
-      if (i != INT_MAX && lane < W) m.cand[lane] = P[lane * ldp + (i - rbeg)];
-      if (j >= rbeg && j < rbeg + rcnt) {
-        if (lane < W) m.rowj[lane] = P[lane * ldp + (j - rbeg)];
-        if (lane == 0) {
-          const T d = P[j * ldp + (j - rbeg)];
-          m.jnan = (d != d) ? 1 : 0;
+      const int crow = (i != INT_MAX) ? i - rbeg : -1;
+      const bool own_j = j >= rbeg && j < rbeg + rcnt;
+      const int jrow = own_j ? j - rbeg : -1;
+      int jnan = 0;
+      if (own_j) {
+        const T d = P[j * ldp + jrow];
+        jnan = (d != d) ? 1 : 0;
+      }
+      T* slot = recv + ((size_t)par * 16 + q) * M::N;  // my slot in every CTA's receive area
+      const uint32_t dst_base = dsmem_map(slot, warp);
+      const uint32_t dst_bar = dsmem_map(&rbar[par], warp);
+      for (int ch = lane; ch < M::CHUNKS; ch += 32) {
+        uint32_t wds[4];
+#pragma unroll
+        for (int e = 0; e < M::PER_CHUNK; ++e) {
+          const T x = msg_elem<T, W>(ch * M::PER_CHUNK + e, P, ldp, crow, jrow, v, i == INT_MAX ? -1 : i, jnan);
+          if constexpr (sizeof(T) == 8) {
+            const unsigned long long u = (unsigned long long)__double_as_longlong((double)x);
+            wds[2 * e] = (uint32_t)u;
+            wds[2 * e + 1] = (uint32_t)(u >> 32);
+          } else {
+            wds[e] = __float_as_uint((float)x);
+          }
         }
+        st_async_16(dst_base + ch * 16, dst_bar, wds[0], wds[1], wds[2], wds[3]);
       }
     }
-    cluster_sync_all();
+    // ---- wait for all C messages of this column ----
+    if (!timed_out && !mbar_wait_spin(&rbar[par], (uint32_t)((j >> 1) & 1), status)) timed_out = true;
 
-    // ---- gather every CTA's candidate over distributed shared memory ----
+    const T* rc = recv + (size_t)par * 16 * M::N;
+    T v = lane < C ? rc[lane * M::N + 0] : T(-1);
+    int i = lane < C ? (int)rc[lane * M::N + 1] : INT_MAX;
+    if (i < 0) i = INT_MAX;
+    int qw = lane;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const T ov = __shfl_xor_sync(0xffffffffu, v, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, i, o);
+      const int oq = __shfl_xor_sync(0xffffffffu, qw, o);
+      if (better(ov, oi, v, i)) { v = ov; i = oi; qw = oq; }
+    }
     const int owner_j = j / rpc;
-    // items: [0, C) values+rows, [C, C + C*W) candidate rows, then row j, then jnan
-    for (int it = tid; it < C + C * W + W + 1; it += kLeafThreads) {
-      if (it < C) {
-        cval[it] = dsmem_ld<T>(dsmem_map(&m.val, it));
-        cidx[it] = dsmem_ld_s32(dsmem_map(&m.idx, it));
-      } else if (it < C + C * W) {
-        const int src = (it - C) / W, e = (it - C) % W;
-        cand_all[src * W + e] = dsmem_ld<T>(dsmem_map(&m.cand[e], src));
-      } else if (it < C + C * W + W) {
-        const int e = it - (C + C * W);
-        rowj_st[e] = dsmem_ld<T>(dsmem_map(&m.rowj[e], owner_j));
-      } else {
-        misc[0] = dsmem_ld_s32(dsmem_map(&m.jnan, owner_j));
-      }
-    }
-    __syncthreads();
-
-    int qw = 0;
-    T vb = cval[0];
-    int ib = cidx[0];
-    for (int s = 1; s < C; ++s)
-      if (better(cval[s], cidx[s], vb, ib)) { vb = cval[s]; ib = cidx[s]; qw = s; }
+    const T* jmsg = rc + owner_j * M::N;
     int p;
     const T* prow;
-    if (misc[0]) {
+    if (jmsg[2] != T(0) || i == INT_MAX || qw >= C) {
       p = j;
-      prow = rowj_st;
+      prow = jmsg + 4 + W;
     } else {
-      p = ib;
-      prow = cand_all + qw * W;
+      p = i;
+      prow = rc + qw * M::N + 4;
     }
+    const T* rowj = jmsg + 4 + W;
     const T piv = prow[j];
+    if (tid == 0) hist[j] = p;
     if (q == 0 && tid == 0) {
       ipiv[c0 + j] = c0 + p;
       if (piv == T(0)) atomicCAS(status + 1, 0, c0 + j + 1);
@@ -194,7 +239,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
           for (int c = 0; c < W; ++c) P[c * ldp + r] = prow[c];
         } else if (gr == p) {
 #pragma unroll
-          for (int c = 0; c < W; ++c) P[c * ldp + r] = rowj_st[c];
+          for (int c = 0; c < W; ++c) P[c * ldp + r] = rowj[c];
         }
         if (gr > j) {
           const T mult = P[j * ldp + r] / piv;
@@ -203,37 +248,83 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
           for (int c = 1; c < W; ++c)
             if (c > j && c < w) P[c * ldp + r] = fma(-mult, prow[c], P[c * ldp + r]);
           if (j + 1 < w) {
-            const T v = absval(P[(j + 1) * ldp + r]);
-            if (better(v, gr, bv, bi)) { bv = v; bi = gr; }
+            const T a1 = absval(P[(j + 1) * ldp + r]);
+            if (better(a1, gr, bv, bi)) { bv = a1; bi = gr; }
           }
         }
       }
     }
+    // the receive slot of this parity is reused two columns later; the
+    // barrier at the top of the next column orders these reads before any
+    // warp of this CTA pushes again, and senders cannot run two columns ahead.
   }
-  // Nobody may leave while others can still read its mailbox.
+  // Nobody may leave while others can still write into it or read from it.
   cluster_sync_all();
-  __syncthreads();
-  for (int i = tid; i < rcnt * W; i += kLeafThreads) {
-    const int r = i / W, c = i % W;
-    if (c < w) A[(long long)(c0 + rbeg + r) * lda + c0 + c] = P[c * ldp + r];
+  {
+    const int total = rcnt * W;
+#pragma unroll 8
+    for (int i = tid; i < total; i += kLeafThreads) {
+      const int r = i / W, c = i % W;
+      if (c < w) A[(long long)(c0 + rbeg + r) * lda + c0 + c] = P[c * ldp + r];
+    }
+  }
+  // This leaf's interchanges on the other columns of the enclosing panel
+  // [pc0, pc0 + pw): compose them (rows relative to c0), gather every touched
+  // row's source over the cluster, barrier, scatter.
+  const int ocols = pw - w;
+  if (ocols > 0) {
+    if (tid == 0) {
+      int m = w;
+      for (int ii = 0; ii < w; ++ii) { trow[ii] = ii; tsrc[ii] = ii; }
+      for (int ii = 0; ii < w; ++ii) {
+        const int pr = hist[ii];
+        if (pr == ii) continue;
+        int sp = -1;
+        if (pr < w) sp = pr;
+        for (int e = w; e < m && sp < 0; ++e)
+          if (trow[e] == pr) sp = e;
+        if (sp < 0) { trow[m] = pr; tsrc[m] = pr; sp = m++; }
+        const int t = tsrc[ii]; tsrc[ii] = tsrc[sp]; tsrc[sp] = t;
+      }
+      *tm = m;
+    }
+    __syncthreads();
+    const int m = *tm;
+    T* stage = P + (size_t)W * ldp;
+    const long long total = (long long)m * ocols;
+    const long long chunk = (total + C - 1) / C;
+    const long long e0 = q * chunk, e1 = min(total, e0 + chunk);
+    const int left = c0 - pc0;  // other columns: [pc0, c0) then [c0 + w, pc0 + pw)
+#pragma unroll 4
+    for (long long e = e0 + tid; e < e1; e += kLeafThreads) {
+      const int ii = (int)(e / ocols), oc = (int)(e % ocols);
+      const int col = oc < left ? pc0 + oc : c0 + w + (oc - left);
+      if (tsrc[ii] != trow[ii]) stage[e - e0] = A[(long long)(c0 + tsrc[ii]) * lda + col];
+    }
+    cluster_sync_all();
+    for (long long e = e0 + tid; e < e1; e += kLeafThreads) {
+      const int ii = (int)(e / ocols), oc = (int)(e % ocols);
+      const int col = oc < left ? pc0 + oc : c0 + w + (oc - left);
+      if (tsrc[ii] != trow[ii]) A[(long long)(c0 + trow[ii]) * lda + col] = stage[e - e0];
+    }
   }
 }
 
 int g_max_cluster[kMaxDevices] = {};
 
 template <typename T, int W>
-int launch_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int* ipiv, cudaStream_t st) {
+int launch_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv, cudaStream_t st) {
   const int R = n - c0;
   const int rpc_max = kLeafRowsTimesW / W;
   const int C = cdiv(R, rpc_max);
   const int rpc = cdiv(R, C);
-  const size_t smem = LeafSmem<T, W>::bytes(rpc);
+  const size_t smem = LeafSmem<T, W>::bytes(rpc, C);
   auto kern = panel_leaf_kernel<T, W>;
   static bool attr_set[kMaxDevices] = {};
   const int dev = ctx_device(c);
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)LeafSmem<T, W>::bytes(rpc_max)));
+                                     (int)LeafSmem<T, W>::bytes(rpc_max, 1)));
     LM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     attr_set[dev] = true;
   }
@@ -249,7 +340,7 @@ int launch_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int* ipiv, cu
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, A, lda, n, c0, w, rpc, ipiv, ctx_status(c)));
+  LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, kern, A, lda, n, c0, w, rpc, pc0, pw, ipiv, ctx_status(c)));
   count_launch(1);
   return LM_OK;
 }
@@ -261,12 +352,12 @@ int max_cluster(Ctx& c) {
   int best = 8;
   auto kern = panel_leaf_kernel<double, 16>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)LeafSmem<double, 16>::bytes(kLeafRowsTimesW / 16)) == cudaSuccess &&
+                           (int)LeafSmem<double, 16>::bytes(kLeafRowsTimesW / 16, 1)) == cudaSuccess &&
       cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(16, 1, 1);
     cfg.blockDim = dim3(kLeafThreads, 1, 1);
-    cfg.dynamicSmemBytes = LeafSmem<double, 16>::bytes(kLeafRowsTimesW / 16);
+    cfg.dynamicSmemBytes = LeafSmem<double, 16>::bytes(kLeafRowsTimesW / 16, 16);
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = 16;
@@ -292,20 +383,21 @@ int panel_leaf_max_width_for(Ctx& c, int rows) {
 }
 
 template <typename T>
-int panel_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int* ipiv, cudaStream_t st) {
+int panel_leaf(Ctx& c, T* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv, cudaStream_t st) {
   if (w <= 0) return LM_OK;
   const int R = n - c0;
   const int wmax = panel_leaf_max_width_for(c, R);
   if (w > wmax || w > 32) return LM_ERR_UNSUPPORTED;
   // smallest compiled width that holds w
-  if (w <= 4 && wmax >= 4) return launch_leaf<T, 4>(c, A, lda, n, c0, w, ipiv, st);
-  if (w <= 8 && wmax >= 8) return launch_leaf<T, 8>(c, A, lda, n, c0, w, ipiv, st);
-  if (w <= 16 && wmax >= 16) return launch_leaf<T, 16>(c, A, lda, n, c0, w, ipiv, st);
-  return launch_leaf<T, 32>(c, A, lda, n, c0, w, ipiv, st);
+  if (pw > 128 || pc0 > c0 || pc0 + pw < c0 + w) return LM_ERR_ARG;
+  if (w <= 4 && wmax >= 4) return launch_leaf<T, 4>(c, A, lda, n, c0, w, pc0, pw, ipiv, st);
+  if (w <= 8 && wmax >= 8) return launch_leaf<T, 8>(c, A, lda, n, c0, w, pc0, pw, ipiv, st);
+  if (w <= 16 && wmax >= 16) return launch_leaf<T, 16>(c, A, lda, n, c0, w, pc0, pw, ipiv, st);
+  return launch_leaf<T, 32>(c, A, lda, n, c0, w, pc0, pw, ipiv, st);
 }
 
-template int panel_leaf<double>(Ctx&, double*, long long, int, int, int, int*, cudaStream_t);
-template int panel_leaf<float>(Ctx&, float*, long long, int, int, int, int*, cudaStream_t);
+template int panel_leaf<double>(Ctx&, double*, long long, int, int, int, int, int, int*, cudaStream_t);
+template int panel_leaf<float>(Ctx&, float*, long long, int, int, int, int, int, int*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Cholesky of one diagonal block (w <= 128), right-looking in SMEM.
@@ -317,6 +409,7 @@ __global__ void __launch_bounds__(512) potrf_block_kernel(T* A, long long lda, i
   extern __shared__ __align__(16) unsigned char sm[];
   T* S = reinterpret_cast<T*>(sm);
   const int ld = w + 1;
+#pragma unroll 8
   for (int i = threadIdx.x; i < w * w; i += blockDim.x) {
     const int r = i / w, c = i % w;
     if (c <= r) S[r * ld + c] = A[(long long)r * lda + c];

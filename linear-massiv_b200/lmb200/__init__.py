@@ -32,7 +32,8 @@ LM_ERR_NOT_CONVERGED = -6
 # Every symbol include/lm_b200.h declares (checked by the CPU test suite).
 EXPORTS = [
     "lm_ctx_create", "lm_ctx_destroy", "lm_ctx_set_stream", "lm_ctx_get_stream",
-    "lm_ctx_synchronize", "lm_ctx_check", "lm_status_string", "lm_last_error",
+    "lm_ctx_synchronize", "lm_ctx_check", "lm_ctx_profile", "lm_ctx_profile_read",
+    "lm_status_string", "lm_last_error",
     "lm_launch_count", "lm_dmalloc", "lm_dfree", "lm_h2d", "lm_d2h", "lm_dgemm",
     "lm_dgetrf", "lm_dgetrs", "lm_dgesv", "lm_dpotrf", "lm_dpotrs", "lm_dposv",
     "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
@@ -76,6 +77,8 @@ def _lib():
                 "lm_ctx_get_stream": ([vp], vp),
                 "lm_ctx_synchronize": ([vp], i),
                 "lm_ctx_check": ([vp], i),
+                "lm_ctx_profile": ([vp, i], i),
+                "lm_ctx_profile_read": ([vp, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp], i),
                 "lm_status_string": ([i], ctypes.c_char_p),
                 "lm_last_error": ([], ctypes.c_char_p),
                 "lm_launch_count": ([], ctypes.c_longlong),
@@ -156,6 +159,19 @@ class Context:
 
     def check(self):
         _check(_lib().lm_ctx_check(self.h), "device status")
+
+    PHASES = ("gemm", "panel", "swap", "trsm", "other")
+
+    def profile(self, enable: bool = True):
+        _check(_lib().lm_ctx_profile(self.h, 1 if enable else 0), "lm_ctx_profile")
+
+    def profile_read(self) -> dict:
+        """Per-phase {launches, ms, flops, bytes} since the last read (synchronises)."""
+        n = len(self.PHASES)
+        L = (ctypes.c_longlong * n)()
+        M, F, B = (ctypes.c_double * n)(), (ctypes.c_double * n)(), (ctypes.c_double * n)()
+        _check(_lib().lm_ctx_profile_read(self.h, L, M, F, B), "lm_ctx_profile_read")
+        return {p: {"launches": int(L[i]), "ms": M[i], "flops": F[i], "bytes": B[i]} for i, p in enumerate(self.PHASES)}
 
 
 _DEFAULT = {}
