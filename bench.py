@@ -7,6 +7,11 @@ Workloads (--workload):
         work buffer (luSolveP's thaw), LU with partial pivoting, solve.
   chol  choleskySolve with A = B B^T + n I, B uniform[-1,1].
   gemm  C = A B, m = n = k.
+  ir    mixed precision: FP32 LU with tcgen05 3xTF32 updates, refined in FP64
+        to the normwise backward error 1e-15 n; A = U diag(sigma) V^T with U, V
+        products of seeded Householder reflectors and sigma geometric from 1
+        to 1/kappa (--kappa; 0 = uniform[-1,1] A).  The plain FP64 LU solve of
+        the same system is timed beside it.
 Metric: FP64-accurate solves per second (GEMMs per second for gemm), whole
 job.  Multi-GPU: replicas only — every rank solves its own system, no
 collective on the data path; value = all solves / max-over-ranks time.
@@ -20,6 +25,7 @@ the n^3 flop count.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -35,6 +41,7 @@ FLOPS = {
     "lu": lambda n, r: 2.0 / 3.0 * n ** 3 + 2.0 * n * n * r,
     "chol": lambda n, r: 1.0 / 3.0 * n ** 3 + 2.0 * n * n * r,
     "gemm": lambda n, r: 2.0 * n ** 3,
+    "ir": lambda n, r: 2.0 / 3.0 * n ** 3 + 2.0 * n * n * r,
 }
 
 
@@ -48,7 +55,9 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["lu", "chol", "gemm"], default="lu")
+    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir"], default="lu")
+    p.add_argument("--kappa", type=float, default=1e6, help="ir: condition number of A (0 = uniform A)")
+    p.add_argument("--reflectors", type=int, default=4, help="ir: Householder reflectors per side")
     p.add_argument("--n", type=int, default=16384)
     p.add_argument("--nrhs", type=int, default=1)
     p.add_argument("--seed", type=int, default=0)
@@ -61,6 +70,10 @@ def parse():
 
 
 def workload_name(a):
+    if a.workload == "ir":
+        spec = (f"A = U diag(sigma) V^T, kappa={a.kappa:g}, {a.reflectors} Householder reflectors per side"
+                if a.kappa > 0 else "A uniform[-1,1]")
+        return f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU + 3xTF32 tcgen05, FP64 refinement"
     if a.workload == "lu":
         return f"luSolve FP64 n={a.n} nrhs={a.nrhs}, A uniform[-1,1]"
     if a.workload == "chol":
@@ -158,10 +171,29 @@ def max_over_ranks(x: float, world: int) -> float:
 
 # ---- inputs ---------------------------------------------------------------------------
 
+def sigma_spectrum_matrix(n, kappa, reflectors, g, torch, np):
+    """A = U diag(sigma) V^T on the GPU (input preparation, not timed): sigma_i =
+    kappa^(-i/(n-1)), U and V products of seeded Householder reflectors."""
+    s = torch.from_numpy(kappa ** (-np.arange(n) / max(n - 1, 1))).cuda()
+    A = torch.diag(s)
+    for side in ("left", "right"):
+        for _ in range(reflectors):
+            v = torch.from_numpy(g.standard_normal(n)).cuda()
+            v /= torch.linalg.norm(v)
+            if side == "left":   # A <- (I - 2 v v^T) A
+                A -= 2.0 * torch.outer(v, v @ A)
+            else:                # A <- A (I - 2 v v^T)
+                A -= 2.0 * torch.outer(A @ v, v)
+    return A.cpu()
+
+
 def make_inputs(a, rank, torch, np):
     g = np.random.Generator(np.random.Philox(a.seed + 7919 * rank))
     n = a.n
-    A = torch.from_numpy(g.uniform(-1.0, 1.0, (n, n)))
+    if a.workload == "ir" and a.kappa > 0:
+        A = sigma_spectrum_matrix(n, a.kappa, a.reflectors, g, torch, np)
+    else:
+        A = torch.from_numpy(g.uniform(-1.0, 1.0, (n, n)))
     if a.workload == "chol":
         Bd = A.cuda()
         S = Bd @ Bd.T  # input preparation only (not timed)
@@ -209,7 +241,7 @@ def cpu_baseline(a):
     b = g.uniform(-1.0, 1.0, ns)
     if a.workload == "chol":
         A = A @ A.T + ns * np.eye(ns)
-    fn = {"lu": lambda: O.lu_solve_p(A, b), "chol": lambda: O.chol_solve_p(A, b),
+    fn = {"lu": lambda: O.lu_solve_p(A, b), "ir": lambda: O.lu_solve_p(A, b), "chol": lambda: O.chol_solve_p(A, b),
           "gemm": lambda: O.matmul_p(A, A)}[a.workload]
     fn()
     t0 = time.perf_counter()
@@ -245,7 +277,7 @@ def run_reference(a, world, rank):
         A = A @ A.T + ns * np.eye(ns)
 
     def step():
-        if a.workload == "lu":
+        if a.workload in ("lu", "ir"):
             O.lu_solve_p_many(A, b, threads, threads)
         elif a.workload == "chol":
             O.chol_solve_p_many(A, b, threads, threads)
@@ -295,7 +327,18 @@ def run_ours(a, world, rank, local):
 
     kk = gemm_k(a)
 
+    ir_stats = {}
+
     def step():
+        if a.workload == "ir":
+            it, be, info = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_int(0)
+            st = lib.lm_dgesv_ir(ctx.h, n, nrhs, P(A_d), n, P(B_d), nrhs, P(X), nrhs, 0.0, 50, ctypes.byref(it),
+                                 ctypes.byref(be), ctypes.byref(info))
+            ir_stats["iters"] = it.value
+            ir_stats["berr"] = be.value
+            if st < 0:
+                raise lmb200.LMError(st, "ir step")
+            return
         if a.workload == "gemm":
             st = lib.lm_dgemm(ctx.h, n, n, kk, 1.0, P(A_d), kk, P(B_d), n, 1.0 if kk != n else 0.0, P(work), n)
         else:
@@ -346,12 +389,45 @@ def run_ours(a, world, rank, local):
     t = max_over_ranks(t_local, world)
     value = world * a.steps / t
 
+    # IR: time the plain FP64 LU solve of the same system beside it
+    fp64_ref = None
+    if a.workload == "ir":
+        def fp64_step():
+            work.copy_(A_d)
+            Xf.copy_(B_d)
+            st = lib.lm_dgesv(ctx.h, n, nrhs, P(work), n, P(ipiv), P(Xf), nrhs, None)
+            if st < 0:
+                raise lmb200.LMError(st, "fp64 step")
+        Xf = torch.empty_like(B_d)
+        for _ in range(2):
+            fp64_step()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        kf = max(2, a.steps // 2)
+        for _ in range(kf):
+            fp64_step()
+        f1.record()
+        torch.cuda.synchronize()
+        tf = f0.elapsed_time(f1) * 1e-3 / kf
+        R = B_d - A_d @ Xf
+        be64 = R.abs().max().item() / (A_d.abs().sum(dim=1).max().item() * Xf.abs().max().item() +
+                                      B_d.abs().max().item())
+        fwd = ((X - Xf).abs().max() / Xf.abs().max()).item()
+        fp64_ref = {"fp64_lu_solves_per_s": 1.0 / tf, "fp64_lu_ms": tf * 1e3, "fp64_backward_error": be64,
+                    "ir_vs_fp64_speedup": (a.steps / t) / (1.0 / tf), "ir_vs_fp64_rel_diff": fwd}
+        del R
+
     # e2e through the host-buffer entry point: H2D of A and B, solve, D2H of X
     Xh = torch.empty((n, n) if a.workload == "gemm" else tuple(B_h.shape), dtype=torch.float64).pin_memory()
     dp = lmb200._np_ptr
 
     def e2e_step():
-        if a.workload == "lu":
+        if a.workload == "ir":
+            it, be, info = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_int(0)
+            st = lib.lm_lu_solve_ir_host(ctx.h, n, nrhs, dp(A_h.numpy()), dp(B_h.numpy()), dp(Xh.numpy()), 0.0, 50,
+                                         ctypes.byref(it), ctypes.byref(be), ctypes.byref(info))
+        elif a.workload == "lu":
             st = lib.lm_lu_solve_host(ctx.h, n, nrhs, dp(A_h.numpy()), dp(B_h.numpy()), dp(Xh.numpy()), None)
         elif a.workload == "chol":
             st = lib.lm_chol_solve_host(ctx.h, n, nrhs, dp(A_h.numpy()), dp(B_h.numpy()), dp(Xh.numpy()), None)
@@ -385,7 +461,8 @@ def run_ours(a, world, rank, local):
                    "l2": "inputs larger than L2 (8 n^2 bytes per matrix)"},
         "gpu_launches": launches,
         "e2e": {"value": e2e_val, "unit": metric_name(a), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": a.e2e_steps, "api": "lm_lu_solve_host / lm_chol_solve_host / lm_matmul_host"},
+                "steps": a.e2e_steps, "api": {"lu": "lm_lu_solve_host", "chol": "lm_chol_solve_host", "gemm": "lm_matmul_host",
+                                             "ir": "lm_lu_solve_ir_host"}[a.workload]},
         "roofline": {"bound": "tensor", "kernel": "dgemm_dmma_kernel (FP64 DMMA trailing updates)",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
@@ -397,6 +474,7 @@ def run_ours(a, world, rank, local):
         "host_enqueue_ms_per_step": host_enqueue_ms,
         "profiled": not a.no_profile,
         "accuracy": accuracy,
+        "ir": ({**ir_stats, **(fp64_ref or {})} if a.workload == "ir" else None),
         "clocks": clk,
     }
     if world == 1 and not a.no_cpu_baseline:

@@ -157,6 +157,23 @@ int lm_det_host(lm_ctx* ctx, int n, const double* A, double* det);
 /* Host helper: swap list -> permutation vector (the reference's `lu` form). */
 int lm_ipiv_to_perm(int n, const int* ipiv, int* perm);
 
+/* ---- mixed precision with iterative refinement -----------------------------
+ * No counterpart in the reference (its solves are FP64 throughout).  A is
+ * rounded to FP32 and factored with partial pivoting, every Schur-complement
+ * update on the tcgen05 tensor cores in TF32 with FP32 accumulation; the
+ * solution is then refined in FP64 (residual r = B - A X with the original A,
+ * correction from the FP32 factors, X += d) until the normwise backward error
+ * ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) of every column is <= tol
+ * (tol <= 0 selects 1e-15 * n).  A and B are not modified; X (n x nrhs,
+ * nrhs <= 64) receives the solution.  Returns LM_ERR_NOT_CONVERGED (with X the
+ * last iterate) when max_iter corrections do not reach tol, e.g. for
+ * condition numbers beyond what FP32/TF32 factors can precondition. */
+int lm_dgesv_ir(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* B, int ldb, double* X,
+                int ldx, double tol, int max_iter, int* iters, double* berr, int* info);
+/* Host-buffer form of lm_dgesv_ir (dense row-major host arrays). */
+int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X, double tol,
+                        int max_iter, int* iters, double* berr, int* info);
+
 /* ---- residual (IR and the reference's scaled residual) ---------------------
  * R = B - A X in FP64 (device), n x nrhs; replaces matvec / rawGemv
  * (L2.hs:123-144, K.hs:119-134) on the refinement path. */

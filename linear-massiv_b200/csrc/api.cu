@@ -593,6 +593,31 @@ int lm_dposv(lm_ctx* ctx, int n, int nrhs, double* A, int lda, double* B, int ld
   });
 }
 
+int lm_dgesv_ir(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* B, int ldb, double* X,
+                int ldx, double tol, int max_iter, int* iters, double* berr, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || nrhs > 64 || max_iter < 1) return LM_ERR_ARG;
+    if (n == 0 || nrhs == 0) {
+      if (iters) *iters = 0;
+      if (berr) *berr = 0.0;
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    if (!A || !B || !X || lda < n || ldb < nrhs || ldx < nrhs) return LM_ERR_ARG;
+    if (tol <= 0) tol = 1e-15 * n;
+    LM_TRY(lm::reset_info(c));
+    const std::string key = lm::gkey("sgetrf_ir", {n, (long long)A, lda});
+    int r = lm::dgesv_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream,
+                         [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+    int inf = 0;
+    int s = lm::read_status(c, &inf);
+    if (s < 0) return s;
+    if (info) *info = inf;
+    if (r < 0) return r;
+    return inf;
+  });
+}
+
 int lm_dresidual(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* X, int ldx,
                  const double* B, int ldb, double* R, int ldr) {
   return guarded(ctx, [&](Ctx& c) {
@@ -709,6 +734,38 @@ int lm_chol_solve_host(lm_ctx* ctx, int n, int nrhs, const double* A, const doub
     int r = lm::read_status(c, &inf);
     if (info) *info = inf;
     return r;
+  });
+}
+
+int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X, double tol,
+                        int max_iter, int* iters, double* berr, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || nrhs > 64 || max_iter < 1) return LM_ERR_ARG;
+    if (n == 0 || nrhs == 0) {
+      if (iters) *iters = 0;
+      if (berr) *berr = 0.0;
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    if (!A || !B || !X) return LM_ERR_ARG;
+    if (tol <= 0) tol = 1e-15 * n;
+    HostBufs hb;
+    LM_TRY(host_bufs(c, n, 2 * nrhs, hb));  // B and X side by side
+    LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
+    LM_TRY(h2d_2d(c, hb.B, hb.ldb, B, nrhs, n, nrhs));
+    LM_TRY(lm::reset_info(c));
+    double* dX = hb.B + nrhs;
+    const std::string key = lm::gkey("sgetrf_ir_host", {n, (long long)hb.A, hb.lda});
+    int r = lm::dgesv_ir(c, n, nrhs, hb.A, hb.lda, hb.B, hb.ldb, dX, hb.ldb, tol, max_iter, iters, berr, c.stream,
+                         [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+    if (r < 0 && r != LM_ERR_NOT_CONVERGED) return r;
+    LM_TRY(d2h_2d(c, X, nrhs, dX, hb.ldb, n, nrhs));
+    int inf = 0;
+    int s = lm::read_status(c, &inf);
+    if (s < 0) return s;
+    if (info) *info = inf;
+    if (r < 0) return r;
+    return inf;
   });
 }
 

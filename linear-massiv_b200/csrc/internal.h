@@ -4,6 +4,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstddef>
+#include <functional>
 
 namespace lm {
 
@@ -107,6 +108,16 @@ int panel_leaf_max_width_for(Ctx& c, int rows);  // widest leaf one cluster hold
 // records the first non-positive pivot (global index base + j + 1) in status[1].
 template <typename T>
 int potrf_block(Ctx& c, T* A, long long lda, int w, int base, cudaStream_t st);
+
+// Mixed precision (ir.cu): FP32 LU with TF32 tensor-core updates, FP32
+// substitutions, FP64 refinement.  `factor_runner` runs the factorisation
+// body (so the caller can capture it into a CUDA graph).
+int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st);
+int sgetrs(Ctx& c, int n, int nrhs, const float* LU, long long lda, const int* ipiv, float* X, long long ldx,
+           cudaStream_t st);
+int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+             long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
+             const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner);
 
 // r = b - A x for nrhs columns (FP64), and max-norm helpers (resid.cu).
 int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* X, long long ldx,

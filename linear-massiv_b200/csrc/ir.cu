@@ -1,0 +1,339 @@
+// Mixed precision: FP32 LU with TF32 tensor-core updates, FP64 iterative
+// refinement.  No counterpart in linear-massiv (its luSolveP, LU.hs:265-304, is
+// FP64 throughout); the refinement recovers FP64-accurate solutions:
+//
+//   A32 = fl32(A);  P A32 = L U   (panel leaves and TRSM in FP32, all
+//                                  Schur-complement GEMMs on tcgen05 TF32)
+//   x = 0, r = b
+//   repeat:  d = U^-1 L^-1 P fl32(r)       (FP32 substitutions)
+//            x = x + d                     (FP64)
+//            r = b - A x                   (FP64, original A)
+//   until  ||r||_inf / (||A||_inf ||x||_inf + ||b||_inf) <= tol  (per column)
+//
+// The stopping metric is the reference test suite's scaledResidualLinear
+// without the n*eps guard (test/Test/Residuals.hs:69-78).
+#include <algorithm>
+#include <cstring>
+#include <functional>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace lm {
+
+void count_launch(int n);
+int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
+               long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
+               const float* Btlo);
+
+namespace {
+
+constexpr int kNB = 128;
+
+__global__ void d2s_kernel(float* dst, long long ldd, const double* src, long long lds, int rows, int cols) {
+  const long long total = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    dst[(long long)r * ldd + c] = (float)src[(long long)r * lds + c];
+  }
+}
+
+__device__ __forceinline__ float tf32_hi(float a) { return __uint_as_float(__float_as_uint(a) & 0xFFFFE000u); }
+
+// Split for 3xTF32: hi = a with the 13 low mantissa bits cleared (exactly
+// representable in TF32), lo = a - hi (exact in FP32).
+// dst_hi/dst_lo (cols x rows) = split(src (rows x cols))^T.
+__global__ void transpose_split_kernel(float* dhi, float* dlo, long long ldd, const float* src, long long lds,
+                                       int rows, int cols) {
+  __shared__ float tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = by + j, c = bx + threadIdx.x;
+    if (r < rows && c < cols) tile[j][threadIdx.x] = src[(long long)r * lds + c];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = bx + j, c = by + threadIdx.x;
+    if (r < cols && c < rows) {
+      const float a = tile[threadIdx.x][j];
+      const float h = tf32_hi(a);
+      dhi[(long long)r * ldd + c] = h;
+      dlo[(long long)r * ldd + c] = a - h;
+    }
+  }
+}
+
+// dst_hi/dst_lo (rows x cols, ldd) = split(src (rows x cols, lds)).
+__global__ void split_kernel(float* dhi, float* dlo, long long ldd, const float* src, long long lds, int rows,
+                             int cols) {
+  const long long total = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    const float a = src[(long long)r * lds + c];
+    const float h = tf32_hi(a);
+    dhi[(long long)r * ldd + c] = h;
+    dlo[(long long)r * ldd + c] = a - h;
+  }
+}
+
+// X[m x nrhs] -= M[m x k] * Y[k x nrhs] in FP32 (exact fp32 FMAs), one warp per
+// row, nrhs <= 64 (the right-hand-side updates of the FP32 substitutions).
+__global__ void sgemm_rhs_kernel(int m, int k, int nrhs, const float* __restrict__ M, long long ldm,
+                                 const float* __restrict__ Y, long long ldy, float* X, long long ldx) {
+  const int warps = blockDim.x >> 5;
+  const int row = blockIdx.x * warps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= m) return;
+  const float* mr = M + (long long)row * ldm;
+  for (int c0 = 0; c0 < nrhs; c0 += 8) {
+    float acc[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) acc[c] = 0.f;
+    for (int kk = lane; kk < k; kk += 32) {
+      const float a = mr[kk];
+#pragma unroll
+      for (int c = 0; c < 8; ++c)
+        if (c0 + c < nrhs) acc[c] = fmaf(a, Y[(long long)kk * ldy + c0 + c], acc[c]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], o);
+    if (lane == 0)
+      for (int c = 0; c < 8 && c0 + c < nrhs; ++c) X[(long long)row * ldx + c0 + c] -= acc[c];
+  }
+}
+
+// X (FP64) += D (FP32); R (FP32) <- fl32(Rd) helpers.
+__global__ void add_s2d_kernel(double* X, long long ldx, const float* D, long long ldd, int rows, int cols) {
+  const long long total = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    X[(long long)r * ldx + c] += (double)D[(long long)r * ldd + c];
+  }
+}
+
+// ||A||_inf (max row sum of |a_ij|) into out[0] as the bits of a non-negative
+// double (atomicMax on the ordered integer image).
+__global__ void norm_inf_rows_kernel(const double* A, long long lda, int n, unsigned long long* out) {
+  const int warps = blockDim.x >> 5;
+  const int row = blockIdx.x * warps + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (row >= n) return;
+  double s = 0.0;
+  for (int j = lane; j < n; j += 32) s += fabs(A[(long long)row * lda + j]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(s));
+}
+
+// Per column c: max_i |V_ic| into out[c] (ordered-integer atomicMax).
+__global__ void colmax_abs_kernel(const double* V, long long ldv, int rows, int cols, unsigned long long* out) {
+  const long long total = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    atomicMax(out + c, (unsigned long long)__double_as_longlong(fabs(V[(long long)r * ldv + c])));
+  }
+}
+
+int grid_of(long long total) { return (int)std::max<long long>(1, std::min<long long>(cdivll(total, 256), 2048)); }
+
+// Scratch for the split operands of the 3xTF32 update: L21 -> Ahi/Alo
+// (m x k), U12^T -> Bhi/Blo (n x k); all with leading dimension 128 (k <= 128).
+struct SScratch {
+  float *Ahi, *Alo, *Bhi, *Blo;
+  long long ld;
+};
+
+int s_update(Ctx& c, int m, int n, int k, float* A21, long long lda, const float* U12, float* C, SScratch& s,
+             cudaStream_t st) {
+  // C -= A21 (m x k) * U12 (k x n), as 3xTF32 on the tensor cores
+  dim3 tb(32, 8), tg(cdiv(n, 32), cdiv(k, 32));
+  transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, U12, lda, k, n);
+  split_kernel<<<grid_of((long long)m * k), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, k);
+  count_launch(2);
+  LM_CUDA_TRY(cudaGetLastError());
+  return sgemm_tf32(c, m, n, k, -1.0f, s.Ahi, s.ld, s.Bhi, s.ld, 1.0f, C, lda, st, s.Alo, s.Blo);
+}
+
+int sgetrf_panel_rec(Ctx& c, float* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv, SScratch& s,
+                     cudaStream_t st) {
+  const int R = n - c0;
+  const int wmax = panel_leaf_max_width_for(c, R);
+  if (wmax <= 0) return LM_ERR_UNSUPPORTED;
+  if (w <= wmax) {
+    Prof p(c, kPhasePanel, (double)R * w * w, 8.0 * R * w, st);
+    return panel_leaf<float>(c, A, lda, n, c0, w, pc0, pw, ipiv, st);
+  }
+  int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
+  if (w1 >= w) w1 = w - 4;
+  const int w2 = w - w1;
+  LM_TRY(sgetrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st));
+  float* A11 = A + (long long)c0 * lda + c0;
+  {
+    Prof p(c, kPhaseTrsm, (double)w1 * w1 * w2, 4.0 * ((double)w1 * w1 / 2 + 2.0 * w1 * w2), st);
+    LM_TRY(trsm_left<float>(A11, lda, w1, true, true, false, A11 + w1, lda, w2, st));
+  }
+  LM_TRY(s_update(c, R - w1, w2, w1, A11 + (long long)w1 * lda, lda, A11 + w1, A11 + (long long)w1 * lda + w1, s, st));
+  return sgetrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st);
+}
+
+}  // namespace
+
+int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
+  void* ws = nullptr;
+  SScratch s;
+  s.ld = kNB;
+  LM_TRY(ctx_workspace(c, 1, 4 * sizeof(float) * (size_t)n * kNB, &ws));
+  s.Ahi = static_cast<float*>(ws);
+  s.Alo = s.Ahi + (size_t)n * kNB;
+  s.Bhi = s.Alo + (size_t)n * kNB;
+  s.Blo = s.Bhi + (size_t)n * kNB;
+  for (int k0 = 0; k0 < n; k0 += kNB) {
+    const int w = std::min(kNB, n - k0);
+    LM_TRY(sgetrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, s, st));
+    {
+      Prof p(c, kPhaseSwap, 0.0, 16.0 * w * (n - w), st);
+      LM_TRY(laswp<float>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st));
+    }
+    if (k0 + w < n) {
+      float* A11 = A + (long long)k0 * lda + k0;
+      {
+        const double nc = n - k0 - w;
+        Prof p(c, kPhaseTrsm, (double)w * w * nc, 4.0 * ((double)w * w / 2 + 2.0 * w * nc), st);
+        LM_TRY(trsm_left<float>(A11, lda, w, true, true, false, A11 + w, lda, n - k0 - w, st));
+      }
+      LM_TRY(s_update(c, n - k0 - w, n - k0 - w, w, A11 + (long long)w * lda, lda, A11 + w,
+                      A11 + (long long)w * lda + w, s, st));
+    }
+  }
+  return LM_OK;
+}
+
+// Solve with the FP32 factors: X (n x nrhs, FP32, ldx) overwritten.
+int sgetrs(Ctx& c, int n, int nrhs, const float* LU, long long lda, const int* ipiv, float* X, long long ldx,
+           cudaStream_t st) {
+  {
+    Prof p(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, st);
+    LM_TRY(laswp<float>(X, ldx, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+  }
+  for (int i0 = 0; i0 < n; i0 += kNB) {
+    const int w = std::min(kNB, n - i0);
+    const float* Lii = LU + (long long)i0 * lda + i0;
+    {
+      Prof p(c, kPhaseTrsm, (double)w * w * nrhs, 4.0 * ((double)w * w / 2 + 2.0 * w * nrhs), st);
+      LM_TRY(trsm_left<float>(Lii, lda, w, true, true, false, X + (long long)i0 * ldx, ldx, nrhs, st));
+    }
+    if (i0 + w < n) {
+      const int m = n - i0 - w;
+      Prof p(c, kPhaseGemm, 2.0 * m * w * nrhs, 4.0 * (double)m * w, st);
+      sgemm_rhs_kernel<<<cdiv(m, 8), 256, 0, st>>>(m, w, nrhs, Lii + (long long)w * lda, lda,
+                                                   X + (long long)i0 * ldx, ldx, X + (long long)(i0 + w) * ldx, ldx);
+      count_launch(1);
+      LM_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  const int nblk = (n + kNB - 1) / kNB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int i0 = b * kNB;
+    const int w = std::min(kNB, n - i0);
+    const float* Uii = LU + (long long)i0 * lda + i0;
+    {
+      Prof p(c, kPhaseTrsm, (double)w * w * nrhs, 4.0 * ((double)w * w / 2 + 2.0 * w * nrhs), st);
+      LM_TRY(trsm_left<float>(Uii, lda, w, false, false, false, X + (long long)i0 * ldx, ldx, nrhs, st));
+    }
+    if (i0 > 0) {
+      Prof p(c, kPhaseGemm, 2.0 * i0 * w * nrhs, 4.0 * (double)i0 * w, st);
+      sgemm_rhs_kernel<<<cdiv(i0, 8), 256, 0, st>>>(i0, w, nrhs, LU + i0, lda, X + (long long)i0 * ldx, ldx, X,
+                                                    ldx);
+      count_launch(1);
+      LM_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  return LM_OK;
+}
+
+int convert_d2s(float* dst, long long ldd, const double* src, long long lds, int rows, int cols, cudaStream_t st) {
+  d2s_kernel<<<grid_of((long long)rows * cols), 256, 0, st>>>(dst, ldd, src, lds, rows, cols);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+// Iterative refinement driver.  A, B, X are FP64 device buffers; X receives
+// the solution.  Returns info (> 0 if the FP32 factor hit a zero pivot),
+// LM_ERR_NOT_CONVERGED if some column misses tol after max_iter steps.
+int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+             long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
+             const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner) {
+  const long long lda32 = (n + 31) / 32 * 32;
+  const long long ldr = (nrhs + 7) / 8 * 8;
+  const size_t a32_bytes = sizeof(float) * (size_t)n * lda32;
+  const size_t piv_bytes = sizeof(int) * (size_t)((n + 63) / 64 * 64);
+  const size_t r_bytes = sizeof(double) * (size_t)n * ldr;
+  const size_t d_bytes = sizeof(float) * (size_t)n * ldr;
+  const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(1 + 3 * 64);
+  void* ws = nullptr;
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes, &ws));
+  char* p = static_cast<char*>(ws);
+  float* A32 = reinterpret_cast<float*>(p);
+  int* ipiv = reinterpret_cast<int*>(p + a32_bytes);
+  double* R = reinterpret_cast<double*>(p + a32_bytes + piv_bytes);
+  float* D = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes);
+  unsigned long long* nrm = reinterpret_cast<unsigned long long*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes);
+  if (nrhs > 64) return LM_ERR_UNSUPPORTED;
+
+  // ||A||_inf and ||B_c||_inf (FP64, from the original data)
+  LM_CUDA_TRY(cudaMemsetAsync(nrm, 0, nrm_bytes, st));
+  norm_inf_rows_kernel<<<cdiv(n, 8), 256, 0, st>>>(A, lda, n, nrm);
+  colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(B, ldb, n, nrhs, nrm + 1);
+  count_launch(2);
+  // factor fl32(A)
+  LM_TRY(factor_runner([&](cudaStream_t s) {
+    LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
+    return sgetrf(c, n, A32, lda32, ipiv, s);
+  }));
+  // x = 0, r = b
+  LM_CUDA_TRY(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * nrhs, n, st));
+  LM_TRY(copy2d<double>(R, ldr, B, ldb, n, nrhs, st));
+  std::vector<unsigned long long> h(1 + 3 * 64);
+  int it = 0;
+  double worst = 0.0;
+  for (it = 1; it <= max_iter; ++it) {
+    LM_TRY(convert_d2s(D, ldr, R, ldr, n, nrhs, st));
+    LM_TRY(sgetrs(c, n, nrhs, A32, lda32, ipiv, D, ldr, st));
+    add_s2d_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, D, ldr, n, nrhs);
+    count_launch(1);
+    LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, st));
+    LM_CUDA_TRY(cudaMemsetAsync(nrm + 1 + 64, 0, sizeof(unsigned long long) * 128, st));
+    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(R, ldr, n, nrhs, nrm + 1 + 64);
+    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, n, nrhs, nrm + 1 + 128);
+    count_launch(2);
+    LM_CUDA_TRY(cudaMemcpyAsync(h.data(), nrm, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
+    LM_CUDA_TRY(cudaStreamSynchronize(st));
+    auto dbl = [](unsigned long long u) {
+      double d;
+      std::memcpy(&d, &u, sizeof d);
+      return d;
+    };
+    const double anorm = dbl(h[0]);
+    worst = 0.0;
+    for (int col = 0; col < nrhs; ++col) {
+      const double rn = dbl(h[1 + 64 + col]), xn = dbl(h[1 + 128 + col]), bn = dbl(h[1 + col]);
+      const double den = anorm * xn + bn;
+      const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
+      worst = std::max(worst, (be != be) ? 1e300 : be);
+    }
+    if (worst <= tol) break;
+  }
+  if (iters_out) *iters_out = std::min(it, max_iter);
+  if (berr_out) *berr_out = worst;
+  return worst <= tol ? LM_OK : LM_ERR_NOT_CONVERGED;
+}
+
+}  // namespace lm

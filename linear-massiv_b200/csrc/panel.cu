@@ -42,15 +42,16 @@ __device__ __forceinline__ T absval(T x) {
   return (a != a) ? T(-1) : a;  // NaN never wins the scan
 }
 
-// One CTA's per-column message, pushed into every CTA of the cluster:
-//   [0] |a| of its best candidate (or -1), [1] that row (relative to c0, as T),
-//   [2] 1 if it owns row j and a_jj is NaN, [3] unused,
-//   [4, 4 + W) the candidate row, [4 + W, 4 + 2W) row j (from its owner).
+// Per-column messages pushed into every CTA of the cluster (T elements):
+//   candidate message (one per source CTA): [0] |a| of its best candidate or
+//     -1, [1] that row relative to c0 (or -1), [2..3] unused, [4, 4 + W) the row;
+//   row-j message (from the CTA owning row j): [0] 1 if a_jj is NaN,
+//     [1..3] unused, [4, 4 + W) row j.
 template <typename T, int W>
 struct LeafMsg {
-  static constexpr int N = 4 + 2 * W;                      // elements
-  static constexpr int BYTES = N * (int)sizeof(T);         // multiple of 16
-  static constexpr int CHUNKS = BYTES / 16;                 // 16-byte st.async pieces
+  static constexpr int N = 4 + W;
+  static constexpr int BYTES = N * (int)sizeof(T);
+  static constexpr int CHUNKS = BYTES / 16;
   static constexpr int PER_CHUNK = 16 / (int)sizeof(T);
   static_assert(BYTES % 16 == 0, "message must be a whole number of 16-byte chunks");
 };
@@ -58,32 +59,46 @@ struct LeafMsg {
 template <typename T, int W>
 struct LeafSmem {
   using M = LeafMsg<T, W>;
-  static constexpr size_t recv_off = 0;                                   // T[2][16][M::N]
-  static constexpr size_t recv_bytes = 2 * 16 * (size_t)M::BYTES;
-  static constexpr size_t bar_off = recv_off + recv_bytes;                // uint64_t[2]
-  static constexpr size_t wval_off = bar_off + 16;                        // T[16]
-  static constexpr size_t widx_off = wval_off + 16 * sizeof(T);           // int[16]
-  static constexpr size_t hist_off = widx_off + 16 * sizeof(int);         // int[W] pivot rows
-  static constexpr size_t trow_off = hist_off + W * sizeof(int);          // int[2W] touched rows
-  static constexpr size_t tsrc_off = trow_off + 2 * W * sizeof(int);      // int[2W] their sources
-  static constexpr size_t tm_off = tsrc_off + 2 * W * sizeof(int);        // int touched count
-  static constexpr size_t p_off = (tm_off + sizeof(int) + 15) / 16 * 16;
+  static constexpr size_t cand_off = 0;                                    // T[2][16][N]
+  static constexpr size_t rowj_off = cand_off + 2 * 16 * (size_t)M::BYTES;  // T[2][N]
+  static constexpr size_t outc_off = rowj_off + 2 * (size_t)M::BYTES;       // T[N] outgoing candidate
+  static constexpr size_t outj_off = outc_off + (size_t)M::BYTES;           // T[N] outgoing row j
+  static constexpr size_t bar_off = outj_off + (size_t)M::BYTES;            // uint64_t[2]
+  static constexpr size_t wval_off = bar_off + 16;                          // T[16]
+  static constexpr size_t widx_off = wval_off + 16 * sizeof(T);             // int[16]
+  static constexpr size_t hist_off = widx_off + 16 * sizeof(int);           // int[W] pivot rows
+  static constexpr size_t trow_off = hist_off + W * sizeof(int);            // int[2W] touched rows
+  static constexpr size_t tsrc_off = trow_off + 2 * W * sizeof(int);        // int[2W] their sources
+  static constexpr size_t tm_off = tsrc_off + 2 * W * sizeof(int);          // int touched count
+  static constexpr size_t stage_off = (tm_off + sizeof(int) + 15) / 16 * 16;
   // Swap staging for the other panel columns: 2W rows x up to 128 columns, split over the cluster.
   static size_t stage_elems(int C) { return (size_t)(2 * W * 128 + C - 1) / C; }
-  static size_t bytes(int rpc, int C) {
-    return p_off + (size_t)W * (rpc + 1) * sizeof(T) + stage_elems(C) * sizeof(T);
-  }
+  static size_t bytes(int /*rpc*/, int C) { return stage_off + stage_elems(C) * sizeof(T); }
 };
 
+template <typename T>
+__device__ __forceinline__ void pack16(const T* src, uint32_t (&w)[4]) {
+  if constexpr (sizeof(T) == 8) {
+    const unsigned long long a = (unsigned long long)__double_as_longlong((double)src[0]);
+    const unsigned long long b = (unsigned long long)__double_as_longlong((double)src[1]);
+    w[0] = (uint32_t)a; w[1] = (uint32_t)(a >> 32); w[2] = (uint32_t)b; w[3] = (uint32_t)(b >> 32);
+  } else {
+    w[0] = __float_as_uint((float)src[0]); w[1] = __float_as_uint((float)src[1]);
+    w[2] = __float_as_uint((float)src[2]); w[3] = __float_as_uint((float)src[3]);
+  }
+}
+
+// Push a message staged in this CTA's shared memory (`msg`) to the same
+// offset `slot` in every CTA of the cluster, completing on their `bar`.
 template <typename T, int W>
-__device__ __forceinline__ T msg_elem(int e, const T* P, int ldp, int crow, int jrow, T val, int idx, int jnan) {
-  // element e of this CTA's message (crow/jrow: slab rows of the candidate / row j, -1 if none)
-  if (e == 0) return val;
-  if (e == 1) return T(idx);
-  if (e == 2) return T(jnan);
-  if (e == 3) return T(0);
-  if (e < 4 + W) return crow >= 0 ? P[(e - 4) * ldp + crow] : T(0);
-  return jrow >= 0 ? P[(e - 4 - W) * ldp + jrow] : T(0);
+__device__ __forceinline__ void push_all(const T* msg, T* slot, uint64_t* bar, int C, int lane) {
+  using M = LeafMsg<T, W>;
+  for (int it = lane; it < C * M::CHUNKS; it += 32) {
+    const int d = it / M::CHUNKS, ch = it % M::CHUNKS;
+    uint32_t w4[4];
+    pack16<T>(msg + ch * M::PER_CHUNK, w4);
+    st_async_16(dsmem_map(slot, d) + ch * 16, dsmem_map(bar, d), w4[0], w4[1], w4[2], w4[3]);
+  }
 }
 
 template <typename T, int W>
@@ -93,7 +108,10 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   using L = LeafSmem<T, W>;
   using M = LeafMsg<T, W>;
   extern __shared__ __align__(16) unsigned char sm[];
-  T* recv = reinterpret_cast<T*>(sm + L::recv_off);
+  T* cand = reinterpret_cast<T*>(sm + L::cand_off);
+  T* rowjb = reinterpret_cast<T*>(sm + L::rowj_off);
+  T* outc = reinterpret_cast<T*>(sm + L::outc_off);
+  T* outj = reinterpret_cast<T*>(sm + L::outj_off);
   uint64_t* rbar = reinterpret_cast<uint64_t*>(sm + L::bar_off);
   T* wval = reinterpret_cast<T*>(sm + L::wval_off);
   int* widx = reinterpret_cast<int*>(sm + L::widx_off);
@@ -101,8 +119,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   int* trow = reinterpret_cast<int*>(sm + L::trow_off);
   int* tsrc = reinterpret_cast<int*>(sm + L::tsrc_off);
   int* tm = reinterpret_cast<int*>(sm + L::tm_off);
-  T* P = reinterpret_cast<T*>(sm + L::p_off);
-  const int ldp = rpc + 1;
+  T* stage = reinterpret_cast<T*>(sm + L::stage_off);
 
   const int q = (int)cluster_ctarank();
   const int C = (int)cluster_nctarank();
@@ -111,43 +128,44 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   const int R = n - c0;
   const int rbeg = q * rpc;
   const int rcnt = max(0, min(rpc, R - rbeg));
-  constexpr int RPT = (kLeafRowsTimesW / W + kLeafThreads - 1) / kLeafThreads;  // rows per thread
+  constexpr int RPT = kLeafRowsTimesW / W / kLeafThreads;  // rows per thread (= 32 / W)
+  static_assert(RPT * W == kLeafRowsTimesW / kLeafThreads, "slab must split evenly");
 
   if (tid == 0) {
     mbar_init(&rbar[0], 1);
     mbar_init(&rbar[1], 1);
     fence_barrier_init();
   }
-  // Load this CTA's slab, column-major: P[c * ldp + r].  Unrolled so each
-  // thread keeps several independent loads in flight.
-  {
-    const int total = rcnt * W;
-#pragma unroll 8
-    for (int i = tid; i < total; i += kLeafThreads) {
-      const int r = i / W, c = i % W;
-      P[c * ldp + r] = (c < w) ? A[(long long)(c0 + rbeg + r) * lda + c0 + c] : T(0);
-    }
+  // This thread's rows of the slab, in registers: row r = tid + u * threads.
+  T x[RPT][W];
+#pragma unroll
+  for (int u = 0; u < RPT; ++u) {
+    const int r = tid + u * kLeafThreads;
+    const T* src = A + (long long)(c0 + rbeg + r) * lda + c0;
+#pragma unroll
+    for (int c = 0; c < W; ++c) x[u][c] = (r < rcnt && c < w) ? src[c] : T(0);
   }
-  // every CTA's barriers exist before anyone pushes into them
-  cluster_sync_all();
+  cluster_sync_all();  // every CTA's barriers exist before anyone pushes into them
 
-  // Local argmax of column 0.
   T bv = T(-1);
   int bi = INT_MAX;
 #pragma unroll
   for (int u = 0; u < RPT; ++u) {
     const int r = tid + u * kLeafThreads;
     if (r < rcnt) {
-      const T v = absval(P[r]);
+      const T v = absval(x[u][0]);
       if (better(v, rbeg + r, bv, bi)) { bv = v; bi = rbeg + r; }
     }
   }
 
   bool timed_out = false;
-  for (int j = 0; j < w; ++j) {
+#pragma unroll
+  for (int j = 0; j < W; ++j) {
+    if (j >= w) break;
     const int par = j & 1;
-    if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)(C * M::BYTES));
-    // ---- CTA-level argmax: warp shuffles, one barrier, every warp reduces ----
+    const int owner_j = j / rpc;
+    if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)((C + 1) * M::BYTES));
+    // ---- CTA argmax: warp shuffles, one barrier, every warp reduces ----
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -156,7 +174,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     }
     if (lane == 0) { wval[warp] = bv; widx[warp] = bi; }
     __syncthreads();
-    if (warp < C) {  // warp d pushes this CTA's message into CTA d
+    {
       T v = lane < kLeafThreads / 32 ? wval[lane] : T(-1);
       int i = lane < kLeafThreads / 32 ? widx[lane] : INT_MAX;
 #pragma unroll
@@ -165,37 +183,57 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
         const int oi = __shfl_xor_sync(0xffffffffu, i, o);
         if (better(ov, oi, v, i)) { v = ov; i = oi; }
       }
-      const int crow = (i != INT_MAX) ? i - rbeg : -1;
-      const bool own_j = j >= rbeg && j < rbeg + rcnt;
-      const int jrow = own_j ? j - rbeg : -1;
-      int jnan = 0;
-      if (own_j) {
-        const T d = P[j * ldp + jrow];
-        jnan = (d != d) ? 1 : 0;
-      }
-      T* slot = recv + ((size_t)par * 16 + q) * M::N;  // my slot in every CTA's receive area
-      const uint32_t dst_base = dsmem_map(slot, warp);
-      const uint32_t dst_bar = dsmem_map(&rbar[par], warp);
-      for (int ch = lane; ch < M::CHUNKS; ch += 32) {
-        uint32_t wds[4];
+      // the warp owning the CTA's best row stages and pushes it (warp 0 if none)
+      const int rl = (i != INT_MAX) ? i - rbeg : -1;
+      const int wo = rl >= 0 ? (rl % kLeafThreads) >> 5 : 0;
+      if (warp == wo) {
+        if (rl >= 0 && tid == rl % kLeafThreads) {
+          const int uo = rl / kLeafThreads;
 #pragma unroll
-        for (int e = 0; e < M::PER_CHUNK; ++e) {
-          const T x = msg_elem<T, W>(ch * M::PER_CHUNK + e, P, ldp, crow, jrow, v, i == INT_MAX ? -1 : i, jnan);
-          if constexpr (sizeof(T) == 8) {
-            const unsigned long long u = (unsigned long long)__double_as_longlong((double)x);
-            wds[2 * e] = (uint32_t)u;
-            wds[2 * e + 1] = (uint32_t)(u >> 32);
-          } else {
-            wds[e] = __float_as_uint((float)x);
-          }
+          for (int u = 0; u < RPT; ++u)
+            if (u == uo) {
+#pragma unroll
+              for (int c = 0; c < W; ++c) outc[4 + c] = x[u][c];
+            }
         }
-        st_async_16(dst_base + ch * 16, dst_bar, wds[0], wds[1], wds[2], wds[3]);
+        if (rl < 0 && lane < W) outc[4 + lane] = T(0);
+        if (lane == 0) {
+          outc[0] = rl >= 0 ? v : T(-1);
+          outc[1] = rl >= 0 ? T(i) : T(-1);
+          outc[2] = T(0);
+          outc[3] = T(0);
+        }
+        __syncwarp();
+        push_all<T, W>(outc, cand + ((size_t)par * 16 + q) * M::N, &rbar[par], C, lane);
+      }
+      // the warp owning row j pushes it
+      if (q == owner_j) {
+        const int rj = j - rbeg;
+        if (warp == ((rj % kLeafThreads) >> 5)) {
+          if (tid == rj % kLeafThreads) {
+            const int uj = rj / kLeafThreads;
+#pragma unroll
+            for (int u = 0; u < RPT; ++u)
+              if (u == uj) {
+#pragma unroll
+                for (int c = 0; c < W; ++c) outj[4 + c] = x[u][c];
+                const T d = x[u][j];
+                outj[0] = (d != d) ? T(1) : T(0);
+                outj[1] = T(0);
+                outj[2] = T(0);
+                outj[3] = T(0);
+              }
+          }
+          __syncwarp();
+          push_all<T, W>(outj, rowjb + (size_t)par * M::N, &rbar[par], C, lane);
+        }
       }
     }
-    // ---- wait for all C messages of this column ----
+    // ---- wait for the C candidates and row j ----
     if (!timed_out && !mbar_wait_spin(&rbar[par], (uint32_t)((j >> 1) & 1), status)) timed_out = true;
 
-    const T* rc = recv + (size_t)par * 16 * M::N;
+    const T* rc = cand + (size_t)par * 16 * M::N;
+    const T* rj = rowjb + (size_t)par * M::N;
     T v = lane < C ? rc[lane * M::N + 0] : T(-1);
     int i = lane < C ? (int)rc[lane * M::N + 1] : INT_MAX;
     if (i < 0) i = INT_MAX;
@@ -207,18 +245,16 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
       const int oq = __shfl_xor_sync(0xffffffffu, qw, o);
       if (better(ov, oi, v, i)) { v = ov; i = oi; qw = oq; }
     }
-    const int owner_j = j / rpc;
-    const T* jmsg = rc + owner_j * M::N;
     int p;
     const T* prow;
-    if (jmsg[2] != T(0) || i == INT_MAX || qw >= C) {
+    if (rj[0] != T(0) || i == INT_MAX || qw >= C) {
       p = j;
-      prow = jmsg + 4 + W;
+      prow = rj + 4;
     } else {
       p = i;
       prow = rc + qw * M::N + 4;
     }
-    const T* rowj = jmsg + 4 + W;
+    const T* rowj = rj + 4;
     const T piv = prow[j];
     if (tid == 0) hist[j] = p;
     if (q == 0 && tid == 0) {
@@ -226,7 +262,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
       if (piv == T(0)) atomicCAS(status + 1, 0, c0 + j + 1);
     }
 
-    // ---- swap, eliminate own rows, and scan column j+1 ----
+    // ---- swap, eliminate own rows in registers, scan column j+1 ----
     bv = T(-1);
     bi = INT_MAX;
 #pragma unroll
@@ -236,36 +272,37 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
         const int gr = rbeg + r;
         if (gr == j) {
 #pragma unroll
-          for (int c = 0; c < W; ++c) P[c * ldp + r] = prow[c];
+          for (int c = 0; c < W; ++c) x[u][c] = prow[c];
         } else if (gr == p) {
 #pragma unroll
-          for (int c = 0; c < W; ++c) P[c * ldp + r] = rowj[c];
+          for (int c = 0; c < W; ++c) x[u][c] = rowj[c];
         }
         if (gr > j) {
-          const T mult = P[j * ldp + r] / piv;
-          P[j * ldp + r] = mult;
+          const T mult = x[u][j] / piv;
+          x[u][j] = mult;
 #pragma unroll
-          for (int c = 1; c < W; ++c)
-            if (c > j && c < w) P[c * ldp + r] = fma(-mult, prow[c], P[c * ldp + r]);
+          for (int c = j + 1; c < W; ++c) x[u][c] = fma(-mult, prow[c], x[u][c]);
           if (j + 1 < w) {
-            const T a1 = absval(P[(j + 1) * ldp + r]);
+            const T a1 = absval(x[u][j + 1]);
             if (better(a1, gr, bv, bi)) { bv = a1; bi = gr; }
           }
         }
       }
     }
-    // the receive slot of this parity is reused two columns later; the
-    // barrier at the top of the next column orders these reads before any
-    // warp of this CTA pushes again, and senders cannot run two columns ahead.
+    // The buffers of this parity are rewritten two columns later; the
+    // barrier at the top of the next column orders these reads before this
+    // CTA pushes again, and no CTA can run two columns ahead of another.
   }
-  // Nobody may leave while others can still write into it or read from it.
+  // Nobody may leave while others can still write into it.
   cluster_sync_all();
-  {
-    const int total = rcnt * W;
-#pragma unroll 8
-    for (int i = tid; i < total; i += kLeafThreads) {
-      const int r = i / W, c = i % W;
-      if (c < w) A[(long long)(c0 + rbeg + r) * lda + c0 + c] = P[c * ldp + r];
+#pragma unroll
+  for (int u = 0; u < RPT; ++u) {
+    const int r = tid + u * kLeafThreads;
+    if (r < rcnt) {
+      T* dst = A + (long long)(c0 + rbeg + r) * lda + c0;
+#pragma unroll
+      for (int c = 0; c < W; ++c)
+        if (c < w) dst[c] = x[u][c];
     }
   }
   // This leaf's interchanges on the other columns of the enclosing panel
@@ -290,7 +327,6 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     }
     __syncthreads();
     const int m = *tm;
-    T* stage = P + (size_t)W * ldp;
     const long long total = (long long)m * ocols;
     const long long chunk = (total + C - 1) / C;
     const long long e0 = q * chunk, e1 = min(total, e0 + chunk);

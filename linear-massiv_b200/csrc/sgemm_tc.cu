@@ -1,0 +1,348 @@
+// FP32-storage GEMM on the 5th-generation tensor cores (tcgen05, kind::tf32),
+// the trailing-matrix contraction of the low-precision factorisation used by
+// iterative refinement:  C = alpha * A * Bt^T + beta * C,  all FP32 row-major,
+// A m x k and Bt n x k (both K-major), products in TF32, accumulation in FP32.
+//
+// One CTA per SM, persistent over 128 x 128 output tiles:
+//   warp 0      TMA producer: A / Bt k-slices (32 floats = one 128-byte
+//               swizzle row) into a 4-stage ring, and each tile's C block;
+//   warp 1      MMA issuer (one thread): 4 x tcgen05.mma (K = 8) per slice
+//               into a TMEM accumulator (two 128-column buffers, so the next
+//               tile's MMAs overlap this tile's epilogue); tcgen05.commit
+//               releases smem stages and hands accumulators to the epilogue;
+//   warps 2..5  epilogue: tcgen05.ld of their 32 TMEM lanes, C read from the
+//               TMA-loaded swizzled block, result written back in place and
+//               stored by one TMA bulk tensor store.
+// Every wait is bounded; on a timeout the kernel records the error, skips the
+// remaining work, and still frees its TMEM before exiting.  No multicast.
+#include "common.cuh"
+#include "internal.h"
+
+namespace lm {
+
+namespace {
+
+constexpr int TBM = 128, TBN = 128, TBK = 32;  // tile M, N; k-slice in floats (128 B)
+constexpr int T_A_BYTES = TBM * TBK * 4;   // 16 KB
+constexpr int T_B_BYTES = TBN * TBK * 4;   // 16 KB
+constexpr int T_C_BYTES = TBM * TBN * 4;   // 64 KB (4 boxes of 32 columns)
+constexpr int T_THREADS = 6 * 32;
+
+// SPLIT = 3xTF32: operands arrive as exactly-TF32 high parts and FP32
+// remainders; each k-step issues hi*hi + hi*lo + lo*hi, which restores close
+// to FP32 accuracy.  Stages hold 2 (plain) or 4 (split) operand tiles.
+template <bool SPLIT>
+struct TcCfg {
+  static constexpr int STAGES = SPLIT ? 2 : 4;
+  static constexpr int STAGE_BYTES = (T_A_BYTES + T_B_BYTES) * (SPLIT ? 2 : 1);
+  static constexpr int SMEM = STAGES * STAGE_BYTES + T_C_BYTES + 1024 + 256;
+};
+constexpr uint32_t T_TMEM_COLS = 256;      // 2 accumulators x 128 fp32 columns
+
+struct SgemmArgs {
+  int m, n, k;
+  float alpha, beta;
+  int tiles_m, tiles_n, num_tiles;
+  int* status;
+};
+
+// ---- tcgen05 / bulk-copy wrappers -------------------------------------------
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst_smem)),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrive on an mbarrier of this CTA when all previously issued tcgen05.mma of
+// this thread have completed.
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+// 32 lanes x 32 consecutive fp32 columns of TMEM into 32 registers per thread.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* tmap, const void* smem_src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                   reinterpret_cast<uint64_t>(tmap)),
+               "r"(x), "r"(y), "r"(smem_u32(smem_src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void named_bar(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+// K-major operand, 128-byte swizzle: 8-row core groups 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t smem_addr) {
+  return (uint64_t)((smem_addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// D f32, A/B tf32, both K-major, N = 128, M = 128.
+constexpr uint32_t kIdescTF32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TBN >> 3) << 17) |
+                                ((uint32_t)(TBM >> 4) << 24);
+
+// byte offset of element (r, c) in a [128 rows][32 floats] 128B-swizzled box
+__device__ __forceinline__ uint32_t cbox_off(int r, int c) {
+  return (uint32_t)(r * 128 + ((((c >> 2) ^ (r & 7))) << 4) + ((c & 3) << 2));
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(T_THREADS, 1)
+    sgemm_tf32_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+                      const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmAl,
+                      const __grid_constant__ CUtensorMap tmBl, SgemmArgs g) {
+  constexpr int TSTAGES = TcCfg<SPLIT>::STAGES;
+  constexpr int T_STAGE_BYTES = TcCfg<SPLIT>::STAGE_BYTES;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* smem =
+      reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // stage s: [A | B | A_lo | B_lo] (the last two only when SPLIT)
+  unsigned char* sA = smem;
+  unsigned char* sC = smem + TSTAGES * T_STAGE_BYTES;
+  uint64_t* full = reinterpret_cast<uint64_t*>(sC + T_C_BYTES);
+  uint64_t* empty = full + TSTAGES;
+  uint64_t* acc_full = empty + TSTAGES;   // [2]
+  uint64_t* acc_empty = acc_full + 2;     // [2]
+  uint64_t* c_full = acc_empty + 2;       // [1]
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(c_full + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int KT = (g.k + TBK - 1) / TBK;
+  const bool use_beta = g.beta != 0.0f;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < TSTAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], 4);
+    }
+    mbar_init(c_full, 1);
+    fence_barrier_init();
+  }
+  if (warp == 1) tmem_alloc(tmem_slot, T_TMEM_COLS);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+  bool ok = true;
+
+  if (warp == 0) {
+    // ---------------- TMA producer ----------------
+    if (lane == 0) {
+      tma_prefetch_desc(&tmA);
+      tma_prefetch_desc(&tmB);
+      int it = 0;
+      for (int t = blockIdx.x; t < g.num_tiles && ok; t += gridDim.x) {
+        const int tm = t % g.tiles_m, tn = t / g.tiles_m;
+        for (int kb = 0; kb < KT && ok; ++kb, ++it) {
+          const int s = it % TSTAGES;
+          const uint32_t ph = (uint32_t)((it / TSTAGES) & 1) ^ 1u;
+          if (!mbar_wait(&empty[s], ph, g.status)) { ok = false; break; }
+          mbar_arrive_expect_tx(&full[s], T_STAGE_BYTES);
+          unsigned char* st0 = sA + s * T_STAGE_BYTES;
+          tma_load_2d(st0, &tmA, kb * TBK, tm * TBM, &full[s]);
+          tma_load_2d(st0 + T_A_BYTES, &tmB, kb * TBK, tn * TBN, &full[s]);
+          if (SPLIT) {
+            tma_load_2d(st0 + T_A_BYTES + T_B_BYTES, &tmAl, kb * TBK, tm * TBM, &full[s]);
+            tma_load_2d(st0 + 2 * T_A_BYTES + T_B_BYTES, &tmBl, kb * TBK, tn * TBN, &full[s]);
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      int it = 0, lt = 0;
+      for (int t = blockIdx.x; t < g.num_tiles && ok; t += gridDim.x, ++lt) {
+        const int b = lt & 1;
+        const uint32_t dt = tbase + (uint32_t)(b * TBN);
+        if (!mbar_wait(&acc_empty[b], (uint32_t)(((lt >> 1) & 1) ^ 1), g.status)) { ok = false; break; }
+        tc_fence_after();
+        for (int kb = 0; kb < KT; ++kb, ++it) {
+          const int s = it % TSTAGES;
+          if (!mbar_wait(&full[s], (uint32_t)((it / TSTAGES) & 1), g.status)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + s * T_STAGE_BYTES);
+          const uint32_t b0 = a0 + T_A_BYTES;
+#pragma unroll
+          for (int kk = 0; kk < TBK / 8; ++kk) {
+            tc_mma_tf32(dt, sw128_kmajor_desc(a0 + kk * 32), sw128_kmajor_desc(b0 + kk * 32), kIdescTF32,
+                        (kb > 0 || kk > 0) ? 1u : 0u);
+            if (SPLIT) {
+              const uint32_t al = b0 + T_B_BYTES, bl = al + T_A_BYTES;
+              tc_mma_tf32(dt, sw128_kmajor_desc(a0 + kk * 32), sw128_kmajor_desc(bl + kk * 32), kIdescTF32, 1u);
+              tc_mma_tf32(dt, sw128_kmajor_desc(al + kk * 32), sw128_kmajor_desc(b0 + kk * 32), kIdescTF32, 1u);
+            }
+          }
+          tc_commit(&empty[s]);  // smem stage free once these MMAs have read it
+        }
+        if (!ok) break;
+        tc_commit(&acc_full[b]);  // accumulator complete
+      }
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5, TMEM lane quarter = warp % 4) ----------------
+    const int quarter = warp & 3;
+    const int row_in_tile = quarter * 32 + lane;
+    const bool leader = (warp == 2 && lane == 0);
+    int lt = 0;
+    for (int t = blockIdx.x; t < g.num_tiles; t += gridDim.x, ++lt) {
+      const int tm = t % g.tiles_m, tn = t / g.tiles_m;
+      const int b = lt & 1;
+      if (ok && use_beta && leader) {
+        bulk_wait_read0();  // the previous tile's store has finished reading sC
+        mbar_arrive_expect_tx(c_full, T_C_BYTES);
+#pragma unroll
+        for (int q = 0; q < TBN / 32; ++q) tma_load_2d(sC + q * (TBM * 128), &tmC, tn * TBN + q * 32, tm * TBM, c_full);
+      }
+      if (ok && !mbar_wait(&acc_full[b], (uint32_t)((lt >> 1) & 1), g.status)) ok = false;
+      if (ok && use_beta && !mbar_wait(c_full, (uint32_t)(lt & 1), g.status)) ok = false;
+      if (!use_beta && leader) bulk_wait_read0();
+      named_bar(1, 128);  // C block present (or free) for all epilogue warps
+      tc_fence_after();
+      if (ok) {
+#pragma unroll 1
+        for (int q = 0; q < TBN / 32; ++q) {
+          float acc[32];
+          tmem_ld32(tbase + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * TBN + q * 32), acc);
+          unsigned char* box = sC + q * (TBM * 128);
+#pragma unroll
+          for (int c4 = 0; c4 < 8; ++c4) {
+            float4* p = reinterpret_cast<float4*>(box + cbox_off(row_in_tile, c4 * 4));
+            float4 o = use_beta ? *p : make_float4(0.f, 0.f, 0.f, 0.f);
+            o.x = fmaf(g.alpha, acc[c4 * 4 + 0], use_beta ? g.beta * o.x : 0.f);
+            o.y = fmaf(g.alpha, acc[c4 * 4 + 1], use_beta ? g.beta * o.y : 0.f);
+            o.z = fmaf(g.alpha, acc[c4 * 4 + 2], use_beta ? g.beta * o.z : 0.f);
+            o.w = fmaf(g.alpha, acc[c4 * 4 + 3], use_beta ? g.beta * o.w : 0.f);
+            *p = o;
+          }
+        }
+      }
+      tc_fence_before();
+      if (lane == 0) mbar_arrive(&acc_empty[b]);  // TMEM buffer may be overwritten
+      fence_proxy_async_smem();                  // smem writes visible to the TMA store
+      named_bar(1, 128);
+      if (ok && leader) {
+#pragma unroll
+        for (int q = 0; q < TBN / 32; ++q) tma_store_2d(&tmC, sC + q * (TBM * 128), tn * TBN + q * 32, tm * TBM);
+        bulk_commit();
+      }
+    }
+    if (leader) bulk_wait0();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tbase, T_TMEM_COLS);
+  }
+}
+
+}  // namespace
+
+void count_launch(int n);
+
+int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
+               long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
+               const float* Btlo) {
+  if (m <= 0 || n <= 0) return LM_OK;
+  if (k <= 0) return LM_ERR_ARG;
+  const bool split = Alo != nullptr && Btlo != nullptr;
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(Bt) | reinterpret_cast<uintptr_t>(C) |
+       reinterpret_cast<uintptr_t>(Alo) | reinterpret_cast<uintptr_t>(Btlo)) & 15)
+    return LM_ERR_UNSUPPORTED;
+  if ((lda | ldb | ldc) & 3) return LM_ERR_UNSUPPORTED;  // 16-byte row strides for TMA
+  static bool attr_set[2][kMaxDevices] = {};
+  const int dev = ctx_device(ctx);
+  if (!attr_set[split][dev]) {
+    if (split)
+      LM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tf32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcCfg<true>::SMEM));
+    else
+      LM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tf32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcCfg<false>::SMEM));
+    attr_set[split][dev] = true;
+  }
+  CUtensorMap tA, tB, tC, tAl, tBl;
+  LM_TRY(make_tmap_2d(&tA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, lda, TBK, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
+  LM_TRY(make_tmap_2d(&tB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Bt, k, n, ldb, TBK, TBN, CU_TENSOR_MAP_SWIZZLE_128B));
+  LM_TRY(make_tmap_2d(&tC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, n, m, ldc, 32, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
+  if (split) {
+    LM_TRY(make_tmap_2d(&tAl, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Alo, k, m, lda, TBK, TBM,
+                        CU_TENSOR_MAP_SWIZZLE_128B));
+    LM_TRY(make_tmap_2d(&tBl, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Btlo, k, n, ldb, TBK, TBN,
+                        CU_TENSOR_MAP_SWIZZLE_128B));
+  } else {
+    tAl = tA;
+    tBl = tB;
+  }
+  SgemmArgs g;
+  g.m = m; g.n = n; g.k = k; g.alpha = alpha; g.beta = beta;
+  g.tiles_m = cdiv(m, TBM);
+  g.tiles_n = cdiv(n, TBN);
+  g.num_tiles = g.tiles_m * g.tiles_n;
+  g.status = ctx_status(ctx);
+  const int grid = std::min(g.num_tiles, ctx_num_sms(ctx));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid, 1, 1);
+  cfg.blockDim = dim3(T_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = split ? TcCfg<true>::SMEM : TcCfg<false>::SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;  // explicit 1-CTA clusters for the shared::cluster forms
+  attr[0].val.clusterDim.x = 1;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  {
+    Prof prof(ctx, kPhaseGemm, 2.0 * m * n * k * (split ? 3 : 1),
+              4.0 * ((double)m * k + (double)n * k) * (split ? 2 : 1) + 8.0 * m * n, st);
+    if (split)
+      LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, sgemm_tf32_kernel<true>, tA, tB, tC, tAl, tBl, g));
+    else
+      LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, sgemm_tf32_kernel<false>, tA, tB, tC, tAl, tBl, g));
+  }
+  count_launch(1);
+  return LM_OK;
+}
+
+}  // namespace lm

@@ -38,6 +38,7 @@ EXPORTS = [
     "lm_dgetrf", "lm_dgetrs", "lm_dgesv", "lm_dpotrf", "lm_dpotrs", "lm_dposv",
     "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
     "lm_lu_host", "lm_cholesky_host", "lm_det_host", "lm_ipiv_to_perm", "lm_dresidual",
+    "lm_dgesv_ir", "lm_lu_solve_ir_host",
 ]
 
 
@@ -102,6 +103,8 @@ def _lib():
                 "lm_det_host": ([vp, i, dp, dp], i),
                 "lm_ipiv_to_perm": ([i, ip, ip], i),
                 "lm_dresidual": ([vp, i, i, vp, i, vp, i, vp, i, vp, i], i),
+                "lm_dgesv_ir": ([vp, i, i, vp, i, vp, i, vp, i, d, i, ip, dp, ip], i),
+                "lm_lu_solve_ir_host": ([vp, i, i, dp, dp, dp, d, i, ip, dp, ip], i),
             }
             for name, (args, res) in sigs.items():
                 fn = getattr(L, name)
@@ -335,6 +338,27 @@ def ipiv_to_perm(ipiv):
     for k, p in enumerate(ipiv):
         perm[k], perm[p] = perm[p], perm[k]
     return perm
+
+
+def luSolveIR(A, b, tol: float = 0.0, max_iter: int = 30, ctx: Context | None = None):
+    """Mixed-precision luSolve: FP32/TF32 LU refined in FP64.
+
+    Returns (x, iterations, backward_error, status); status is 0, info > 0
+    for a zero FP32 pivot, or LM_ERR_NOT_CONVERGED (x is the last iterate).
+    """
+    import torch
+
+    ctx = ctx or default_context(A.device.index or 0)
+    B, vec = _as_cols(b)
+    B = B.contiguous()
+    X = torch.empty_like(B)
+    it, be, info = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_int(0)
+    st = _lib().lm_dgesv_ir(ctx.h, A.shape[0], B.shape[1], _ptr(A), A.stride(0), _ptr(B), B.stride(0), _ptr(X),
+                            X.stride(0), float(tol), int(max_iter), ctypes.byref(it), ctypes.byref(be),
+                            ctypes.byref(info))
+    if st < 0 and st != LM_ERR_NOT_CONVERGED:
+        raise LMError(st, "lm_dgesv_ir")
+    return (X[:, 0] if vec else X), it.value, be.value, st
 
 
 # ---- host-buffer entry points (what a pure FFI binding calls) -----------------
