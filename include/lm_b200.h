@@ -174,6 +174,21 @@ int lm_dgesv_ir(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const do
 int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X, double tol,
                         int max_iter, int* iters, double* berr, int* info);
 
+/* ---- factorisation without allocation -----------------------------------------
+ * No counterpart in the reference.  lm_dpotrf without any allocation: for
+ * callers that cannot call cudaMalloc at call time (a runtime whose memory
+ * pool owns every allocation, a real-time loop that forbids allocation, a
+ * plugin host that only hands out pre-registered buffers).  Same result as
+ * lm_dpotrf on `stream` (cudaStream_t as void*, 0 = legacy default stream),
+ * on the current device, synchronising to report info.  Its scratch is one
+ * static device array of the library, about 4.3 MB held by every GPU that
+ * loads the library until exit; it limits n to 4096 (larger n returns
+ * LM_ERR_ARG) and needs A 16-byte aligned with an even lda.  The first call
+ * on a device looks up the array's device address: make that call before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+int lm_dpotrf_noalloc(void* stream, int n, double* A, int lda, int* info);
+
 /* ---- residual (IR and the reference's scaled residual) ---------------------
  * R = B - A X in FP64 (device), n x nrhs; replaces matvec / rawGemv
  * (L2.hs:123-144, K.hs:119-134) on the refinement path. */

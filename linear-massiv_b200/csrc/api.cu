@@ -245,6 +245,21 @@ int run_graphed(Ctx& c, const std::string& key0, F&& body) {
   return LM_OK;
 }
 
+int dpotrf_borrowed(int device, int num_sms, cudaStream_t st, int n, double* A, long long lda, int* d_status,
+                    void* scratch, size_t scratch_bytes) {
+  Ctx c;
+  c.device = device;
+  c.num_sms = num_sms;
+  c.stream = st;
+  c.graphs = false;
+  c.d_status = d_status;
+  c.ws[1] = scratch;  // grow-only workspace that never needs to grow
+  c.ws_bytes[1] = scratch_bytes;
+  const int r = dpotrf(c, n, A, lda, st);
+  c.ws[1] = nullptr;  // borrowed: nothing to free
+  return r;
+}
+
 std::string gkey(const char* op, std::initializer_list<long long> v) {
   std::string k(op);
   for (long long x : v) k += "," + std::to_string(x);

@@ -119,6 +119,11 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
              long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
              const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner);
 
+// Run dpotrf with caller-provided device scratch (workspace slot 1) and
+// status words instead of a context's own allocations (api.cu).
+int dpotrf_borrowed(int device, int num_sms, cudaStream_t st, int n, double* A, long long lda, int* d_status,
+                    void* scratch, size_t scratch_bytes);
+
 // r = b - A x for nrhs columns (FP64), and max-norm helpers (resid.cu).
 int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* X, long long ldx,
               const double* B, long long ldb, double* R, long long ldr, cudaStream_t st);

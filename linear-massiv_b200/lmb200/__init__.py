@@ -38,7 +38,7 @@ EXPORTS = [
     "lm_dgetrf", "lm_dgetrs", "lm_dgesv", "lm_dpotrf", "lm_dpotrs", "lm_dposv",
     "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
     "lm_lu_host", "lm_cholesky_host", "lm_det_host", "lm_ipiv_to_perm", "lm_dresidual",
-    "lm_dgesv_ir", "lm_lu_solve_ir_host",
+    "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_dpotrf_noalloc",
 ]
 
 
@@ -105,6 +105,7 @@ def _lib():
                 "lm_dresidual": ([vp, i, i, vp, i, vp, i, vp, i, vp, i], i),
                 "lm_dgesv_ir": ([vp, i, i, vp, i, vp, i, vp, i, d, i, ip, dp, ip], i),
                 "lm_lu_solve_ir_host": ([vp, i, i, dp, dp, dp, d, i, ip, dp, ip], i),
+                "lm_dpotrf_noalloc": ([vp, i, vp, i, ip], i),
             }
             for name, (args, res) in sigs.items():
                 fn = getattr(L, name)
