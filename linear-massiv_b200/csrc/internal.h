@@ -40,6 +40,20 @@ int make_tmap_2d(CUtensorMap* tm, CUtensorMapDataType dt, int elem_bytes, const 
                  long long inner, long long outer, long long ld, int box_inner, int box_outer,
                  CUtensorMapSwizzle swz);
 
+// --- few-rhs persistent substitutions (trsv.cu) ------------------------------
+// Elements of one factor's diagonal-block inverses for order n.
+template <typename T>
+size_t trsv_inv_elems(int n);
+// DinvL / DinvU <- inverses of the diagonal blocks of the packed LU factor's
+// unit-lower L and upper U (16-byte aligned, trsv_inv_elems<T>(n) each).
+template <typename T>
+int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaStream_t st);
+// X (n x nrhs, nrhs <= 4) <- U^-1 L^-1 X in two persistent launches; `sync`
+// is 4 ints of device scratch.
+template <typename T>
+int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
+            int* sync, int* status, cudaStream_t st);
+
 // --- FP64 GEMM (dgemm.cu) ----------------------------------------------------
 // C = alpha * op(A) * op(B) + beta * C, row-major.
 //   a_trans = false: A is m x k (lda)  | true: A^T is stored, k x m (lda)

@@ -27,6 +27,7 @@ int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long 
                long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
                const float* Btlo);
 
+
 namespace {
 
 constexpr int kNB = 128;
@@ -277,15 +278,22 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   const size_t piv_bytes = sizeof(int) * (size_t)((n + 63) / 64 * 64);
   const size_t r_bytes = sizeof(double) * (size_t)n * ldr;
   const size_t d_bytes = sizeof(float) * (size_t)n * ldr;
-  const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(1 + 3 * 64);
+  const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(2 + 3 * 64);  // 16-byte multiple
+  const size_t inv_elems = trsv_inv_elems<float>(n);
+  const size_t inv_bytes = 2 * sizeof(float) * inv_elems;  // diagonal-block inverses of L and U
+  const size_t sync_bytes = 64;
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes, &ws));
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + sync_bytes, &ws));
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   int* ipiv = reinterpret_cast<int*>(p + a32_bytes);
   double* R = reinterpret_cast<double*>(p + a32_bytes + piv_bytes);
   float* D = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes);
   unsigned long long* nrm = reinterpret_cast<unsigned long long*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes);
+  float* DinvL = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes);
+  float* DinvU = DinvL + inv_elems;
+  int* tsync = reinterpret_cast<int*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes);
+  const bool fast_trsv = nrhs <= 4;
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
 
   // ||A||_inf and ||B_c||_inf (FP64, from the original data)
@@ -296,7 +304,9 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   // factor fl32(A)
   LM_TRY(factor_runner([&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
-    return sgetrf(c, n, A32, lda32, ipiv, s);
+    LM_TRY(sgetrf(c, n, A32, lda32, ipiv, s));
+    if (!fast_trsv) return LM_OK;
+    return tri_inv_blocks<float>(A32, lda32, n, DinvL, DinvU, s);
   }));
   // x = 0, r = b
   LM_CUDA_TRY(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * nrhs, n, st));
@@ -306,7 +316,16 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   double worst = 0.0;
   for (it = 1; it <= max_iter; ++it) {
     LM_TRY(convert_d2s(D, ldr, R, ldr, n, nrhs, st));
-    LM_TRY(sgetrs(c, n, nrhs, A32, lda32, ipiv, D, ldr, st));
+    if (fast_trsv) {
+      {
+        Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, st);
+        LM_TRY(laswp<float>(D, ldr, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+      }
+      Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, st);
+      LM_TRY(trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, D, ldr, tsync, ctx_status(c), st));
+    } else {
+      LM_TRY(sgetrs(c, n, nrhs, A32, lda32, ipiv, D, ldr, st));
+    }
     add_s2d_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, D, ldr, n, nrhs);
     count_launch(1);
     LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, st));

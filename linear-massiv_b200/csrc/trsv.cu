@@ -1,0 +1,291 @@
+// Triangular solves with few right-hand sides as one persistent launch per
+// direction (the refinement loop's substitutions; counterpart of the packed
+// substitutions rawForwardSubUnitPackedSIMD / rawBackSubPackedSIMD,
+// K.hs:2205-2314).
+//
+//   tri_inv_blocks : inverts every BS x BS diagonal block of L (unit lower)
+//                    and U (upper) once per factorisation;
+//   trsv_kernel    : row-block b (taken in dependency order through an atomic
+//                    ticket, so a block only ever waits on blocks that are
+//                    already running) accumulates  y_b = rhs_b - sum_j T_bj x_j
+//                    over its dependencies in the order they complete, then
+//                    x_b = inv(T_bb) y_b, publishes x_b and advances the
+//                    direction's progress counter (blocks finish in ticket
+//                    order, so one counter says which x_j are ready).
+// Each T_bj tile is constant and is loaded before waiting on x_j; the
+// right-hand side and inv(T_bb) are loaded before the first wait.  Every wait
+// is bounded (kSpinLimit polls, then LM_DEVERR_TIMEOUT).
+//
+// Block size: 128 rows for FP32 (512 threads), 64 for FP64 (256 threads; the
+// inversion's two 128 x 129 FP64 tiles would not fit in shared memory).
+// Thread (r, q) of a block owns row r and, of every tile, the float4/double2
+// groups at columns 16 v + 4 q (FP32) so that the four threads of a row read
+// 64 contiguous bytes per load instruction.
+#include "common.cuh"
+#include "internal.h"
+
+namespace lm {
+
+void count_launch(int n);
+
+namespace {
+
+constexpr int MAX_RHS = 4;
+
+template <typename T>
+struct TrsvCfg;
+template <>
+struct TrsvCfg<float> {
+  static constexpr int BS = 128, NT = 512, VEC = 4;  // VEC elements per 16-byte load
+};
+template <>
+struct TrsvCfg<double> {
+  static constexpr int BS = 64, NT = 256, VEC = 2;
+};
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+template <typename T>
+__device__ __forceinline__ T ld_volatile(const T* p) {
+  return *reinterpret_cast<const volatile T*>(p);
+}
+
+// inv of the b-th diagonal block of the unit-lower (lower = 1) or upper
+// (lower = 0) factor, row-major BS x BS into Dinv + b * BS * BS.
+template <typename T>
+__global__ void __launch_bounds__(TrsvCfg<T>::NT) tri_inv_blocks_kernel(const T* __restrict__ LU, long long lda,
+                                                                       int n, int lower, T* Dinv) {
+  constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, RG = NT / BS;
+  extern __shared__ __align__(16) unsigned char inv_smem[];
+  T(*Ts)[BS + 1] = reinterpret_cast<T(*)[BS + 1]>(inv_smem);
+  T(*Xs)[BS + 1] = Ts + BS;
+  const int b = blockIdx.x;
+  const int r0 = b * BS;
+  const int w = min(BS, n - r0);
+  for (int i = threadIdx.x; i < BS * BS; i += NT) {
+    const int r = i / BS, c = i % BS;
+    T t = T(0);
+    if (r < w && c < w) {
+      const T v = LU[(long long)(r0 + r) * lda + r0 + c];
+      if (lower)
+        t = (c < r) ? v : (c == r ? T(1) : T(0));
+      else
+        t = (c >= r) ? v : T(0);
+    } else if (r == c) {
+      t = T(1);  // pad the last block with the identity
+    }
+    Ts[r][c] = t;
+    Xs[r][c] = (r == c) ? T(1) : T(0);
+  }
+  __syncthreads();
+  const int c = threadIdx.x % BS;   // column of X this thread updates
+  const int rg = threadIdx.x / BS;  // row group
+  if (lower) {
+    for (int k = 0; k < BS; ++k) {  // rows i > k:  X[i] -= L[i][k] X[k]
+      const T xk = Xs[k][c];
+      for (int i = k + 1 + ((rg - (k + 1)) % RG + RG) % RG; i < BS; i += RG) Xs[i][c] = fma(-Ts[i][k], xk, Xs[i][c]);
+      __syncthreads();
+    }
+  } else {
+    for (int k = BS - 1; k >= 0; --k) {  // X[k] /= U[k][k]; rows i < k: X[i] -= U[i][k] X[k]
+      if (threadIdx.x < BS) Xs[k][threadIdx.x] = Xs[k][threadIdx.x] / Ts[k][k];
+      __syncthreads();
+      const T xk = Xs[k][c];
+      for (int i = rg; i < k; i += RG) Xs[i][c] = fma(-Ts[i][k], xk, Xs[i][c]);
+      __syncthreads();
+    }
+  }
+  T* D = Dinv + (size_t)b * BS * BS;
+  for (int i = threadIdx.x; i < BS * BS; i += NT) D[i] = Xs[i / BS][i % BS];
+}
+
+// Loads this thread's share of a BS-wide slice of row `src` (columns c0 ..):
+// groups of VEC at c0 + 4 VEC v + VEC q, v = 0 .. BS/(4 VEC) - 1.
+template <typename T>
+__device__ __forceinline__ void load_row_share(T* out, const T* src, int c0, int q, int n, bool row_ok,
+                                               bool vec_ok) {
+  constexpr int BS = TrsvCfg<T>::BS, VEC = TrsvCfg<T>::VEC, G = BS / (4 * VEC);
+#pragma unroll
+  for (int v = 0; v < G; ++v) {
+    const int c = c0 + 4 * VEC * v + VEC * q;
+    if (vec_ok && row_ok && c + VEC <= n) {
+      if constexpr (VEC == 4) {
+        const float4 x = *reinterpret_cast<const float4*>(src + c);
+        out[4 * v] = x.x, out[4 * v + 1] = x.y, out[4 * v + 2] = x.z, out[4 * v + 3] = x.w;
+      } else {
+        const double2 x = *reinterpret_cast<const double2*>(src + c);
+        out[2 * v] = x.x, out[2 * v + 1] = x.y;
+      }
+    } else {
+#pragma unroll
+      for (int e = 0; e < VEC; ++e) out[VEC * v + e] = (row_ok && c + e < n) ? src[c + e] : T(0);
+    }
+  }
+}
+
+// One direction of the blocked substitution.  forward: L unit lower, blocks in
+// increasing order; backward: U upper, blocks in decreasing order.
+// sync[0] = progress counter, sync[1] = ticket dispenser (both zero at launch).
+template <typename T>
+__global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
+                                                             int nrhs, int forward, const T* __restrict__ Dinv,
+                                                             T* X, long long ldx, int* sync, int* status,
+                                                             int vec_ok) {
+  constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
+  static_assert(NT == 4 * BS, "four threads per row");
+  __shared__ int tk_sh, prog_sh;
+  __shared__ T xj[2][BS][MAX_RHS];
+  __shared__ T ys[BS][MAX_RHS];
+  const int nb = (n + BS - 1) / BS;
+  if (threadIdx.x == 0) tk_sh = atomicAdd(sync + 1, 1);
+  __syncthreads();
+  const int t = tk_sh;
+  const int b = forward ? t : nb - 1 - t;
+  const int r0 = b * BS;
+  const int rows = min(BS, n - r0);
+  const int r = threadIdx.x >> 2, q = threadIdx.x & 3;
+  const bool row_ok = r < rows;
+  // column index of the e-th element of this thread's share
+  auto col_of = [&](int e) { return 4 * VEC * (e / VEC) + VEC * q + (e % VEC); };
+
+  T rhs[MAX_RHS];
+#pragma unroll
+  for (int h = 0; h < MAX_RHS; ++h) rhs[h] = (q == 0 && row_ok && h < nrhs) ? X[(long long)(r0 + r) * ldx + h] : T(0);
+  T dv[CP];
+  load_row_share<T>(dv, Dinv + (size_t)b * BS * BS + (size_t)r * BS, 0, q, BS, true, true);
+
+  T acc[MAX_RHS];
+#pragma unroll
+  for (int h = 0; h < MAX_RHS; ++h) acc[h] = T(0);
+  const int ndep = forward ? b : nb - 1 - b;  // dependencies = tickets 0 .. t-1
+  int known = 0;
+  bool ok = true;
+  for (int d = 0; d < ndep; ++d) {
+    const int j = forward ? d : nb - 1 - d;  // ticket d, in completion order
+    T tv[CP];
+    load_row_share<T>(tv, LU + (long long)(r0 + r) * lda, j * BS, q, n, row_ok, vec_ok != 0);
+    if (d >= known) {
+      if (threadIdx.x == 0) {
+        int p = ld_acquire(sync);
+        for (uint32_t it = 0; ok && p <= d; p = ld_acquire(sync))
+          if (++it > kSpinLimit) {
+            atomicCAS(status, 0, LM_DEVERR_TIMEOUT);
+            ok = false;
+          }
+        prog_sh = ok ? p : nb;  // on timeout, run to the end without waiting
+      }
+      __syncthreads();
+      known = prog_sh;
+    }
+    T(*xs)[MAX_RHS] = xj[d & 1];
+    for (int i = threadIdx.x; i < BS * nrhs; i += NT) {
+      const int rr = i / nrhs, h = i % nrhs;
+      const int row = j * BS + rr;
+      xs[rr][h] = row < n ? ld_volatile(X + (long long)row * ldx + h) : T(0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < CP; ++e) {
+      const int cc = col_of(e);
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h)
+        if (h < nrhs) acc[h] = fma(tv[e], xs[cc][h], acc[h]);
+    }
+    // xj is double-buffered: the next write to this buffer comes after the
+    // next iteration's barrier, which every thread reaches after this FMA.
+  }
+  // y = rhs - T_b,dep x_dep  (the four lanes of a row are adjacent)
+#pragma unroll
+  for (int h = 0; h < MAX_RHS; ++h) {
+    acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 1);
+    acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 2);
+  }
+  if (q == 0)
+#pragma unroll
+    for (int h = 0; h < MAX_RHS; ++h) ys[r][h] = row_ok ? rhs[h] - acc[h] : T(0);
+  __syncthreads();
+  // x_b = inv(T_bb) y
+#pragma unroll
+  for (int h = 0; h < MAX_RHS; ++h) acc[h] = T(0);
+#pragma unroll
+  for (int e = 0; e < CP; ++e) {
+    const int cc = col_of(e);
+#pragma unroll
+    for (int h = 0; h < MAX_RHS; ++h)
+      if (h < nrhs) acc[h] = fma(dv[e], ys[cc][h], acc[h]);
+  }
+#pragma unroll
+  for (int h = 0; h < MAX_RHS; ++h) {
+    acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 1);
+    acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 2);
+  }
+  if (q == 0 && row_ok)
+#pragma unroll
+    for (int h = 0; h < MAX_RHS; ++h)
+      if (h < nrhs) X[(long long)(r0 + r) * ldx + h] = acc[h];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    st_release(sync, t + 1);
+  }
+}
+
+}  // namespace
+
+template <typename T>
+size_t trsv_inv_elems(int n) {
+  constexpr int BS = TrsvCfg<T>::BS;
+  return (size_t)((n + BS - 1) / BS) * BS * BS;
+}
+
+// Inverses of the diagonal blocks of L (unit lower) and U of a packed LU
+// factor: DinvL and DinvU each hold trsv_inv_elems<T>(n) elements.
+template <typename T>
+int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaStream_t st) {
+  constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT;
+  if (n <= 0) return LM_OK;
+  const int nb = (n + BS - 1) / BS;
+  const int smem = (int)(2 * BS * (BS + 1) * sizeof(T));
+  LM_CUDA_TRY(cudaFuncSetAttribute(tri_inv_blocks_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  tri_inv_blocks_kernel<T><<<nb, NT, smem, st>>>(LU, lda, n, 1, DinvL);
+  tri_inv_blocks_kernel<T><<<nb, NT, smem, st>>>(LU, lda, n, 0, DinvU);
+  count_launch(2);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+// X (n x nrhs, nrhs <= 4) <- U^-1 L^-1 X with the packed factor and its block
+// inverses; `sync` holds 4 ints of device scratch.
+template <typename T>
+int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
+            int* sync, int* status, cudaStream_t st) {
+  constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC;
+  if (nrhs > MAX_RHS) return LM_ERR_UNSUPPORTED;
+  if (n <= 0 || nrhs <= 0) return LM_OK;
+  if (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16) return LM_ERR_ARG;
+  const int nb = (n + BS - 1) / BS;
+  const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
+  LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
+  trsv_kernel<T><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok);
+  trsv_kernel<T><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok);
+  count_launch(2);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+template size_t trsv_inv_elems<float>(int);
+template size_t trsv_inv_elems<double>(int);
+template int tri_inv_blocks<float>(const float*, long long, int, float*, float*, cudaStream_t);
+template int tri_inv_blocks<double>(const double*, long long, int, double*, double*, cudaStream_t);
+template int trsv_lu<float>(const float*, long long, int, int, const float*, const float*, float*, long long, int*,
+                            int*, cudaStream_t);
+template int trsv_lu<double>(const double*, long long, int, int, const double*, const double*, double*, long long,
+                             int*, int*, cudaStream_t);
+
+}  // namespace lm

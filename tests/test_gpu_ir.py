@@ -64,3 +64,18 @@ def test_ir_uniform_matrix(ctx):
     x, iters, berr, st = lmb200.luSolveIR(dev(A), dev(b), ctx=ctx)
     assert st == 0 and berr <= 1e-15 * n
     assert backward_error(A, x.cpu().numpy(), b) <= 1e-15 * n
+
+
+@pytest.mark.parametrize("n,nrhs", [(65, 2), (1000, 3), (4097, 4), (4100, 1)])
+def test_ir_few_rhs_persistent_substitution(ctx, n, nrhs):
+    """nrhs <= 4 runs the substitutions as one persistent launch per direction
+    (64-row blocks with inverted diagonal blocks); ragged last blocks included."""
+    g = philox(9300 + n + nrhs)
+    A = gen_randsvd(g, n, 1e2, -1.0, 1.0)
+    B = g.uniform(-1, 1, (n, nrhs))
+    X, iters, berr, st = lmb200.luSolveIR(dev(A), dev(B), ctx=ctx)
+    assert st == 0 and berr <= 1e-15 * n, f"status {st}, {iters} iterations, berr {berr}"
+    Xn = X.cpu().numpy()
+    assert backward_error(A, Xn, B) <= 1e-15 * n
+    Xo, _, _ = O.lu_solve_p(A, B)
+    assert rel_forward(Xn, Xo) <= max(1e-12, 8 * 1e2 * 1e-15 * n)
