@@ -14,7 +14,9 @@
 //   mathematics as the reference's left-looking panelCholFactor
 //   (Chol.hs:279-321), different association.
 // dgetrs / dpotrs — blocked substitutions: a 128 x 128 triangular block
-//   solve, then the rest of the right-hand side updated by GEMM.
+//   solve, then the rest of the right-hand side updated by GEMM; dgetrs with
+//   at most 4 right-hand sides runs one persistent launch per direction
+//   (trsv.cu).
 #include <algorithm>
 
 #include "common.cuh"
@@ -187,6 +189,17 @@ int forward_blocked(Ctx& c, int n, int nrhs, const double* M, long long ldm, boo
 
 int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* ipiv, double* B,
            long long ldb, cudaStream_t st) {
+  if (nrhs <= 4) {
+    // few right-hand sides: P b, then one persistent launch per direction
+    void* ws = nullptr;
+    LM_TRY(ctx_workspace(c, 2, 64, &ws));
+    {
+      Prof p(c, kPhaseSwap, 0.0, 32.0 * n * nrhs, st);
+      LM_TRY(laswp<double>(B, ldb, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+    }
+    Prof p(c, kPhaseTrsm, 2.0 * n * n * nrhs, 8.0 * n * n, st);
+    return trsv_lu<double>(LU, lda, n, nrhs, nullptr, nullptr, B, ldb, static_cast<int*>(ws), ctx_status(c), st);
+  }
   SolveBufs sb;
   LM_TRY(solve_bufs(c, n, nrhs, LU, lda, B, ldb, sb, st));
   // P b (applyPivotsForward, LU.hs:493-507)

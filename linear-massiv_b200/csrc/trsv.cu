@@ -16,8 +16,13 @@
 // right-hand side and inv(T_bb) are loaded before the first wait.  Every wait
 // is bounded (kSpinLimit polls, then LM_DEVERR_TIMEOUT).
 //
-// Block size: 128 rows for FP32 (512 threads), 64 for FP64 (256 threads; the
-// inversion's two 128 x 129 FP64 tiles would not fit in shared memory).
+// Diagonal blocks: FP32 multiplies by the precomputed inverse (the refinement
+// loop absorbs its rounding); FP64, the drop-in path, solves the diagonal block
+// by substitution in one warp (column sweep over a shared-memory copy of
+// T_bb), so its accuracy is that of the reference's substitutions
+// (LU.hs:493-507, K.hs:2205-2314) rather than that of an explicit inverse.
+//
+// Block size: 128 rows for FP32 (512 threads), 64 for FP64 (256 threads).
 // Thread (r, q) of a block owns row r and, of every tile, the float4/double2
 // groups at columns 16 v + 4 q (FP32) so that the four threads of a row read
 // 64 contiguous bytes per load instruction.
@@ -37,11 +42,23 @@ struct TrsvCfg;
 template <>
 struct TrsvCfg<float> {
   static constexpr int BS = 128, NT = 512, VEC = 4;  // VEC elements per 16-byte load
+  static constexpr bool EXACT = false;               // diagonal block by its inverse
 };
 template <>
 struct TrsvCfg<double> {
   static constexpr int BS = 64, NT = 256, VEC = 2;
+  static constexpr bool EXACT = true;                // diagonal block by substitution
 };
+
+// Shared memory of trsv_kernel: the diagonal block only when it is solved by
+// substitution.
+template <typename T, bool EXACT>
+struct TrsvDiag {
+  T t[TrsvCfg<T>::BS][TrsvCfg<T>::BS + 1];
+  T rdiag[TrsvCfg<T>::BS];  // 1 / T_kk, formed before the first wait
+};
+template <typename T>
+struct TrsvDiag<T, false> {};
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -138,10 +155,13 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
                                                              T* X, long long ldx, int* sync, int* status,
                                                              int vec_ok) {
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
+  constexpr bool EXACT = TrsvCfg<T>::EXACT;
   static_assert(NT == 4 * BS, "four threads per row");
+  static_assert(!EXACT || BS == 64, "the one-warp substitution holds two rows per lane");
   __shared__ int tk_sh, prog_sh;
   __shared__ T xj[2][BS][MAX_RHS];
   __shared__ T ys[BS][MAX_RHS];
+  __shared__ TrsvDiag<T, EXACT> diag;
   const int nb = (n + BS - 1) / BS;
   if (threadIdx.x == 0) tk_sh = atomicAdd(sync + 1, 1);
   __syncthreads();
@@ -157,8 +177,25 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
   T rhs[MAX_RHS];
 #pragma unroll
   for (int h = 0; h < MAX_RHS; ++h) rhs[h] = (q == 0 && row_ok && h < nrhs) ? X[(long long)(r0 + r) * ldx + h] : T(0);
-  T dv[CP];
-  load_row_share<T>(dv, Dinv + (size_t)b * BS * BS + (size_t)r * BS, 0, q, BS, true, true);
+  T dv[EXACT ? 1 : CP];
+  if constexpr (EXACT) {
+    // T_bb with the unit (forward) or the stored (backward) diagonal; the
+    // padding of a ragged last block is the identity.
+    for (int i = threadIdx.x; i < BS * BS; i += NT) {
+      const int rr = i / BS, cc = i % BS;
+      T v = T(0);
+      if (rr < rows && cc < rows) {
+        if (forward ? cc < rr : cc >= rr) v = LU[(long long)(r0 + rr) * lda + r0 + cc];
+        if (forward && cc == rr) v = T(1);
+      } else if (rr == cc) {
+        v = T(1);
+      }
+      diag.t[rr][cc] = v;
+      if (rr == cc) diag.rdiag[rr] = T(1) / v;
+    }
+  } else {
+    load_row_share<T>(dv, Dinv + (size_t)b * BS * BS + (size_t)r * BS, 0, q, BS, true, true);
+  }
 
   T acc[MAX_RHS];
 #pragma unroll
@@ -210,25 +247,71 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
 #pragma unroll
     for (int h = 0; h < MAX_RHS; ++h) ys[r][h] = row_ok ? rhs[h] - acc[h] : T(0);
   __syncthreads();
-  // x_b = inv(T_bb) y
+  if constexpr (EXACT) {
+    // warp 0: column-sweep substitution, lane l holding rows l and l + 32
+    if (threadIdx.x < 32) {
+      const int l = threadIdx.x;
+      T y0[MAX_RHS], y1[MAX_RHS];
 #pragma unroll
-  for (int h = 0; h < MAX_RHS; ++h) acc[h] = T(0);
+      for (int h = 0; h < MAX_RHS; ++h) y0[h] = ys[l][h], y1[h] = ys[l + 32][h];
+      // (nrhs is uniform across the warp, so the guarded shuffles are too)
+      if (forward) {
+        for (int k = 0; k < BS; ++k) {
+          const T a0 = diag.t[l][k], a1 = diag.t[l + 32][k];
 #pragma unroll
-  for (int e = 0; e < CP; ++e) {
-    const int cc = col_of(e);
+          for (int h = 0; h < MAX_RHS; ++h)
+            if (h < nrhs) {
+              const T xk = __shfl_sync(0xffffffffu, k < 32 ? y0[h] : y1[h], k & 31);
+              if (l > k) y0[h] = fma(-a0, xk, y0[h]);
+              if (l + 32 > k) y1[h] = fma(-a1, xk, y1[h]);
+            }
+        }
+      } else {
+        // x_k = y_k / T_kk as a product with the reciprocal formed off the
+        // critical path (within one rounding of the quotient)
+        for (int k = BS - 1; k >= 0; --k) {
+          const T a0 = diag.t[l][k], a1 = diag.t[l + 32][k], rk = diag.rdiag[k];
 #pragma unroll
-    for (int h = 0; h < MAX_RHS; ++h)
-      if (h < nrhs) acc[h] = fma(dv[e], ys[cc][h], acc[h]);
+          for (int h = 0; h < MAX_RHS; ++h)
+            if (h < nrhs) {
+              const T xk = __shfl_sync(0xffffffffu, k < 32 ? y0[h] : y1[h], k & 31) * rk;
+              if (l == (k & 31)) {
+                if (k < 32) y0[h] = xk;
+                else y1[h] = xk;
+              }
+              if (l < k) y0[h] = fma(-a0, xk, y0[h]);
+              if (l + 32 < k) y1[h] = fma(-a1, xk, y1[h]);
+            }
+        }
+      }
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h)
+        if (h < nrhs) {
+          if (l < rows) X[(long long)(r0 + l) * ldx + h] = y0[h];
+          if (l + 32 < rows) X[(long long)(r0 + l + 32) * ldx + h] = y1[h];
+        }
+    }
+  } else {
+    // x_b = inv(T_bb) y
+#pragma unroll
+    for (int h = 0; h < MAX_RHS; ++h) acc[h] = T(0);
+#pragma unroll
+    for (int e = 0; e < CP; ++e) {
+      const int cc = col_of(e);
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h)
+        if (h < nrhs) acc[h] = fma(dv[e], ys[cc][h], acc[h]);
+    }
+#pragma unroll
+    for (int h = 0; h < MAX_RHS; ++h) {
+      acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 1);
+      acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 2);
+    }
+    if (q == 0 && row_ok)
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h)
+        if (h < nrhs) X[(long long)(r0 + r) * ldx + h] = acc[h];
   }
-#pragma unroll
-  for (int h = 0; h < MAX_RHS; ++h) {
-    acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 1);
-    acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 2);
-  }
-  if (q == 0 && row_ok)
-#pragma unroll
-    for (int h = 0; h < MAX_RHS; ++h)
-      if (h < nrhs) X[(long long)(r0 + r) * ldx + h] = acc[h];
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
@@ -260,15 +343,17 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
   return LM_OK;
 }
 
-// X (n x nrhs, nrhs <= 4) <- U^-1 L^-1 X with the packed factor and its block
-// inverses; `sync` holds 4 ints of device scratch.
+// X (n x nrhs, nrhs <= 4) <- U^-1 L^-1 X with the packed factor and (FP32)
+// its block inverses; FP64 ignores DinvL / DinvU.  `sync` holds 4 ints of
+// device scratch.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
             int* sync, int* status, cudaStream_t st) {
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC;
   if (nrhs > MAX_RHS) return LM_ERR_UNSUPPORTED;
   if (n <= 0 || nrhs <= 0) return LM_OK;
-  if (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16) return LM_ERR_ARG;
+  if (!TrsvCfg<T>::EXACT && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
+    return LM_ERR_ARG;
   const int nb = (n + BS - 1) / BS;
   const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
   LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
