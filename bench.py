@@ -34,6 +34,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "linear-massiv_b200"))
 
@@ -55,7 +57,10 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir"], default="lu")
+    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir", "batch"], default="lu")
+    p.add_argument("--count", type=int, default=10000, help="batch: number of instances")
+    p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
+    p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
     p.add_argument("--kappa", type=float, default=1e6, help="ir: condition number of A (0 = uniform A)")
     p.add_argument("--reflectors", type=int, default=4, help="ir: Householder reflectors per side")
     p.add_argument("--n", type=int, default=16384)
@@ -70,6 +75,10 @@ def parse():
 
 
 def workload_name(a):
+    if a.workload == "batch":
+        return (f"batched solves, {a.count} instances in one persistent launch, n uniform in [8,256], nrhs uniform "
+                f"in [1,16], half SPD (B B^T + n I, Cholesky) half general (uniform[-1,1], LU), "
+                f"{'FP64' if a.precision == 'fp64' else 'FP32 factor + FP64 refinement'}")
     if a.workload == "ir":
         spec = (f"A = U diag(sigma) V^T, kappa={a.kappa:g}, {a.reflectors} Householder reflectors per side"
                 if a.kappa > 0 else "A uniform[-1,1]")
@@ -85,6 +94,165 @@ def workload_name(a):
 
 def metric_name(a):
     return "FP64 GEMMs/s" if a.workload == "gemm" else "FP64-accurate solves/s"
+
+
+# ---- batched uneven solves ----------------------------------------------------------------
+
+def batch_inputs(a, rank, np):
+    """Seeded instances: sizes, kinds and the packed A / B (host, float64)."""
+    g = np.random.Generator(np.random.Philox(a.seed + 7919 * rank))
+    cnt = a.count
+    n = g.integers(8, 257, cnt).astype(np.int32)
+    nrhs = g.integers(1, 17, cnt).astype(np.int32)
+    kind = (np.arange(cnt) % 2).astype(np.int32)
+    a_off = np.concatenate([[0], np.cumsum(n.astype(np.int64) ** 2)])
+    b_off = np.concatenate([[0], np.cumsum(n.astype(np.int64) * nrhs)])
+    A = np.empty(a_off[-1])
+    for i in range(cnt):
+        m = int(n[i])
+        M = g.uniform(-1.0, 1.0, (m, m))
+        if kind[i] == 1:
+            M = M @ M.T + m * np.eye(m)
+        A[a_off[i]:a_off[i + 1]] = M.ravel()
+    B = g.uniform(-1.0, 1.0, b_off[-1])
+    return n, nrhs, kind, A, B, a_off, b_off
+
+
+def batch_flops(n, nrhs, kind):
+    n = n.astype(np.float64) if hasattr(n, "astype") else n
+    return float(((kind == 0) * (2.0 / 3.0) * n ** 3 + (kind == 1) * (1.0 / 3.0) * n ** 3 + 2.0 * n * n * nrhs).sum())
+
+
+def run_batch(a, world, rank, local):
+    import torch
+
+    import lmb200
+
+    torch.cuda.set_device(local)
+    ctx = lmb200.Context(local)
+    n, nrhs, kind, A, B, a_off, b_off = batch_inputs(a, rank, np)
+    prec = lmb200.PREC_FP64 if a.precision == "fp64" else lmb200.PREC_FP32_IR
+    tuned = None
+    if a.tune:
+        tuned = lmb200.batch_tune(prec, None, ctx)
+    plan = lmb200.Batch(n, nrhs, kind, prec, ctx)
+    A_h = torch.from_numpy(A).pin_memory()
+    B_h = torch.from_numpy(B).pin_memory()
+    A_d, B_d = A_h.cuda(), B_h.cuda()
+    X_d = torch.empty_like(B_d)
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device="cuda")  # 256 MB > L2
+
+    def step():
+        plan.solve(A_d, B_d, X_d, tol=0.0, max_iter=10)
+
+    for _ in range(a.warmup):
+        step()
+    torch.cuda.synchronize()
+    info, iters, berr = plan.results()
+    # accuracy of the warm-up result on a sample of instances (host FP64)
+    Xh = X_d.cpu().numpy()
+    worst = 0.0
+    for i in range(0, a.count, max(1, a.count // 200)):
+        m, r = int(n[i]), int(nrhs[i])
+        Ai = A[a_off[i]:a_off[i + 1]].reshape(m, m)
+        Bi = B[b_off[i]:b_off[i + 1]].reshape(m, r)
+        Xi = Xh[b_off[i]:b_off[i + 1]].reshape(m, r)
+        res = np.abs(Ai @ Xi - Bi).max(axis=0)
+        den = np.abs(Ai).sum(axis=1).max() * np.abs(Xi).max(axis=0) + np.abs(Bi).max(axis=0)
+        worst = max(worst, float((res / den).max() / (1e-15 * m)))
+    launches0 = lmb200.launch_count()
+    clocks = Clocks(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    ms = []
+    for _ in range(a.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        step()
+        e1.record(st)
+        ms.append((e0, e1))
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    t_local = sum(e0.elapsed_time(e1) for e0, e1 in ms) * 1e-3
+    launches = lmb200.launch_count() - launches0
+    t = max_over_ranks(t_local, world)
+    value = world * a.count * a.steps / t
+    flops = batch_flops(n, nrhs, kind)
+    peak = measure_fp64_peak(torch) if (rank == 0 and not a.no_peak) else None
+    achieved = flops * a.steps / t_local / 1e12
+    # e2e: host (pinned) buffers through lm_batch_solve_host
+    Xp = torch.empty_like(B_h).pin_memory()
+    P = lmb200._np_ptr
+    lib = lmb200.lib()
+
+    def e2e_step():
+        stt = lib.lm_batch_solve_host(plan.h, P(A_h.numpy()), P(B_h.numpy()), P(Xp.numpy()), 0.0, 10)
+        if stt < 0:
+            raise lmb200.LMError(stt, "lm_batch_solve_host")
+
+    e2e_val = None
+    if a.e2e_steps > 0:
+        e2e_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(a.e2e_steps):
+            e2e_step()
+        e2e_val = world * a.count * a.e2e_steps / max_over_ranks(time.perf_counter() - t0, world)
+    if rank != 0:
+        return
+    nb = lmb200.batch_tune_get(ctx)
+    line = {
+        "metric": metric_name(a), "value": value, "unit": metric_name(a), "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32 factor / f64 refinement",
+        "data": "synthetic (seeded numpy Philox)",
+        "config": {"workload": workload_name(a), "count": a.count, "parallelism": f"replicas x{world}",
+                   "l2": "256 MB buffer written between timed steps (L2 flush)",
+                   "panel_width_per_bucket": nb[prec], "autotuned": bool(a.tune)},
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_val, "unit": metric_name(a), "h2d_bytes_per_step": int(A.nbytes + B.nbytes),
+                "d2h_bytes_per_step": int(B.nbytes), "steps": a.e2e_steps, "api": "lm_batch_solve_host"},
+        "roofline": {"bound": "fp64", "kernel": "batch_kernel (persistent, one CTA per instance)",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if peak else None, "traffic": None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 peak; MEASURED_PEAKS.json has no FP64)",
+                     "algorithmic_flops_per_step": flops},
+        "tflops_whole_step": flops * a.steps / t / 1e12,
+        "accuracy": {"worst_backward_error_over_1e-15n": worst, "sampled_instances": len(range(0, a.count, max(1, a.count // 200))),
+                     "info_nonzero": int((info != 0).sum()), "fp64_fallbacks": int((iters < 0).sum()),
+                     "mean_corrections": float(iters[iters >= 0].mean()) if (iters >= 0).any() else None},
+        "clocks": clk,
+    }
+    if world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_batch(a, n, nrhs, kind, A, B, a_off, b_off)
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline_batch(a, n, nrhs, kind, A, B, a_off, b_off):
+    """Oracle luSolveP / choleskySolveP on the leading instances for about 10 s, one thread."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    t0 = time.perf_counter()
+    done = 0
+    for i in range(a.count):
+        m, r = int(n[i]), int(nrhs[i])
+        Ai = A[a_off[i]:a_off[i + 1]].reshape(m, m)
+        Bi = B[b_off[i]:b_off[i + 1]].reshape(m, r)
+        if kind[i] == 0:
+            O.lu_solve_p(Ai, Bi)
+        else:
+            O.chol_solve_p(Ai, Bi)
+        done += 1
+        if time.perf_counter() - t0 > 10.0:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "FP64-accurate solves/s", "cores": 1, "kind": "port",
+            "sample": f"the first {done} instances of the same batch solved one by one by the oracle "
+                      f"(luSolveP / choleskySolveP restatement) on one host thread in {dt:.1f} s"}
 
 
 # ---- clocks sampled during the timed region ----------------------------------------
@@ -488,6 +656,8 @@ def main():
     try:
         if a.impl == "reference":
             run_reference(a, world, rank)
+        elif a.workload == "batch":
+            run_batch(a, world, rank, local)
         else:
             run_ours(a, world, rank, local)
     finally:

@@ -189,6 +189,52 @@ int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const dou
  * race and must be serialised by the caller. */
 int lm_dpotrf_noalloc(void* stream, int n, double* A, int lda, int* info);
 
+/* ---- batched uneven-size solves in one persistent launch -----------------------
+ * No counterpart in the reference (its solves take one system at a time).
+ * A plan fixes the sizes of `count` independent systems A_i X_i = B_i:
+ * n_i in [0, 256], nrhs_i in [0, 16], kind_i LM_BATCH_GENERAL (LU with partial
+ * pivoting, luSolveP, LU.hs:265-357) or LM_BATCH_SPD (Cholesky,
+ * choleskySolveP, Chol.hs:241-321).  Inputs are packed back to back in the
+ * caller's order: A_i at A + a_off[i] (n_i x n_i row-major), B_i and X_i at
+ * + b_off[i] (n_i x nrhs_i row-major); lm_batch_offsets returns the offsets
+ * (count + 1 entries each, host arrays).  lm_batch_solve runs the whole batch
+ * as one persistent kernel (captured in a CUDA graph after its first call):
+ * A and B are read-only device buffers, X (device) receives the solutions.
+ * precision LM_PREC_FP64: factor and solve in FP64.  LM_PREC_FP32_IR: factor
+ * in FP32 and refine in FP64 until each instance's normwise backward error is
+ * <= tol (tol <= 0 selects 1e-15 * n_i per instance); an instance not
+ * converged after max_iter corrections is redone in FP64.
+ * lm_batch_results copies per-instance info (LAPACK-style, 0 = ok), the
+ * number of corrections (-1 = FP64 fallback, 0 for LM_PREC_FP64) and the
+ * final backward error (IR only) to host arrays (any may be NULL); it
+ * synchronises.  Panel widths per size bucket come from the context's tuning
+ * table (lm_batch_tune). */
+#define LM_BATCH_GENERAL 0
+#define LM_BATCH_SPD 1
+#define LM_PREC_FP64 0
+#define LM_PREC_FP32_IR 1
+typedef struct lm_batch lm_batch;
+int lm_batch_create(lm_ctx* ctx, lm_batch** plan, int count, const int* n, const int* nrhs, const int* kind,
+                    int precision);
+int lm_batch_destroy(lm_batch* plan);
+int lm_batch_offsets(const lm_batch* plan, long long* a_off, long long* b_off);
+int lm_batch_solve(lm_batch* plan, const double* A, const double* B, double* X, double tol, int max_iter);
+int lm_batch_results(lm_batch* plan, int* info, int* iters, double* berr);
+/* Device pointers of the plan's factor workspace (instance i's LU or G at
+ * F + a_off[i], FP64 plans) and swap lists (instance i's at ipiv + p_off[i],
+ * p_off[i] = sum of n_j, j < i); valid until the next solve or destroy. */
+int lm_batch_factors(const lm_batch* plan, const double** F, const int** ipiv);
+/* Host-buffer form: copies the packed A and B in, solves, copies X out. */
+int lm_batch_solve_host(lm_batch* plan, const double* A, const double* B, double* X, double tol, int max_iter);
+/* Project-written autotuner: for each size bucket (n <= 32, 64, 128, 256)
+ * times the batch kernel on a seeded synthetic batch of that bucket with each
+ * candidate panel width (8, 16, 32) and keeps the fastest in the context's
+ * table; `path` (may be NULL) receives the table as JSON.  lm_batch_tune_get /
+ * lm_batch_tune_set read and write the table (nb[precision][bucket]). */
+int lm_batch_tune(lm_ctx* ctx, int precision, const char* path);
+int lm_batch_tune_get(lm_ctx* ctx, int* nb /* [2][4] */);
+int lm_batch_tune_set(lm_ctx* ctx, const int* nb /* [2][4] */);
+
 /* ---- residual (IR and the reference's scaled residual) ---------------------
  * R = B - A X in FP64 (device), n x nrhs; replaces matvec / rawGemv
  * (L2.hs:123-144, K.hs:119-134) on the refinement path. */

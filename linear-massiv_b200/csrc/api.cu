@@ -45,6 +45,8 @@ struct Ctx {
   void* ws[kWsSlots] = {};
   size_t ws_bytes[kWsSlots] = {};
   std::mutex mu;
+  // batch kernel panel width per precision and size bucket (lm_batch_tune)
+  int batch_nb[2][BatchLimits::kBuckets] = {{16, 16, 16, 16}, {16, 16, 16, 16}};
 };
 
 namespace {
@@ -883,6 +885,371 @@ int lm_det_host(lm_ctx* ctx, int n, const double* A, double* det) {
     ++swaps;
   }
   *det = (swaps % 2 == 0) ? prod : -prod;
+  return LM_OK;
+}
+
+}  // extern "C"
+
+// ---- batched uneven-size solves ------------------------------------------------
+struct lm_batch {
+  lm_ctx* ctx = nullptr;
+  long long id = 0;  // unique per plan: keys its captured graphs (a freed plan's address can be reused)
+  int count = 0, prec = 0;
+  int nmax = 0, rmax = 0, nbmax = 0;
+  std::vector<long long> a_off, b_off;
+  lm::BatchItem* d_items = nullptr;
+  double* d_F = nullptr;
+  int* d_ipiv = nullptr;
+  int* d_info = nullptr;
+  int* d_iters = nullptr;
+  double* d_berr = nullptr;
+  int* d_ticket = nullptr;
+  double *hA = nullptr, *hB = nullptr, *hX = nullptr;  // device buffers of the host-buffer entry point
+  size_t smem = 0;
+  int grid = 0;
+};
+
+namespace {
+
+std::atomic<long long> g_plan_ids{0};
+
+// Drop the captured graphs of one plan (their kernels hold its buffers).
+void evict_graphs(Ctx& c, const std::string& prefix) {
+  for (auto it = c.gcache.begin(); it != c.gcache.end();) {
+    if (it->key.compare(0, prefix.size(), prefix) == 0) {
+      if (it->exec) cudaGraphExecDestroy(it->exec);
+      it = c.gcache.erase(it);
+    } else {
+      ++it;
+    }
+  }
+}
+
+void batch_free(lm_batch* p) {
+  cudaFree(p->d_items);
+  cudaFree(p->d_F);
+  cudaFree(p->d_ipiv);
+  cudaFree(p->d_info);
+  cudaFree(p->d_iters);
+  cudaFree(p->d_berr);
+  cudaFree(p->d_ticket);
+  cudaFree(p->hA);
+  cudaFree(p->hB);
+  cudaFree(p->hX);
+}
+
+int batch_build(Ctx& c, lm_batch* p, int count, const int* n, const int* nrhs, const int* kind, int prec) {
+  p->count = count;
+  p->prec = prec;
+  p->a_off.assign(count + 1, 0);
+  p->b_off.assign(count + 1, 0);
+  std::vector<long long> p_off(count + 1, 0);
+  std::vector<lm::BatchItem> items(count);
+  for (int i = 0; i < count; ++i) {
+    if (n[i] < 0 || n[i] > lm::BatchLimits::kMaxN || nrhs[i] < 0 || nrhs[i] > lm::BatchLimits::kMaxRhs ||
+        (kind[i] != LM_BATCH_GENERAL && kind[i] != LM_BATCH_SPD)) {
+      lm::set_last_error("batch instance " + std::to_string(i) + ": n must be in [0, 256], nrhs in [0, 16]");
+      return LM_ERR_ARG;
+    }
+    p->a_off[i + 1] = p->a_off[i] + (long long)n[i] * n[i];
+    p->b_off[i + 1] = p->b_off[i] + (long long)n[i] * nrhs[i];
+    p_off[i + 1] = p_off[i] + n[i];
+    lm::BatchItem& it = items[i];
+    it.a_off = p->a_off[i];
+    it.b_off = p->b_off[i];
+    it.f_off = p->a_off[i];
+    it.p_off = p_off[i];
+    it.n = n[i];
+    it.nrhs = nrhs[i];
+    it.kind = kind[i];
+    it.nb = c.batch_nb[prec][lm::batch_bucket(std::max(n[i], 1))];
+    it.index = i;
+    p->nmax = std::max(p->nmax, n[i]);
+    p->rmax = std::max(p->rmax, nrhs[i]);
+    p->nbmax = std::max(p->nbmax, it.nb);
+  }
+  p->nmax = std::max(p->nmax, 1);
+  p->rmax = std::max(p->rmax, 1);
+  p->nbmax = std::max(p->nbmax, 1);
+  // longest processing time first: the largest instances are taken first so
+  // the small ones fill in behind them
+  auto cost = [](const lm::BatchItem& it) {
+    const double nn = it.n;
+    return (it.kind == LM_BATCH_GENERAL ? 2.0 / 3.0 : 1.0 / 3.0) * nn * nn * nn + 2.0 * nn * nn * it.nrhs +
+           64.0 * nn * nn;
+  };
+  std::stable_sort(items.begin(), items.end(),
+                   [&](const lm::BatchItem& a, const lm::BatchItem& b) { return cost(a) > cost(b); });
+  const size_t ni = std::max(count, 1);
+  LM_CUDA_TRY(cudaMalloc(&p->d_items, sizeof(lm::BatchItem) * ni));
+  LM_CUDA_TRY(cudaMalloc(&p->d_F, sizeof(double) * std::max<long long>(p->a_off[count], 1)));
+  LM_CUDA_TRY(cudaMalloc(&p->d_ipiv, sizeof(int) * std::max<long long>(p_off[count], 1)));
+  LM_CUDA_TRY(cudaMalloc(&p->d_info, sizeof(int) * ni));
+  LM_CUDA_TRY(cudaMalloc(&p->d_iters, sizeof(int) * ni));
+  LM_CUDA_TRY(cudaMalloc(&p->d_berr, sizeof(double) * ni));
+  LM_CUDA_TRY(cudaMalloc(&p->d_ticket, sizeof(int) * 4));
+  if (count > 0)
+    LM_CUDA_TRY(cudaMemcpy(p->d_items, items.data(), sizeof(lm::BatchItem) * count, cudaMemcpyHostToDevice));
+  LM_CUDA_TRY(cudaMemset(p->d_info, 0, sizeof(int) * ni));
+  LM_CUDA_TRY(cudaMemset(p->d_iters, 0, sizeof(int) * ni));
+  LM_CUDA_TRY(cudaMemset(p->d_berr, 0, sizeof(double) * ni));
+  p->smem = lm::batch_smem_bytes(p->nmax, p->rmax, p->nbmax);
+  if (p->smem > 200 * 1024) {
+    lm::set_last_error("batch: shared memory of the largest instance exceeds 200 KB");
+    return LM_ERR_UNSUPPORTED;
+  }
+  int per_sm = 0;
+  LM_TRY(lm::batch_occupancy(p->smem, &per_sm));
+  per_sm = std::max(per_sm, 1);
+  p->grid = std::max(1, std::min(count, per_sm * c.num_sms));
+  return LM_OK;
+}
+
+int batch_run(Ctx& c, lm_batch* p, const double* A, const double* B, double* X, double tol, int max_iter) {
+  if (p->count == 0) return LM_OK;
+  lm::BatchArgs g;
+  g.items = p->d_items;
+  g.count = p->count;
+  g.prec = p->prec;
+  g.nmax = p->nmax;
+  g.rmax = p->rmax;
+  g.nbmax = p->nbmax;
+  g.A = A;
+  g.B = B;
+  g.X = X;
+  g.F = p->d_F;
+  g.ipiv = p->d_ipiv;
+  g.info = p->d_info;
+  g.iters = p->d_iters;
+  g.berr = p->d_berr;
+  g.ticket = p->d_ticket;
+  g.tol = tol;
+  g.max_iter = max_iter;
+  const std::string key = lm::gkey("batch", {p->id, (long long)A, (long long)B, (long long)X,
+                                             (long long)(tol * 1e30), max_iter});
+  return lm::run_graphed(c, key, [&](cudaStream_t s) { return lm::batch_launch(g, p->grid, p->smem, s); });
+}
+
+// Seeded synthetic instances for the tuner: general ones uniform[-1,1], SPD
+// ones (R + R^T)/2 + n I (diagonally dominant).
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+double unif(uint64_t& s) { return (double)(splitmix(s) >> 11) * (2.0 / 9007199254740992.0) - 1.0; }
+
+}  // namespace
+
+extern "C" {
+
+int lm_batch_create(lm_ctx* ctx, lm_batch** plan, int count, const int* n, const int* nrhs, const int* kind,
+                    int precision) {
+  if (!plan) return LM_ERR_ARG;
+  *plan = nullptr;
+  return guarded(ctx, [&](Ctx& c) {
+    if (count < 0 || (count > 0 && (!n || !nrhs || !kind))) return LM_ERR_ARG;
+    if (precision != LM_PREC_FP64 && precision != LM_PREC_FP32_IR) return LM_ERR_ARG;
+    lm_batch* p = new lm_batch;
+    p->ctx = ctx;
+    p->id = ++g_plan_ids;
+    const int r = batch_build(c, p, count, n, nrhs, kind, precision);
+    if (r != LM_OK) {
+      batch_free(p);
+      delete p;
+      return r;
+    }
+    *plan = p;
+    return LM_OK;
+  });
+}
+
+int lm_batch_destroy(lm_batch* plan) {
+  if (!plan) return LM_OK;
+  return guarded(plan->ctx, [&](Ctx& c) {
+    cudaStreamSynchronize(c.stream);
+    evict_graphs(c, lm::gkey("batch", {plan->id}) + ",");
+    batch_free(plan);
+    delete plan;
+    return LM_OK;
+  });
+}
+
+int lm_batch_offsets(const lm_batch* plan, long long* a_off, long long* b_off) {
+  if (!plan) return LM_ERR_ARG;
+  if (a_off) std::copy(plan->a_off.begin(), plan->a_off.end(), a_off);
+  if (b_off) std::copy(plan->b_off.begin(), plan->b_off.end(), b_off);
+  return LM_OK;
+}
+
+int lm_batch_solve(lm_batch* plan, const double* A, const double* B, double* X, double tol, int max_iter) {
+  if (!plan) return LM_ERR_ARG;
+  return guarded(plan->ctx, [&](Ctx& c) {
+    if (plan->count > 0 && (!A || !B || !X)) return LM_ERR_ARG;
+    if (max_iter < 1) max_iter = 1;
+    return batch_run(c, plan, A, B, X, tol, max_iter);
+  });
+}
+
+int lm_batch_results(lm_batch* plan, int* info, int* iters, double* berr) {
+  if (!plan) return LM_ERR_ARG;
+  return guarded(plan->ctx, [&](Ctx& c) {
+    const size_t k = plan->count;
+    if (k == 0) return LM_OK;
+    if (info) LM_CUDA_TRY(cudaMemcpyAsync(info, plan->d_info, sizeof(int) * k, cudaMemcpyDeviceToHost, c.stream));
+    if (iters)
+      LM_CUDA_TRY(cudaMemcpyAsync(iters, plan->d_iters, sizeof(int) * k, cudaMemcpyDeviceToHost, c.stream));
+    if (berr)
+      LM_CUDA_TRY(cudaMemcpyAsync(berr, plan->d_berr, sizeof(double) * k, cudaMemcpyDeviceToHost, c.stream));
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    int h[2] = {0, 0};
+    LM_CUDA_TRY(cudaMemcpy(h, c.d_status, sizeof(h), cudaMemcpyDeviceToHost));
+    return h[0] != 0 ? LM_ERR_TIMEOUT : LM_OK;
+  });
+}
+
+int lm_batch_factors(const lm_batch* plan, const double** F, const int** ipiv) {
+  if (!plan) return LM_ERR_ARG;
+  if (F) *F = plan->d_F;
+  if (ipiv) *ipiv = plan->d_ipiv;
+  return LM_OK;
+}
+
+int lm_batch_solve_host(lm_batch* plan, const double* A, const double* B, double* X, double tol, int max_iter) {
+  if (!plan) return LM_ERR_ARG;
+  return guarded(plan->ctx, [&](Ctx& c) {
+    const long long na = plan->a_off.back(), nbv = plan->b_off.back();
+    if (plan->count == 0) return LM_OK;
+    if (!A || !B || !X) return LM_ERR_ARG;
+    if (!plan->hA) {
+      LM_CUDA_TRY(cudaMalloc(&plan->hA, sizeof(double) * std::max(na, 1LL)));
+      LM_CUDA_TRY(cudaMalloc(&plan->hB, sizeof(double) * std::max(nbv, 1LL)));
+      LM_CUDA_TRY(cudaMalloc(&plan->hX, sizeof(double) * std::max(nbv, 1LL)));
+    }
+    LM_CUDA_TRY(cudaMemcpyAsync(plan->hA, A, sizeof(double) * na, cudaMemcpyHostToDevice, c.stream));
+    LM_CUDA_TRY(cudaMemcpyAsync(plan->hB, B, sizeof(double) * nbv, cudaMemcpyHostToDevice, c.stream));
+    LM_TRY(batch_run(c, plan, plan->hA, plan->hB, plan->hX, tol, std::max(max_iter, 1)));
+    LM_CUDA_TRY(cudaMemcpyAsync(X, plan->hX, sizeof(double) * nbv, cudaMemcpyDeviceToHost, c.stream));
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    return LM_OK;
+  });
+}
+
+int lm_batch_tune_get(lm_ctx* ctx, int* nb) {
+  if (!nb) return LM_ERR_ARG;
+  return guarded(ctx, [&](Ctx& c) {
+    std::memcpy(nb, c.batch_nb, sizeof(c.batch_nb));
+    return LM_OK;
+  });
+}
+
+int lm_batch_tune_set(lm_ctx* ctx, const int* nb) {
+  if (!nb) return LM_ERR_ARG;
+  for (int i = 0; i < 2 * lm::BatchLimits::kBuckets; ++i)
+    if (nb[i] != 8 && nb[i] != 16 && nb[i] != 32) return LM_ERR_ARG;
+  return guarded(ctx, [&](Ctx& c) {
+    std::memcpy(c.batch_nb, nb, sizeof(c.batch_nb));
+    return LM_OK;
+  });
+}
+
+int lm_batch_tune(lm_ctx* ctx, int precision, const char* path) {
+  if (!ctx || (precision != LM_PREC_FP64 && precision != LM_PREC_FP32_IR)) return LM_ERR_ARG;
+  const int lo[4] = {1, 33, 65, 129}, hi[4] = {32, 64, 128, 256};
+  const int cands[3] = {8, 16, 32};
+  double best_ms[4] = {0, 0, 0, 0};
+  int num_sms = 0;
+  {
+    int r = guarded(ctx, [&](Ctx& c) { num_sms = c.num_sms; return LM_OK; });
+    if (r) return r;
+  }
+  for (int b = 0; b < 4; ++b) {
+    const int count = 4 * num_sms;
+    std::vector<int> n(count), nrhs(count), kind(count);
+    uint64_t seed = 0x5eed0000ULL + b;
+    for (int i = 0; i < count; ++i) {
+      n[i] = lo[b] + (int)(splitmix(seed) % (uint64_t)(hi[b] - lo[b] + 1));
+      nrhs[i] = 1 + (int)(splitmix(seed) % 16);
+      kind[i] = i & 1;
+    }
+    std::vector<long long> ao(count + 1), bo(count + 1);
+    for (int i = 0; i < count; ++i) {
+      ao[i + 1] = ao[i] + (long long)n[i] * n[i];
+      bo[i + 1] = bo[i] + (long long)n[i] * nrhs[i];
+    }
+    std::vector<double> A(ao[count]), B(bo[count]);
+    for (int i = 0; i < count; ++i) {
+      double* a = A.data() + ao[i];
+      const int m = n[i];
+      for (long long e = 0; e < (long long)m * m; ++e) a[e] = unif(seed);
+      if (kind[i] == LM_BATCH_SPD)
+        for (int r = 0; r < m; ++r) {
+          for (int q = 0; q < r; ++q) a[(long long)r * m + q] = a[(long long)q * m + r] = 0.5 * (a[(long long)r * m + q] + a[(long long)q * m + r]);
+          a[(long long)r * m + r] += m;
+        }
+    }
+    for (auto& v : B) v = unif(seed);
+    double *dA = nullptr, *dB = nullptr, *dX = nullptr;
+    if (cudaMalloc(&dA, sizeof(double) * A.size()) != cudaSuccess || cudaMalloc(&dB, sizeof(double) * B.size()) != cudaSuccess ||
+        cudaMalloc(&dX, sizeof(double) * B.size()) != cudaSuccess) {
+      cudaFree(dA); cudaFree(dB); cudaFree(dX);
+      return LM_ERR_NOMEM;
+    }
+    cudaMemcpy(dA, A.data(), sizeof(double) * A.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(dB, B.data(), sizeof(double) * B.size(), cudaMemcpyHostToDevice);
+    int keep = 16;
+    double keep_ms = 1e30;
+    int saved[2][4];
+    lm_batch_tune_get(ctx, &saved[0][0]);
+    int rc = LM_OK;
+    for (int nb : cands) {
+      int t[2][4];
+      std::memcpy(t, saved, sizeof(t));
+      t[precision][b] = nb;
+      lm_batch_tune_set(ctx, &t[0][0]);
+      lm_batch* plan = nullptr;
+      rc = lm_batch_create(ctx, &plan, count, n.data(), nrhs.data(), kind.data(), precision);
+      if (rc) break;
+      float ms = 0.f;
+      cudaStream_t st = (cudaStream_t)lm_ctx_get_stream(ctx);
+      cudaEvent_t e0, e1;
+      cudaEventCreate(&e0);
+      cudaEventCreate(&e1);
+      for (int w = 0; w < 2 && !rc; ++w) rc = lm_batch_solve(plan, dA, dB, dX, 0.0, 10);
+      float best = 1e30f;
+      for (int rep = 0; rep < 3 && !rc; ++rep) {
+        cudaEventRecord(e0, st);
+        rc = lm_batch_solve(plan, dA, dB, dX, 0.0, 10);
+        cudaEventRecord(e1, st);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        best = std::min(best, ms);
+      }
+      if (!rc) rc = lm_batch_results(plan, nullptr, nullptr, nullptr);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      lm_batch_destroy(plan);
+      if (rc) break;
+      if (best < keep_ms) { keep_ms = best; keep = nb; }
+    }
+    cudaFree(dA); cudaFree(dB); cudaFree(dX);
+    saved[precision][b] = keep;
+    lm_batch_tune_set(ctx, &saved[0][0]);
+    if (rc) return rc;
+    best_ms[b] = keep_ms;
+  }
+  if (path) {
+    FILE* f = std::fopen(path, "w");
+    if (!f) return LM_ERR_ARG;
+    int t[2][4];
+    lm_batch_tune_get(ctx, &t[0][0]);
+    std::fprintf(f, "{\"precision\": %d, \"buckets\": [32, 64, 128, 256], \"nb\": [[%d, %d, %d, %d], [%d, %d, %d, %d]], "
+                    "\"best_ms\": [%.4f, %.4f, %.4f, %.4f]}\n",
+                 precision, t[0][0], t[0][1], t[0][2], t[0][3], t[1][0], t[1][1], t[1][2], t[1][3], best_ms[0],
+                 best_ms[1], best_ms[2], best_ms[3]);
+    std::fclose(f);
+  }
   return LM_OK;
 }
 

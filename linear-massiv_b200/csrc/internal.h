@@ -142,4 +142,46 @@ int dpotrf_borrowed(int device, int num_sms, cudaStream_t st, int n, double* A, 
 int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* X, long long ldx,
               const double* B, long long ldb, double* R, long long ldr, cudaStream_t st);
 
+
+// --- batched persistent factor + solve (batch.cu) ------------------------------
+struct BatchLimits {
+  static constexpr int kMaxN = 256;    // largest order per instance
+  static constexpr int kMaxRhs = 16;   // most right-hand sides per instance
+  static constexpr int kBuckets = 4;   // size buckets n <= 32, 64, 128, 256
+};
+inline int batch_bucket(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2 : 3; }
+
+// One instance, in schedule order (largest first).
+struct BatchItem {
+  long long a_off;  // A_i at A + a_off: n x n row-major, ld n
+  long long b_off;  // B_i and X_i at + b_off: n x nrhs row-major, ld nrhs
+  long long f_off;  // factor workspace at F + f_off: n * n doubles
+  long long p_off;  // swap list at ipiv + p_off: n ints
+  int n, nrhs, kind, nb, index;
+};
+
+struct BatchArgs {
+  const BatchItem* items;
+  int count;
+  int prec;             // LM_PREC_FP64 or LM_PREC_FP32_IR
+  int nmax, rmax, nbmax;
+  const double* A;
+  const double* B;
+  double* X;
+  double* F;
+  int* ipiv;
+  int* info;
+  int* iters;
+  double* berr;
+  int* ticket;
+  double tol;
+  int max_iter;
+};
+// Dynamic shared memory of the batch kernel for the given maxima.
+size_t batch_smem_bytes(int nmax, int rmax, int nbmax);
+// Resident CTAs per SM of the batch kernel at that shared-memory size.
+int batch_occupancy(size_t smem, int* per_sm);
+// Reset the ticket and launch `grid` persistent CTAs on `st`.
+int batch_launch(const BatchArgs& g, int grid, size_t smem, cudaStream_t st);
+
 }  // namespace lm

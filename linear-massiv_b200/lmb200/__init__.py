@@ -39,7 +39,14 @@ EXPORTS = [
     "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
     "lm_lu_host", "lm_cholesky_host", "lm_det_host", "lm_ipiv_to_perm", "lm_dresidual",
     "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_dpotrf_noalloc",
+    "lm_batch_create", "lm_batch_destroy", "lm_batch_offsets", "lm_batch_solve", "lm_batch_results",
+    "lm_batch_factors", "lm_batch_solve_host", "lm_batch_tune", "lm_batch_tune_get", "lm_batch_tune_set",
 ]
+
+BATCH_GENERAL = 0
+BATCH_SPD = 1
+PREC_FP64 = 0
+PREC_FP32_IR = 1
 
 
 class LMError(RuntimeError):
@@ -106,6 +113,16 @@ def _lib():
                 "lm_dgesv_ir": ([vp, i, i, vp, i, vp, i, vp, i, d, i, ip, dp, ip], i),
                 "lm_lu_solve_ir_host": ([vp, i, i, dp, dp, dp, d, i, ip, dp, ip], i),
                 "lm_dpotrf_noalloc": ([vp, i, vp, i, ip], i),
+                "lm_batch_create": ([vp, ctypes.POINTER(vp), i, ip, ip, ip, i], i),
+                "lm_batch_destroy": ([vp], i),
+                "lm_batch_offsets": ([vp, vp, vp], i),
+                "lm_batch_solve": ([vp, vp, vp, vp, d, i], i),
+                "lm_batch_results": ([vp, ip, ip, dp], i),
+                "lm_batch_factors": ([vp, ctypes.POINTER(vp), ctypes.POINTER(vp)], i),
+                "lm_batch_solve_host": ([vp, dp, dp, dp, d, i], i),
+                "lm_batch_tune": ([vp, i, ctypes.c_char_p], i),
+                "lm_batch_tune_get": ([vp, ip], i),
+                "lm_batch_tune_set": ([vp, ip], i),
             }
             for name, (args, res) in sigs.items():
                 fn = getattr(L, name)
@@ -434,3 +451,101 @@ def cholesky_host(A, ctx: Context | None = None):
     _check(_lib().lm_cholesky_host(ctx.h, A.shape[0], _np_ptr(A), _np_ptr(G), ctypes.byref(info)),
            "lm_cholesky_host")
     return G, info.value
+
+
+# ---- batched uneven-size solves (one persistent launch) -------------------------
+
+class Batch:
+    """A plan for `count` independent solves A_i X_i = B_i of uneven sizes
+    (n_i <= 256, nrhs_i <= 16), general (LU) or SPD (Cholesky) per instance,
+    run as one persistent kernel.  Inputs are packed back to back
+    (offsets()); solve() takes device float64 tensors."""
+
+    def __init__(self, n, nrhs, kind, precision: int = PREC_FP64, ctx: Context | None = None):
+        import numpy as np
+
+        self.ctx = ctx or default_context(0)
+        self.n = np.ascontiguousarray(n, dtype=np.int32)
+        self.nrhs = np.ascontiguousarray(nrhs, dtype=np.int32)
+        self.kind = np.ascontiguousarray(kind, dtype=np.int32)
+        self.count = len(self.n)
+        self.precision = precision
+        h = ctypes.c_void_p()
+        ip = ctypes.POINTER(ctypes.c_int)
+        _check(_lib().lm_batch_create(self.ctx.h, ctypes.byref(h), self.count, self.n.ctypes.data_as(ip),
+                                      self.nrhs.ctypes.data_as(ip), self.kind.ctypes.data_as(ip), precision),
+               "lm_batch_create")
+        self.h = h
+        a = np.zeros(self.count + 1, dtype=np.int64)
+        b = np.zeros(self.count + 1, dtype=np.int64)
+        _check(_lib().lm_batch_offsets(self.h, ctypes.c_void_p(a.ctypes.data), ctypes.c_void_p(b.ctypes.data)),
+               "lm_batch_offsets")
+        self.a_off, self.b_off = a, b
+        self.p_off = np.concatenate([[0], np.cumsum(self.n.astype(np.int64))])
+
+    def offsets(self):
+        return self.a_off, self.b_off
+
+    def solve(self, A, B, X, tol: float = 0.0, max_iter: int = 10):
+        _check(_lib().lm_batch_solve(self.h, _ptr(A), _ptr(B), _ptr(X), float(tol), int(max_iter)),
+               "lm_batch_solve")
+        return X
+
+    def solve_host(self, A, B, tol: float = 0.0, max_iter: int = 10):
+        import numpy as np
+
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        X = np.empty_like(B)
+        _check(_lib().lm_batch_solve_host(self.h, _np_ptr(A), _np_ptr(B), _np_ptr(X), float(tol), int(max_iter)),
+               "lm_batch_solve_host")
+        return X
+
+    def results(self):
+        """(info, iters, berr) per instance, as numpy arrays (synchronises)."""
+        import numpy as np
+
+        info = np.zeros(max(self.count, 1), dtype=np.int32)
+        iters = np.zeros(max(self.count, 1), dtype=np.int32)
+        berr = np.zeros(max(self.count, 1), dtype=np.float64)
+        ip = ctypes.POINTER(ctypes.c_int)
+        _check(_lib().lm_batch_results(self.h, info.ctypes.data_as(ip), iters.ctypes.data_as(ip), _np_ptr(berr)),
+               "lm_batch_results")
+        return info[:self.count], iters[:self.count], berr[:self.count]
+
+    def factors(self):
+        """Device pointers (ints) of the factor workspace and the swap lists."""
+        f, p = ctypes.c_void_p(), ctypes.c_void_p()
+        _check(_lib().lm_batch_factors(self.h, ctypes.byref(f), ctypes.byref(p)), "lm_batch_factors")
+        return f.value, p.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().lm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_tune(precision: int = PREC_FP64, path: str | None = None, ctx: Context | None = None):
+    """Autotune the batch kernel's panel width per size bucket; returns the table nb[2][4]."""
+    ctx = ctx or default_context(0)
+    _check(_lib().lm_batch_tune(ctx.h, precision, path.encode() if path else None), "lm_batch_tune")
+    return batch_tune_get(ctx)
+
+
+def batch_tune_get(ctx: Context | None = None):
+    ctx = ctx or default_context(0)
+    t = (ctypes.c_int * 8)()
+    _check(_lib().lm_batch_tune_get(ctx.h, t), "lm_batch_tune_get")
+    return [list(t[0:4]), list(t[4:8])]
+
+
+def batch_tune_set(table, ctx: Context | None = None):
+    ctx = ctx or default_context(0)
+    t = (ctypes.c_int * 8)(*(list(table[0]) + list(table[1])))
+    _check(_lib().lm_batch_tune_set(ctx.h, t), "lm_batch_tune_set")
