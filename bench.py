@@ -57,7 +57,11 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir", "batch"], default="lu")
+    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir", "batch", "serve"], default="lu")
+    p.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (requests/s)")
+    p.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
+    p.add_argument("--pool", type=int, default=48, help="serve: distinct pregenerated systems")
+    p.add_argument("--max-n", type=int, default=4096, help="serve: largest order")
     p.add_argument("--count", type=int, default=10000, help="batch: number of instances")
     p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
     p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
@@ -75,6 +79,11 @@ def parse():
 
 
 def workload_name(a):
+    if a.workload == "serve":
+        return (f"serving loop, Poisson arrivals at {a.rate:g} req/s for {a.duration:g} s, n log-uniform in "
+                f"[16,{a.max_n}], nrhs in {{1,8,32}}, 70% general / 30% SPD, kappa log-uniform in [1e1,1e6] "
+                f"(sigma-spectrum, {a.pool} pregenerated systems), mixed-precision IR with FP64 fallback, "
+                f"HBM-budget admission")
     if a.workload == "batch":
         return (f"batched solves, {a.count} instances in one persistent launch, n uniform in [8,256], nrhs uniform "
                 f"in [1,16], half SPD (B B^T + n I, Cholesky) half general (uniform[-1,1], LU), "
@@ -228,6 +237,132 @@ def run_batch(a, world, rank, local):
     }
     if world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_batch(a, n, nrhs, kind, A, B, a_off, b_off)
+    print(json.dumps(line), flush=True)
+
+
+def serve_pool(a, torch):
+    """Pregenerated request systems: (A pinned, kind, kappa) with n log-uniform."""
+    g = np.random.Generator(np.random.Philox(a.seed + 4242))
+    pool = []
+    for _ in range(a.pool):
+        n = int(np.exp(g.uniform(np.log(16), np.log(a.max_n))))
+        spd = g.uniform() < 0.3
+        kappa = float(np.exp(g.uniform(np.log(1e1), np.log(1e6))))
+        s = torch.from_numpy(kappa ** (-np.arange(n) / max(n - 1, 1))).cuda()
+        U = torch.eye(n, dtype=torch.float64, device="cuda")
+        for _ in range(4):
+            v = torch.from_numpy(g.standard_normal(n)).cuda()
+            v /= torch.linalg.norm(v)
+            U -= 2.0 * torch.outer(v, v @ U)
+        if spd:
+            V = U
+        else:
+            V = torch.eye(n, dtype=torch.float64, device="cuda")
+            for _ in range(4):
+                v = torch.from_numpy(g.standard_normal(n)).cuda()
+                v /= torch.linalg.norm(v)
+                V -= 2.0 * torch.outer(v, v @ V)
+        A = ((U * s) @ V.T).cpu().pin_memory()
+        pool.append((A, 1 if spd else 0, kappa))
+    return pool
+
+
+def run_serve(a, world, rank, local):
+    import torch
+
+    import lmb200
+
+    torch.cuda.set_device(local)
+    pool = serve_pool(a, torch)
+    g = np.random.Generator(np.random.Philox(a.seed + 99 + 7919 * rank))
+    rhs = {r: torch.from_numpy(g.uniform(-1.0, 1.0, (a.max_n, r))).pin_memory() for r in (1, 8, 32)}
+    free_b, _ = torch.cuda.mem_get_info()
+    srv = lmb200.Server(local, max_n=a.max_n, max_nrhs=32, large_workers=4, batch_lanes=2,
+                        hbm_budget=int(min(free_b // 3, 48 << 30)))
+    # arrival schedule and request draws (seeded, fixed before the run)
+    total = int(a.rate * a.duration)
+    gaps = g.exponential(1.0 / a.rate, total)
+    picks = g.integers(0, len(pool), total)
+    nrhs_of = g.choice([1, 8, 32], total)
+    nmax_pool = max(p[0].shape[0] for p in pool)
+    # output buffers are recycled round-robin: the timed requests' solutions
+    # are not read (accuracy is checked on separate requests below)
+    outs = [torch.empty((nmax_pool, 32), dtype=torch.float64).pin_memory() for _ in range(64)]
+
+    def submit_sys(j, r, out):
+        A, kind, _ = pool[j]
+        n = A.shape[0]
+        return srv.submit_raw(n, r, kind, A.data_ptr(), rhs[r].data_ptr(), out.data_ptr())
+
+    def submit(i, out):
+        return submit_sys(int(picks[i]), int(nrhs_of[i]), out)
+
+    # warm-up: every pool system once with each right-hand-side count
+    for j in range(len(pool)):
+        for r in (1, 8, 32):
+            srv.wait(submit_sys(j, r, outs[0]), 120.0)
+    srv.drain(120.0)
+    srv.reset_stats()
+    clocks = Clocks(local)
+    launches0 = lmb200.launch_count()
+    ids = []
+    t0 = time.perf_counter()
+    t_next = t0
+    k = 0
+    for i in range(total):
+        t_next += gaps[i]
+        while True:
+            d = t_next - time.perf_counter()
+            if d <= 0:
+                break
+            if d > 2e-4:
+                time.sleep(d - 1e-4)
+        ids.append(submit(i, outs[k]))
+        k = (k + 1) % 64
+    t_arrivals = time.perf_counter() - t0
+    drained = True
+    try:
+        srv.drain(max(120.0, 2 * a.duration))
+    except Exception:
+        drained = False
+    clk = clocks.stop()
+    st = srv.stats()
+    launches = lmb200.launch_count() - launches0
+    # accuracy on a sample: re-solve a few pool systems through the server and check on the host
+    worst = 0.0
+    for j in range(min(len(pool), 12)):
+        A, kind, _ = pool[j]
+        n = A.shape[0]
+        out = torch.empty((n, 8), dtype=torch.float64).pin_memory()
+        rid = srv.submit_raw(n, 8, kind, A.data_ptr(), rhs[8].data_ptr(), out.data_ptr())
+        srv.wait(rid, 120.0)
+        An, Xn, Bn = A.numpy(), out.numpy(), rhs[8].numpy().ravel()[:n * 8].reshape(n, 8)
+        r = np.abs(An @ Xn - Bn).max(axis=0)
+        den = np.abs(An).sum(axis=1).max() * np.abs(Xn).max(axis=0) + np.abs(Bn).max(axis=0)
+        worst = max(worst, float((r / den).max() / (1e-15 * n)))
+    srv.close()
+    if rank != 0:
+        return
+    value = st["solves_per_s"] * world
+    line = {
+        "metric": "FP64-accurate solves/s (serving) with p50/p99 latency", "value": value,
+        "unit": "FP64-accurate solves/s", "n_gpus": world, "steps": total, "warmup": len(pool),
+        "ms_per_step": 1e3 / value if value else None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 factor / f64 refinement (large), f64 (batched small)",
+        "data": "synthetic (seeded numpy Philox; sigma-spectrum systems)",
+        "config": {"workload": workload_name(a), "parallelism": f"replicas x{world}",
+                   "arrivals_offered": total, "arrival_window_s": t_arrivals, "drained": drained,
+                   "l2": "inputs far larger than L2 across the pool"},
+        "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"], "max": st["max_ms"]},
+        "serving": {k2: st[k2] for k2 in ("completed", "rejected", "failed", "fp64_fallbacks", "queue_peak",
+                                          "inflight_peak", "micro_batches", "small_solved", "arena_bytes",
+                                          "arena_peak_bytes", "fixed_bytes", "span_s", "tflops")},
+        "gpu_launches": launches,
+        "e2e": {"value": value, "unit": "FP64-accurate solves/s", "api": "lm_server_submit / lm_server_drain",
+                "note": "every request is host-to-host: A, B copied in and X copied out inside its latency"},
+        "accuracy": {"worst_backward_error_over_1e-15n": worst, "sampled_systems": min(len(pool), 12)},
+        "clocks": clk,
+    }
     print(json.dumps(line), flush=True)
 
 
@@ -658,6 +793,8 @@ def main():
             run_reference(a, world, rank)
         elif a.workload == "batch":
             run_batch(a, world, rank, local)
+        elif a.workload == "serve":
+            run_serve(a, world, rank, local)
         else:
             run_ours(a, world, rank, local)
     finally:

@@ -235,6 +235,60 @@ int lm_batch_tune(lm_ctx* ctx, int precision, const char* path);
 int lm_batch_tune_get(lm_ctx* ctx, int* nb /* [2][4] */);
 int lm_batch_tune_set(lm_ctx* ctx, const int* nb /* [2][4] */);
 
+/* ---- serving loop: continuous batching of arriving solves -----------------------
+ * No counterpart in the reference.  A server owns a device arena of
+ * `hbm_budget` bytes (0 = a quarter of the free memory after start-up) from
+ * which every admitted request takes one block (its A, B, X, factor and
+ * pivots).  Requests are admitted as soon as an execution slot and a block are
+ * free; small ones (n <= small_max_n, nrhs <= 16) are run as micro-batches of
+ * the persistent batch kernel (batch_lanes streams, each micro-batch taking
+ * every small request queued when its lane frees up), larger ones each take
+ * one of `large_workers` contexts (own stream; workspaces pre-grown at start-up
+ * for max_n x max_nrhs): mixed-precision LU + FP64 refinement for general
+ * matrices (large_precision LM_PREC_FP32_IR), FP64 LU when refinement does not
+ * converge, FP64 Cholesky for SPD ones.  A, B (read) and X (written) are the
+ * caller's host buffers (pinned for asynchronous copies) and must stay valid
+ * until the request completes.  Status of a completed request: 0, LAPACK-style
+ * info > 0, or < 0 on error / cancellation. */
+typedef struct {
+  size_t hbm_budget;    /* bytes of the request arena (0 = 1/4 of free memory) */
+  int large_workers;    /* concurrent large solves (default 4) */
+  int batch_lanes;      /* concurrent micro-batches (default 2) */
+  int small_max_n;      /* largest n sent to the batch kernel (default 256, <= 256) */
+  int small_precision;  /* LM_PREC_FP64 (default) or LM_PREC_FP32_IR */
+  int large_precision;  /* LM_PREC_FP32_IR (default) or LM_PREC_FP64 */
+  int max_batch;        /* most requests per micro-batch (default 4096) */
+  int max_n;            /* largest admissible order (default 4096) */
+  int max_nrhs;         /* most right-hand sides (default 64, <= 64) */
+  int nb[4];            /* batch-kernel panel width per size bucket (default 16) */
+} lm_server_config;
+typedef struct {
+  long long completed, rejected, cancelled, failed, fp64_fallbacks;
+  long long queue_peak, pending, micro_batches, small_solved;
+  int inflight, inflight_peak;
+  size_t arena_bytes, arena_peak_bytes, fixed_bytes;
+  double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> X in the host buffer */
+  double span_s, solves_per_s, tflops;    /* first submission to last completion */
+} lm_server_stats_t;
+int lm_server_default_config(lm_server_config* cfg);
+typedef struct lm_server lm_server;
+int lm_server_create(lm_server** server, int device, const lm_server_config* cfg);
+/* Queue one request; *id identifies it.  LM_ERR_ARG for sizes outside the
+ * configuration, LM_ERR_NOMEM for a request larger than the whole arena. */
+int lm_server_submit(lm_server* server, int n, int nrhs, int kind, const double* A, const double* B, double* X,
+                     long long* id);
+/* Non-blocking: *done = 1 once X is written (the id is then released). */
+int lm_server_test(lm_server* server, long long id, int* done, int* status, double* latency_ms);
+/* Blocking (timeout_s <= 0: no limit; LM_ERR_TIMEOUT when it expires). */
+int lm_server_wait(lm_server* server, long long id, int* status, double* latency_ms, double timeout_s);
+/* Remove a request that is still queued (LM_ERR_UNSUPPORTED once admitted). */
+int lm_server_cancel(lm_server* server, long long id);
+int lm_server_drain(lm_server* server, double timeout_s);
+int lm_server_stats(lm_server* server, lm_server_stats_t* stats);
+int lm_server_reset_stats(lm_server* server);
+/* Finishes admitted requests, cancels queued ones, frees everything. */
+int lm_server_destroy(lm_server* server);
+
 /* ---- residual (IR and the reference's scaled residual) ---------------------
  * R = B - A X in FP64 (device), n x nrhs; replaces matvec / rawGemv
  * (L2.hs:123-144, K.hs:119-134) on the refinement path. */

@@ -276,6 +276,14 @@ struct lm_ctx {
 
 using lm::Ctx;
 
+namespace lm {
+void ctx_set_graphs(lm_ctx* ctx, bool on) {
+  if (!ctx) return;
+  std::lock_guard<std::mutex> lock(ctx->c.mu);
+  ctx->c.graphs = on;
+}
+}  // namespace lm
+
 namespace {
 
 template <typename F>
@@ -957,6 +965,7 @@ int batch_build(Ctx& c, lm_batch* p, int count, const int* n, const int* nrhs, c
     lm::BatchItem& it = items[i];
     it.a_off = p->a_off[i];
     it.b_off = p->b_off[i];
+    it.x_off = p->b_off[i];
     it.f_off = p->a_off[i];
     it.p_off = p_off[i];
     it.n = n[i];

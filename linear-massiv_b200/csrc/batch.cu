@@ -588,7 +588,7 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BatchArgs g) {
       run_fp64(it, g, sm, fx, Xs, &info);
     }
     __syncthreads();
-    for (int e = tid_(); e < it.n * it.nrhs; e += kBT) g.X[it.b_off + e] = Xs[e];
+    for (int e = tid_(); e < it.n * it.nrhs; e += kBT) g.X[it.x_off + e] = Xs[e];
     if (tid_() == 0) {
       g.info[it.index] = info;
       g.iters[it.index] = iters;

@@ -6,6 +6,8 @@
 #include <cstddef>
 #include <functional>
 
+#include "lm_b200.h"
+
 namespace lm {
 
 constexpr int kMaxDevices = 64;
@@ -143,6 +145,11 @@ int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const dou
               const double* B, long long ldb, double* R, long long ldr, cudaStream_t st);
 
 
+// Turn CUDA-graph capture of repeated call sequences on or off for a context
+// (api.cu); the serving loop's workers run each request on fresh arena
+// addresses, where capture would not pay.
+void ctx_set_graphs(lm_ctx* ctx, bool on);
+
 // --- batched persistent factor + solve (batch.cu) ------------------------------
 struct BatchLimits {
   static constexpr int kMaxN = 256;    // largest order per instance
@@ -154,7 +161,8 @@ inline int batch_bucket(int n) { return n <= 32 ? 0 : n <= 64 ? 1 : n <= 128 ? 2
 // One instance, in schedule order (largest first).
 struct BatchItem {
   long long a_off;  // A_i at A + a_off: n x n row-major, ld n
-  long long b_off;  // B_i and X_i at + b_off: n x nrhs row-major, ld nrhs
+  long long b_off;  // B_i at B + b_off: n x nrhs row-major, ld nrhs
+  long long x_off;  // X_i at X + x_off (same shape)
   long long f_off;  // factor workspace at F + f_off: n * n doubles
   long long p_off;  // swap list at ipiv + p_off: n ints
   int n, nrhs, kind, nb, index;

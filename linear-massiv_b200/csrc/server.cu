@@ -1,0 +1,763 @@
+// Serving loop: continuous batching of arriving solves of uneven sizes.
+//
+// Requests (A_i X_i = B_i, host buffers) are queued by lm_server_submit and
+// admitted as soon as an execution slot and enough of the device arena are
+// free; their work overlaps on the device:
+//   small requests (n <= small_max_n, nrhs <= 16) are gathered into
+//     micro-batches: whenever a batch lane is idle it takes every queued small
+//     request that fits and runs them as ONE launch of the persistent batch
+//     kernel (batch.cu) on its own stream; requests arriving meanwhile join
+//     the next micro-batch on whichever lane frees first;
+//   larger requests each take a worker (own context, stream and pre-grown
+//     workspace): mixed-precision LU with FP64 refinement (lm_dgesv_ir), FP64
+//     LU when refinement does not converge or the FP32 factor breaks down, and
+//     FP64 Cholesky for SPD requests.
+// Admission by HBM footprint: every admitted request holds one block of a
+// device arena (its A, B, X, factor and pivots); a request is admitted only
+// when its block can be carved from the free space (first fit, coalescing on
+// release), and one whose block exceeds the whole arena is rejected at
+// submission.  Large requests are admitted in arrival order among themselves;
+// small ones never wait behind a large one that does not fit.
+// Latency = completion time (X written to the caller's host buffer) minus
+// submission time, host steady clock; p50 / p99 over completed requests.
+//
+// Failure handling is host-side: a request that fails (bad pivot, CUDA error)
+// completes with its status; cancel removes a request that is still queued;
+// destroy drains admitted work and cancels the rest.  No device-side waits.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+constexpr size_t kAlign = 256;
+size_t rup(size_t a) { return (a + kAlign - 1) / kAlign * kAlign; }
+
+// First-fit sub-allocator over one device allocation.
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0, in_use = 0, peak = 0;
+  std::map<size_t, size_t> free_;  // offset -> length
+  void init(char* b, size_t s) {
+    base = b;
+    size = s;
+    free_.clear();
+    free_[0] = s;
+  }
+  bool alloc(size_t bytes, size_t* off) {
+    bytes = rup(bytes);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= bytes) {
+        *off = it->first;
+        const size_t rest = it->second - bytes;
+        const size_t noff = it->first + bytes;
+        free_.erase(it);
+        if (rest) free_[noff] = rest;
+        in_use += bytes;
+        peak = std::max(peak, in_use);
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(size_t off, size_t bytes) {
+    bytes = rup(bytes);
+    in_use -= bytes;
+    auto it = free_.emplace(off, bytes).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_.erase(nx);
+    }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_.erase(it);
+      }
+    }
+  }
+};
+
+struct Req {
+  long long id = 0;
+  int n = 0, nrhs = 0, kind = 0;
+  const double* A = nullptr;
+  const double* B = nullptr;
+  double* X = nullptr;
+  bool small = false;
+  double t_submit = 0, t_admit = 0, t_done = 0;
+  // arena block: [A n*n][B n*r][X n*r][F n*n (small only)][ipiv n ints]
+  size_t off = 0, bytes = 0, oA = 0, oB = 0, oX = 0, oF = 0, oP = 0;
+  int status = 0, iters = 0;
+  bool fallback = false, done = false, cancelled = false;
+};
+
+size_t layout(Req& r) {
+  const size_t nn = (size_t)r.n * r.n * 8, nr = (size_t)r.n * r.nrhs * 8;
+  r.oA = 0;
+  r.oB = rup(r.oA + nn);
+  r.oX = rup(r.oB + nr);
+  r.oF = rup(r.oX + nr);
+  r.oP = rup(r.oF + (r.small ? nn : 0));
+  return rup(r.oP + (size_t)r.n * 4);
+}
+
+}  // namespace
+
+struct lm_server;
+
+namespace {
+
+struct Lane {
+  lm_server* s = nullptr;
+  int idx = 0;
+  std::thread th;
+  cudaStream_t st = nullptr;
+  lm::BatchItem* d_items = nullptr;
+  lm::BatchItem* h_items = nullptr;
+  int *d_info = nullptr, *d_iters = nullptr, *d_ticket = nullptr;
+  double* d_berr = nullptr;
+  int *h_info = nullptr, *h_iters = nullptr;
+  std::vector<Req*> jobs;
+  bool busy = false;
+  std::condition_variable cv;
+  double busy_s = 0;
+  long long batches = 0, solved = 0;
+};
+
+struct Worker {
+  lm_server* s = nullptr;
+  std::thread th;
+  lm_ctx* ctx = nullptr;
+  Req* job = nullptr;
+  bool busy = false;
+  std::condition_variable cv;
+  double busy_s = 0;
+};
+
+}  // namespace
+
+struct lm_server {
+  int device = 0;
+  int num_sms = 0;
+  lm_server_config cfg{};
+  std::mutex mu;
+  std::condition_variable cv_done;
+  std::deque<Req*> pending;
+  std::unordered_map<long long, Req*> live;
+  Arena arena;
+  std::vector<Lane*> lanes;
+  std::vector<Worker*> workers;
+  std::vector<double> lat_ms;
+  long long next_id = 1, completed = 0, rejected = 0, cancelled = 0, fallbacks = 0, failed = 0;
+  size_t queue_peak = 0;
+  int inflight = 0, inflight_peak = 0;
+  bool stopping = false;
+  double t_first = 0, t_last = 0;
+  double flops_done = 0;
+  size_t fixed_bytes = 0;  // pre-grown worker workspaces (outside the arena)
+};
+
+namespace {
+
+double req_flops(const Req& r) {
+  const double n = r.n;
+  return (r.kind == LM_BATCH_GENERAL ? 2.0 / 3.0 : 1.0 / 3.0) * n * n * n + 2.0 * n * n * r.nrhs;
+}
+
+void complete(lm_server* s, Req* r) {  // under s->mu
+  r->t_done = now_s();
+  r->done = true;
+  s->arena.release(r->off, r->bytes);
+  --s->inflight;
+  ++s->completed;
+  s->t_last = r->t_done;
+  s->lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
+  if (r->status < 0) ++s->failed;
+  if (r->fallback) ++s->fallbacks;
+  s->flops_done += req_flops(*r);
+}
+
+bool admit(lm_server* s, Req* r) {  // under s->mu
+  if (!s->arena.alloc(r->bytes, &r->off)) return false;
+  r->t_admit = now_s();
+  ++s->inflight;
+  s->inflight_peak = std::max(s->inflight_peak, s->inflight);
+  return true;
+}
+
+// Hand queued requests to idle lanes / workers.  Under s->mu.
+void pump(lm_server* s) {
+  // small requests: one micro-batch per idle lane, in arrival order
+  for (Lane* ln : s->lanes) {
+    if (ln->busy) continue;
+    std::vector<Req*> take;
+    for (auto it = s->pending.begin(); it != s->pending.end() && (int)take.size() < s->cfg.max_batch;) {
+      Req* r = *it;
+      if (r->small && admit(s, r)) {
+        take.push_back(r);
+        it = s->pending.erase(it);
+      } else if (r->small) {
+        break;  // arena full: the rest waits for releases
+      } else {
+        ++it;
+      }
+    }
+    if (take.empty()) break;
+    ln->jobs = std::move(take);
+    ln->busy = true;
+    ln->cv.notify_one();
+  }
+  // large requests: arrival order among themselves
+  for (auto it = s->pending.begin(); it != s->pending.end();) {
+    Req* r = *it;
+    if (r->small) {
+      ++it;
+      continue;
+    }
+    Worker* w = nullptr;
+    for (Worker* x : s->workers)
+      if (!x->busy) {
+        w = x;
+        break;
+      }
+    if (!w || !admit(s, r)) break;
+    it = s->pending.erase(it);
+    w->job = r;
+    w->busy = true;
+    w->cv.notify_one();
+  }
+}
+
+// ---- batch lane: one persistent-kernel launch per micro-batch -------------------------
+void lane_run(Lane* ln) {
+  lm_server* s = ln->s;
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    ln->cv.wait(lk, [&] { return ln->busy || s->stopping; });
+    if (!ln->busy && s->stopping) return;
+    std::vector<Req*> jobs = ln->jobs;
+    lk.unlock();
+    const double t0 = now_s();
+    char* base = s->arena.base;
+    int nmax = 1, rmax = 1;
+    int nbmax = 1;
+    int err = LM_OK;
+    const int k = (int)jobs.size();
+    for (int i = 0; i < k && err == LM_OK; ++i) {
+      Req* r = jobs[i];
+      char* blk = base + r->off;
+      if (cudaMemcpyAsync(blk + r->oA, r->A, (size_t)r->n * r->n * 8, cudaMemcpyHostToDevice, ln->st) != cudaSuccess ||
+          cudaMemcpyAsync(blk + r->oB, r->B, (size_t)r->n * r->nrhs * 8, cudaMemcpyHostToDevice, ln->st) !=
+              cudaSuccess)
+        err = LM_ERR_CUDA;
+      lm::BatchItem& it = ln->h_items[i];
+      it.a_off = (long long)((r->off + r->oA) / 8);
+      it.b_off = (long long)((r->off + r->oB) / 8);
+      it.x_off = (long long)((r->off + r->oX) / 8);
+      it.f_off = (long long)((r->off + r->oF) / 8);
+      it.p_off = (long long)((r->off + r->oP) / 4);
+      it.n = r->n;
+      it.nrhs = r->nrhs;
+      it.kind = r->kind;
+      it.nb = s->cfg.nb[lm::batch_bucket(std::max(r->n, 1))];
+      it.index = i;
+      nmax = std::max(nmax, r->n);
+      rmax = std::max(rmax, r->nrhs);
+      nbmax = std::max(nbmax, it.nb);
+    }
+    // largest first within the micro-batch
+    std::sort(ln->h_items, ln->h_items + k, [](const lm::BatchItem& a, const lm::BatchItem& b) {
+      return (double)a.n * a.n * a.n > (double)b.n * b.n * b.n;
+    });
+    if (err == LM_OK && cudaMemcpyAsync(ln->d_items, ln->h_items, sizeof(lm::BatchItem) * k, cudaMemcpyHostToDevice,
+                                        ln->st) != cudaSuccess)
+      err = LM_ERR_CUDA;
+    if (err == LM_OK) {
+      lm::BatchArgs g;
+      g.items = ln->d_items;
+      g.count = k;
+      g.prec = s->cfg.small_precision;
+      g.nmax = nmax;
+      g.rmax = rmax;
+      g.nbmax = nbmax;
+      g.A = reinterpret_cast<const double*>(base);
+      g.B = reinterpret_cast<const double*>(base);
+      g.X = reinterpret_cast<double*>(base);
+      g.F = reinterpret_cast<double*>(base);
+      g.ipiv = reinterpret_cast<int*>(base);
+      g.info = ln->d_info;
+      g.iters = ln->d_iters;
+      g.berr = ln->d_berr;
+      g.ticket = ln->d_ticket;
+      g.tol = 0.0;
+      g.max_iter = 10;
+      const size_t smem = lm::batch_smem_bytes(nmax, rmax, nbmax);
+      int per_sm = 1;
+      err = lm::batch_occupancy(smem, &per_sm);
+      const int grid = std::max(1, std::min(k, std::max(per_sm, 1) * s->num_sms));
+      if (err == LM_OK) err = lm::batch_launch(g, grid, smem, ln->st);
+    }
+    for (int i = 0; i < k && err == LM_OK; ++i) {
+      Req* r = jobs[i];
+      if (cudaMemcpyAsync(r->X, base + r->off + r->oX, (size_t)r->n * r->nrhs * 8, cudaMemcpyDeviceToHost, ln->st) !=
+          cudaSuccess)
+        err = LM_ERR_CUDA;
+    }
+    if (err == LM_OK) {
+      cudaMemcpyAsync(ln->h_info, ln->d_info, sizeof(int) * k, cudaMemcpyDeviceToHost, ln->st);
+      cudaMemcpyAsync(ln->h_iters, ln->d_iters, sizeof(int) * k, cudaMemcpyDeviceToHost, ln->st);
+      if (cudaStreamSynchronize(ln->st) != cudaSuccess) err = LM_ERR_CUDA;
+    }
+    lk.lock();
+    for (int i = 0; i < k; ++i) {
+      Req* r = jobs[i];
+      r->status = err != LM_OK ? err : ln->h_info[i];
+      r->iters = err != LM_OK ? 0 : ln->h_iters[i];
+      r->fallback = err == LM_OK && ln->h_iters[i] < 0;
+      complete(s, r);
+    }
+    ln->busy_s += now_s() - t0;
+    ++ln->batches;
+    ln->solved += k;
+    ln->jobs.clear();
+    ln->busy = false;
+    pump(s);
+    s->cv_done.notify_all();
+  }
+}
+
+// ---- worker: one larger request at a time on its own context -------------------------
+int worker_solve(lm_server* s, Worker* w, Req* r) {
+  char* blk = s->arena.base + r->off;
+  double* dA = reinterpret_cast<double*>(blk + r->oA);
+  double* dB = reinterpret_cast<double*>(blk + r->oB);
+  double* dX = reinterpret_cast<double*>(blk + r->oX);
+  int* dP = reinterpret_cast<int*>(blk + r->oP);
+  cudaStream_t st = static_cast<cudaStream_t>(lm_ctx_get_stream(w->ctx));
+  const size_t nn = (size_t)r->n * r->n * 8, nr = (size_t)r->n * r->nrhs * 8;
+  LM_CUDA_TRY(cudaMemcpyAsync(dA, r->A, nn, cudaMemcpyHostToDevice, st));
+  LM_CUDA_TRY(cudaMemcpyAsync(dB, r->B, nr, cudaMemcpyHostToDevice, st));
+  int info = 0, rc = LM_OK;
+  bool fp64 = true;
+  if (r->kind == LM_BATCH_GENERAL && s->cfg.large_precision == LM_PREC_FP32_IR) {
+    int it = 0;
+    double be = 0;
+    rc = lm_dgesv_ir(w->ctx, r->n, r->nrhs, dA, r->n, dB, r->nrhs, dX, r->nrhs, 0.0, 30, &it, &be, &info);
+    if (rc == LM_OK) {
+      fp64 = false;
+      r->iters = it;
+    } else if (rc == LM_ERR_NOT_CONVERGED || rc > 0) {
+      r->fallback = true;
+      r->iters = -1;
+    } else {
+      return rc;
+    }
+  }
+  if (fp64) {
+    LM_CUDA_TRY(cudaMemcpyAsync(dX, dB, nr, cudaMemcpyDeviceToDevice, st));
+    rc = r->kind == LM_BATCH_GENERAL ? lm_dgesv(w->ctx, r->n, r->nrhs, dA, r->n, dP, dX, r->nrhs, &info)
+                                      : lm_dposv(w->ctx, r->n, r->nrhs, dA, r->n, dX, r->nrhs, &info);
+    if (rc < 0) return rc;
+  }
+  LM_CUDA_TRY(cudaMemcpyAsync(r->X, dX, nr, cudaMemcpyDeviceToHost, st));
+  LM_CUDA_TRY(cudaStreamSynchronize(st));
+  return info;
+}
+
+void worker_run(Worker* w) {
+  lm_server* s = w->s;
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    w->cv.wait(lk, [&] { return w->busy || s->stopping; });
+    if (!w->busy && s->stopping) return;
+    Req* r = w->job;
+    lk.unlock();
+    const double t0 = now_s();
+    const int st = worker_solve(s, w, r);
+    lk.lock();
+    r->status = st;
+    complete(s, r);
+    w->busy_s += now_s() - t0;
+    w->job = nullptr;
+    w->busy = false;
+    pump(s);
+    s->cv_done.notify_all();
+  }
+}
+
+void server_stop(lm_server* s) {
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    // queued requests that never started are cancelled; admitted ones finish
+    for (Req* r : s->pending) {
+      r->cancelled = true;
+      r->done = true;
+      r->status = LM_ERR_ARG;
+      ++s->cancelled;
+    }
+    s->pending.clear();
+    s->cv_done.wait(lk, [&] { return s->inflight == 0; });
+    s->stopping = true;
+    for (Lane* ln : s->lanes) ln->cv.notify_all();
+    for (Worker* w : s->workers) w->cv.notify_all();
+  }
+  for (Lane* ln : s->lanes)
+    if (ln->th.joinable()) ln->th.join();
+  for (Worker* w : s->workers)
+    if (w->th.joinable()) w->th.join();
+}
+
+void server_free(lm_server* s) {
+  for (Lane* ln : s->lanes) {
+    cudaFree(ln->d_items);
+    cudaFree(ln->d_info);
+    cudaFree(ln->d_iters);
+    cudaFree(ln->d_berr);
+    cudaFree(ln->d_ticket);
+    cudaFreeHost(ln->h_items);
+    cudaFreeHost(ln->h_info);
+    cudaFreeHost(ln->h_iters);
+    if (ln->st) cudaStreamDestroy(ln->st);
+    delete ln;
+  }
+  for (Worker* w : s->workers) {
+    if (w->ctx) lm_ctx_destroy(w->ctx);
+    delete w;
+  }
+  cudaFree(s->arena.base);
+  for (auto& kv : s->live) delete kv.second;
+  delete s;
+}
+
+// Grow a worker context's workspaces to the largest admissible request with
+// one solve of each kind (SPD diagonal matrix, so every path succeeds).
+int prewarm(lm_server* s, Worker* w) {
+  const int n = s->cfg.max_n, r = s->cfg.max_nrhs;
+  double *A = nullptr, *B = nullptr, *X = nullptr;
+  int* P = nullptr;
+  const size_t nn = (size_t)n * n * 8, nr = (size_t)n * r * 8;
+  LM_CUDA_TRY(cudaMalloc(&A, nn));
+  LM_CUDA_TRY(cudaMalloc(&B, nr));
+  LM_CUDA_TRY(cudaMalloc(&X, nr));
+  LM_CUDA_TRY(cudaMalloc(&P, (size_t)n * 4));
+  std::vector<double> h((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) h[(size_t)i * n + i] = 1.0 + i % 7;
+  int rc = LM_OK;
+  if (cudaMemcpy(A, h.data(), nn, cudaMemcpyHostToDevice) != cudaSuccess || cudaMemset(B, 0, nr) != cudaSuccess)
+    rc = LM_ERR_CUDA;
+  int it = 0, info = 0;
+  double be = 0;
+  if (rc == LM_OK && s->cfg.large_precision == LM_PREC_FP32_IR) {
+    // both substitution paths: few right-hand sides and many
+    for (int rr : {1, r}) {
+      rc = lm_dgesv_ir(w->ctx, n, rr, A, n, B, rr, X, rr, 0.0, 30, &it, &be, &info);
+      if (rc > 0 || rc == LM_ERR_NOT_CONVERGED) rc = LM_OK;
+      if (rc != LM_OK) break;
+    }
+  }
+  if (rc == LM_OK) rc = lm_dgesv(w->ctx, n, r, A, n, P, X, r, &info);
+  if (rc == LM_OK) {
+    cudaMemcpy(A, h.data(), nn, cudaMemcpyHostToDevice);
+    rc = lm_dposv(w->ctx, n, r, A, n, X, r, &info);
+  }
+  if (rc > 0) rc = LM_OK;
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(X);
+  cudaFree(P);
+  return rc;
+}
+
+int server_init(lm_server* s) {
+  LM_CUDA_TRY(cudaSetDevice(s->device));
+  LM_CUDA_TRY(cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device));
+  size_t free_b = 0, total_b = 0;
+  LM_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b));
+  // workers first (their pre-grown workspaces are fixed overhead)
+  for (int i = 0; i < s->cfg.large_workers; ++i) {
+    Worker* w = new Worker;
+    w->s = s;
+    s->workers.push_back(w);
+    LM_TRY(lm_ctx_create(&w->ctx, s->device));
+    lm::ctx_set_graphs(w->ctx, false);  // arena addresses change per request
+    LM_TRY(prewarm(s, w));
+  }
+  size_t free_after = 0;
+  LM_CUDA_TRY(cudaMemGetInfo(&free_after, &total_b));
+  s->fixed_bytes = free_b > free_after ? free_b - free_after : 0;
+  size_t budget = s->cfg.hbm_budget;
+  if (budget == 0) budget = free_after / 4;
+  budget = rup(budget);
+  char* base = nullptr;
+  if (cudaMalloc(&base, budget) != cudaSuccess) {
+    cudaGetLastError();
+    lm::set_last_error("server: arena allocation failed");
+    return LM_ERR_NOMEM;
+  }
+  s->arena.init(base, budget);
+  const int mb = s->cfg.max_batch;
+  for (int i = 0; i < s->cfg.batch_lanes; ++i) {
+    Lane* ln = new Lane;
+    ln->s = s;
+    ln->idx = i;
+    s->lanes.push_back(ln);
+    LM_CUDA_TRY(cudaStreamCreateWithFlags(&ln->st, cudaStreamNonBlocking));
+    LM_CUDA_TRY(cudaMalloc(&ln->d_items, sizeof(lm::BatchItem) * mb));
+    LM_CUDA_TRY(cudaMalloc(&ln->d_info, sizeof(int) * mb));
+    LM_CUDA_TRY(cudaMalloc(&ln->d_iters, sizeof(int) * mb));
+    LM_CUDA_TRY(cudaMalloc(&ln->d_berr, sizeof(double) * mb));
+    LM_CUDA_TRY(cudaMalloc(&ln->d_ticket, sizeof(int) * 4));
+    LM_CUDA_TRY(cudaMallocHost(&ln->h_items, sizeof(lm::BatchItem) * mb));
+    LM_CUDA_TRY(cudaMallocHost(&ln->h_info, sizeof(int) * mb));
+    LM_CUDA_TRY(cudaMallocHost(&ln->h_iters, sizeof(int) * mb));
+  }
+  // the batch kernel's shared-memory limit for the largest micro-batch shape
+  int per_sm = 0;
+  LM_TRY(lm::batch_occupancy(lm::batch_smem_bytes(s->cfg.small_max_n, 16, 32), &per_sm));
+  for (Lane* ln : s->lanes) ln->th = std::thread(lane_run, ln);
+  for (Worker* w : s->workers) w->th = std::thread(worker_run, w);
+  return LM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lm_server_default_config(lm_server_config* c) {
+  if (!c) return LM_ERR_ARG;
+  std::memset(c, 0, sizeof(*c));
+  c->hbm_budget = 0;
+  c->large_workers = 4;
+  c->batch_lanes = 2;
+  c->small_max_n = 256;
+  c->small_precision = LM_PREC_FP64;
+  c->large_precision = LM_PREC_FP32_IR;
+  c->max_batch = 4096;
+  c->max_n = 4096;
+  c->max_nrhs = 64;
+  for (int b = 0; b < 4; ++b) c->nb[b] = 16;
+  return LM_OK;
+}
+
+int lm_server_create(lm_server** out, int device, const lm_server_config* cfg) {
+  if (!out) return LM_ERR_ARG;
+  *out = nullptr;
+  lm_server_config c;
+  if (cfg) {
+    c = *cfg;
+  } else {
+    lm_server_default_config(&c);
+  }
+  if (c.large_workers < 1 || c.large_workers > 32 || c.batch_lanes < 1 || c.batch_lanes > 8 || c.small_max_n < 0 ||
+      c.small_max_n > lm::BatchLimits::kMaxN || c.max_batch < 1 || c.max_n < 1 || c.max_nrhs < 1 ||
+      c.max_nrhs > 64 || (c.small_precision != LM_PREC_FP64 && c.small_precision != LM_PREC_FP32_IR) ||
+      (c.large_precision != LM_PREC_FP64 && c.large_precision != LM_PREC_FP32_IR))
+    return LM_ERR_ARG;
+  for (int b = 0; b < 4; ++b)
+    if (c.nb[b] != 8 && c.nb[b] != 16 && c.nb[b] != 32) return LM_ERR_ARG;
+  lm_server* s = new lm_server;
+  s->device = device;
+  s->cfg = c;
+  const int r = server_init(s);
+  if (r != LM_OK) {
+    server_stop(s);
+    server_free(s);
+    return r;
+  }
+  *out = s;
+  return LM_OK;
+}
+
+int lm_server_submit(lm_server* s, int n, int nrhs, int kind, const double* A, const double* B, double* X,
+                     long long* id) {
+  if (!s || !id) return LM_ERR_ARG;
+  *id = 0;
+  if (n < 1 || nrhs < 1 || !A || !B || !X || (kind != LM_BATCH_GENERAL && kind != LM_BATCH_SPD) ||
+      n > s->cfg.max_n || nrhs > s->cfg.max_nrhs) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    ++s->rejected;
+    lm::set_last_error("server: request outside the admissible sizes");
+    return LM_ERR_ARG;
+  }
+  Req* r = new Req;
+  r->n = n;
+  r->nrhs = nrhs;
+  r->kind = kind;
+  r->A = A;
+  r->B = B;
+  r->X = X;
+  r->small = n <= s->cfg.small_max_n && nrhs <= lm::BatchLimits::kMaxRhs;
+  r->bytes = layout(*r);
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->stopping) {
+    delete r;
+    return LM_ERR_ARG;
+  }
+  if (rup(r->bytes) > s->arena.size) {
+    ++s->rejected;
+    delete r;
+    lm::set_last_error("server: request larger than the whole HBM budget");
+    return LM_ERR_NOMEM;
+  }
+  r->id = s->next_id++;
+  r->t_submit = now_s();
+  if (s->t_first == 0) s->t_first = r->t_submit;
+  s->live[r->id] = r;
+  s->pending.push_back(r);
+  s->queue_peak = std::max(s->queue_peak, s->pending.size());
+  pump(s);
+  *id = r->id;
+  return LM_OK;
+}
+
+int lm_server_test(lm_server* s, long long id, int* done, int* status, double* latency_ms) {
+  if (!s || !done) return LM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return LM_ERR_ARG;
+  Req* r = it->second;
+  *done = r->done ? 1 : 0;
+  if (r->done) {
+    if (status) *status = r->status;
+    if (latency_ms) *latency_ms = r->cancelled ? 0.0 : (r->t_done - r->t_submit) * 1e3;
+    s->live.erase(it);
+    delete r;
+  }
+  return LM_OK;
+}
+
+int lm_server_wait(lm_server* s, long long id, int* status, double* latency_ms, double timeout_s) {
+  if (!s) return LM_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return LM_ERR_ARG;
+  Req* r = it->second;
+  const auto pred = [&] { return r->done; };
+  if (timeout_s > 0) {
+    if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) return LM_ERR_TIMEOUT;
+  } else {
+    s->cv_done.wait(lk, pred);
+  }
+  if (status) *status = r->status;
+  if (latency_ms) *latency_ms = r->cancelled ? 0.0 : (r->t_done - r->t_submit) * 1e3;
+  s->live.erase(id);
+  delete r;
+  return LM_OK;
+}
+
+int lm_server_cancel(lm_server* s, long long id) {
+  if (!s) return LM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->live.find(id);
+  if (it == s->live.end()) return LM_ERR_ARG;
+  Req* r = it->second;
+  auto q = std::find(s->pending.begin(), s->pending.end(), r);
+  if (q == s->pending.end()) return LM_ERR_UNSUPPORTED;  // already admitted (or done)
+  s->pending.erase(q);
+  r->cancelled = true;
+  r->done = true;
+  r->status = LM_ERR_ARG;
+  ++s->cancelled;
+  s->cv_done.notify_all();
+  return LM_OK;
+}
+
+int lm_server_drain(lm_server* s, double timeout_s) {
+  if (!s) return LM_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  const auto pred = [&] { return s->pending.empty() && s->inflight == 0; };
+  if (timeout_s > 0) {
+    if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) return LM_ERR_TIMEOUT;
+  } else {
+    s->cv_done.wait(lk, pred);
+  }
+  return LM_OK;
+}
+
+int lm_server_stats(lm_server* s, lm_server_stats_t* o) {
+  if (!s || !o) return LM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  std::memset(o, 0, sizeof(*o));
+  o->completed = s->completed;
+  o->rejected = s->rejected;
+  o->cancelled = s->cancelled;
+  o->failed = s->failed;
+  o->fp64_fallbacks = s->fallbacks;
+  o->queue_peak = (long long)s->queue_peak;
+  o->inflight_peak = s->inflight_peak;
+  o->arena_bytes = s->arena.size;
+  o->arena_peak_bytes = s->arena.peak;
+  o->fixed_bytes = s->fixed_bytes;
+  o->pending = (long long)s->pending.size();
+  o->inflight = s->inflight;
+  std::vector<double> v = s->lat_ms;
+  if (!v.empty()) {
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double p) {
+      const double pos = p * (v.size() - 1);
+      const size_t i = (size_t)pos;
+      const double f = pos - i;
+      return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+    };
+    o->p50_ms = pct(0.50);
+    o->p99_ms = pct(0.99);
+    o->max_ms = v.back();
+    double sum = 0;
+    for (double x : v) sum += x;
+    o->mean_ms = sum / v.size();
+  }
+  const double span = s->t_last > s->t_first ? s->t_last - s->t_first : 0.0;
+  o->span_s = span;
+  o->solves_per_s = span > 0 ? s->completed / span : 0.0;
+  o->tflops = span > 0 ? s->flops_done / span / 1e12 : 0.0;
+  long long batches = 0, small = 0;
+  for (Lane* ln : s->lanes) {
+    batches += ln->batches;
+    small += ln->solved;
+  }
+  o->micro_batches = batches;
+  o->small_solved = small;
+  return LM_OK;
+}
+
+int lm_server_reset_stats(lm_server* s) {
+  if (!s) return LM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->lat_ms.clear();
+  s->completed = s->rejected = s->cancelled = s->failed = s->fallbacks = 0;
+  s->queue_peak = 0;
+  s->inflight_peak = s->inflight;
+  s->t_first = s->t_last = 0;
+  s->flops_done = 0;
+  s->arena.peak = s->arena.in_use;
+  for (Lane* ln : s->lanes) ln->batches = ln->solved = 0;
+  return LM_OK;
+}
+
+int lm_server_destroy(lm_server* s) {
+  if (!s) return LM_OK;
+  server_stop(s);
+  server_free(s);
+  return LM_OK;
+}
+
+}  // extern "C"

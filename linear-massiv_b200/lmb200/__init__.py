@@ -41,6 +41,8 @@ EXPORTS = [
     "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_dpotrf_noalloc",
     "lm_batch_create", "lm_batch_destroy", "lm_batch_offsets", "lm_batch_solve", "lm_batch_results",
     "lm_batch_factors", "lm_batch_solve_host", "lm_batch_tune", "lm_batch_tune_get", "lm_batch_tune_set",
+    "lm_server_default_config", "lm_server_create", "lm_server_submit", "lm_server_test", "lm_server_wait",
+    "lm_server_cancel", "lm_server_drain", "lm_server_stats", "lm_server_reset_stats", "lm_server_destroy",
 ]
 
 BATCH_GENERAL = 0
@@ -123,6 +125,16 @@ def _lib():
                 "lm_batch_tune": ([vp, i, ctypes.c_char_p], i),
                 "lm_batch_tune_get": ([vp, ip], i),
                 "lm_batch_tune_set": ([vp, ip], i),
+                "lm_server_default_config": ([vp], i),
+                "lm_server_create": ([ctypes.POINTER(vp), i, vp], i),
+                "lm_server_submit": ([vp, i, i, i, vp, vp, vp, ctypes.POINTER(ctypes.c_longlong)], i),
+                "lm_server_test": ([vp, ctypes.c_longlong, ip, ip, dp], i),
+                "lm_server_wait": ([vp, ctypes.c_longlong, ip, dp, d], i),
+                "lm_server_cancel": ([vp, ctypes.c_longlong], i),
+                "lm_server_drain": ([vp, d], i),
+                "lm_server_stats": ([vp, vp], i),
+                "lm_server_reset_stats": ([vp], i),
+                "lm_server_destroy": ([vp], i),
             }
             for name, (args, res) in sigs.items():
                 fn = getattr(L, name)
@@ -549,3 +561,109 @@ def batch_tune_set(table, ctx: Context | None = None):
     ctx = ctx or default_context(0)
     t = (ctypes.c_int * 8)(*(list(table[0]) + list(table[1])))
     _check(_lib().lm_batch_tune_set(ctx.h, t), "lm_batch_tune_set")
+
+
+# ---- serving loop ----------------------------------------------------------------
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("large_workers", ctypes.c_int), ("batch_lanes", ctypes.c_int),
+                ("small_max_n", ctypes.c_int), ("small_precision", ctypes.c_int), ("large_precision", ctypes.c_int),
+                ("max_batch", ctypes.c_int), ("max_n", ctypes.c_int), ("max_nrhs", ctypes.c_int),
+                ("nb", ctypes.c_int * 4)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_longlong), ("rejected", ctypes.c_longlong), ("cancelled", ctypes.c_longlong),
+                ("failed", ctypes.c_longlong), ("fp64_fallbacks", ctypes.c_longlong),
+                ("queue_peak", ctypes.c_longlong), ("pending", ctypes.c_longlong),
+                ("micro_batches", ctypes.c_longlong), ("small_solved", ctypes.c_longlong),
+                ("inflight", ctypes.c_int), ("inflight_peak", ctypes.c_int),
+                ("arena_bytes", ctypes.c_size_t), ("arena_peak_bytes", ctypes.c_size_t),
+                ("fixed_bytes", ctypes.c_size_t),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
+                ("max_ms", ctypes.c_double), ("span_s", ctypes.c_double), ("solves_per_s", ctypes.c_double),
+                ("tflops", ctypes.c_double)]
+
+
+class Server:
+    """Continuous-batching solve server (lm_server_*).  submit() takes host
+    numpy arrays (A n x n, B n x nrhs, float64, C order); the arrays are kept
+    referenced until the request completes."""
+
+    def __init__(self, device: int = 0, **cfg):
+        c = ServerConfig()
+        _check(_lib().lm_server_default_config(ctypes.byref(c)), "lm_server_default_config")
+        for k, v in cfg.items():
+            if k == "nb":
+                c.nb = (ctypes.c_int * 4)(*v)
+            else:
+                setattr(c, k, v)
+        self.config = c
+        h = ctypes.c_void_p()
+        _check(_lib().lm_server_create(ctypes.byref(h), device, ctypes.byref(c)), "lm_server_create")
+        self.h = h
+        self._keep = {}
+
+    def submit(self, A, B, kind: int = BATCH_GENERAL):
+        """Queue A X = B; returns (id, X) with X the output array (filled on completion)."""
+        import numpy as np
+
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        B2 = np.ascontiguousarray(B.reshape(A.shape[0], -1), dtype=np.float64)
+        X = np.empty_like(B2)
+        rid = ctypes.c_longlong(0)
+        _check(_lib().lm_server_submit(self.h, A.shape[0], B2.shape[1], kind, ctypes.c_void_p(A.ctypes.data),
+                                       ctypes.c_void_p(B2.ctypes.data), ctypes.c_void_p(X.ctypes.data),
+                                       ctypes.byref(rid)), "lm_server_submit")
+        self._keep[rid.value] = (A, B2, X)
+        return rid.value, X
+
+    def submit_raw(self, n, nrhs, kind, A_ptr, B_ptr, X_ptr):
+        """Queue with caller-managed buffers (addresses as ints); returns the id."""
+        rid = ctypes.c_longlong(0)
+        _check(_lib().lm_server_submit(self.h, n, nrhs, kind, ctypes.c_void_p(A_ptr), ctypes.c_void_p(B_ptr),
+                                       ctypes.c_void_p(X_ptr), ctypes.byref(rid)), "lm_server_submit")
+        return rid.value
+
+    def wait(self, rid: int, timeout_s: float = 0.0):
+        """Block until done: (status, latency_ms)."""
+        st, lat = ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(_lib().lm_server_wait(self.h, rid, ctypes.byref(st), ctypes.byref(lat), float(timeout_s)),
+               "lm_server_wait")
+        self._keep.pop(rid, None)
+        return st.value, lat.value
+
+    def test(self, rid: int):
+        """Non-blocking: (done, status, latency_ms)."""
+        dn, st, lat = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_double(0.0)
+        _check(_lib().lm_server_test(self.h, rid, ctypes.byref(dn), ctypes.byref(st), ctypes.byref(lat)),
+               "lm_server_test")
+        if dn.value:
+            self._keep.pop(rid, None)
+        return bool(dn.value), st.value, lat.value
+
+    def cancel(self, rid: int) -> int:
+        return _lib().lm_server_cancel(self.h, rid)
+
+    def drain(self, timeout_s: float = 0.0):
+        _check(_lib().lm_server_drain(self.h, float(timeout_s)), "lm_server_drain")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_lib().lm_server_stats(self.h, ctypes.byref(st)), "lm_server_stats")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def reset_stats(self):
+        _check(_lib().lm_server_reset_stats(self.h), "lm_server_reset_stats")
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib().lm_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
