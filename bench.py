@@ -2,16 +2,21 @@
 """Benchmark of the B200 dense-solve path (one JSON line on rank 0).
 
 Workloads (--workload):
-  lu    (default) luSolve, A n x n i.i.d. uniform[-1,1] (numpy Philox, seeded),
+  lu    luSolve, A n x n i.i.d. uniform[-1,1] (numpy Philox, seeded),
         b uniform[-1,1], nrhs right-hand sides; one step = copy A into the
         work buffer (luSolveP's thaw), LU with partial pivoting, solve.
   chol  choleskySolve with A = B B^T + n I, B uniform[-1,1].
   gemm  C = A B, m = n = k.
-  ir    mixed precision: FP32 LU with tcgen05 3xTF32 updates, refined in FP64
-        to the normwise backward error 1e-15 n; A = U diag(sigma) V^T with U, V
-        products of seeded Householder reflectors and sigma geometric from 1
-        to 1/kappa (--kappa; 0 = uniform[-1,1] A).  The plain FP64 LU solve of
-        the same system is timed beside it.
+  ir    (default) mixed precision: random butterflies + FP32 LU without
+        pivoting with tcgen05 3xTF32 updates (partial pivoting if refinement
+        stalls), refined in FP64 to the normwise backward error 1e-15 n;
+        A = U diag(sigma) V^T with U, V products of seeded Householder
+        reflectors and sigma geometric from 1 to 1/kappa (--kappa; 0 =
+        uniform[-1,1] A).  The plain FP64 LU solve of the same system is timed
+        beside it (the metric's comparison).
+The timed region replays the solve's captured CUDA graphs; per-kernel CUDA
+events (the roofline's kernel time and the phase breakdown) come from
+--profile-steps extra steps after it.
 Metric: FP64-accurate solves per second (GEMMs per second for gemm), whole
 job.  Multi-GPU: replicas only — every rank solves its own system, no
 collective on the data path; value = all solves / max-over-ranks time.
@@ -57,7 +62,7 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir", "batch", "serve"], default="lu")
+    p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir", "batch", "serve"], default="ir")
     p.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (requests/s)")
     p.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
     p.add_argument("--pool", type=int, default=48, help="serve: distinct pregenerated systems")
@@ -74,7 +79,8 @@ def parse():
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS DGEMM peak measurement")
     p.add_argument("--k", type=int, default=0, help="gemm inner dimension (default n); k < n adds beta = 1")
-    p.add_argument("--no-profile", action="store_true", help="time without the per-phase event tracing")
+    p.add_argument("--profile-steps", type=int, default=1,
+                   help="steps run with per-kernel CUDA events after the timed region (0 = none)")
     return p.parse_args()
 
 
@@ -513,21 +519,35 @@ def make_inputs(a, rank, torch, np):
 
 def measure_fp64_peak(torch):
     """cuBLAS DGEMM 8192^3 throughput on this GPU (the FP64 roofline denominator)."""
+    return _measure_peak(torch, torch.float64, False)
+
+
+def measure_tf32_peak(torch):
+    """cuBLAS FP32-storage GEMM with TF32 tensor cores, 8192^3 (the TF32 denominator)."""
+    return _measure_peak(torch, torch.float32, True)
+
+
+def _measure_peak(torch, dtype, tf32):
     n = 8192
-    x = torch.rand((n, n), dtype=torch.float64, device="cuda")
-    y = torch.rand((n, n), dtype=torch.float64, device="cuda")
-    for _ in range(2):
-        torch.matmul(x, y)
-    best = 0.0
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(x, y)
-        e1.record()
-        torch.cuda.synchronize()
-        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3))
-    del x, y
-    torch.cuda.empty_cache()
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = tf32
+    try:
+        x = torch.rand((n, n), dtype=dtype, device="cuda")
+        y = torch.rand((n, n), dtype=dtype, device="cuda")
+        for _ in range(2):
+            torch.matmul(x, y)
+        best = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(x, y)
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3))
+        del x, y
+        torch.cuda.empty_cache()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
     return best / 1e12
 
 
@@ -608,6 +628,22 @@ def run_reference(a, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes per unit of algorithmic work of the dominant kernel, from the ncu
+# captures summarised under profiles/ (dram__bytes_read.sum + write.sum of one
+# launch divided by that launch's algorithmic bytes); the per-launch traffic
+# of this run is that ratio times its own average algorithmic bytes per launch.
+DRAM_PER_ALGO_BYTE = {
+    "dgemm": 1.11e9 / 1.090e9,   # profiles/dgemm_dmma_k128_n8192.md
+}
+
+
+def traffic_per_launch(a, gp, steps):
+    key = "dgemm" if a.workload in ("lu", "chol", "gemm") else None
+    if key is None or key not in DRAM_PER_ALGO_BYTE or not gp.get("launches"):
+        return None
+    return DRAM_PER_ALGO_BYTE[key] * gp["bytes"] / gp["launches"]
+
+
 # ---- our arm ------------------------------------------------------------------------------
 
 def run_ours(a, world, rank, local):
@@ -659,6 +695,7 @@ def run_ours(a, world, rank, local):
         step()
     torch.cuda.synchronize()
     ctx.check()
+    ir_method = ctx.ir_last_method() if a.workload == "ir" else None
     # accuracy of the last warm-up result (FP64 backward error, checked on the GPU)
     accuracy = {}
     if a.workload != "gemm":
@@ -667,10 +704,11 @@ def run_ours(a, world, rank, local):
         den = A_d.abs().sum(dim=1).max().item() * X.abs().max().item() + B_d.abs().max().item()
         accuracy = {"backward_error": num / den, "bound": 1e-15 * n}
         del R
-    peak = measure_fp64_peak(torch) if (rank == 0 and not a.no_peak) else None
+    peak = None
+    if rank == 0 and not a.no_peak:
+        peak = measure_tf32_peak(torch) if a.workload == "ir" else measure_fp64_peak(torch)
 
-    ctx.profile(not a.no_profile)
-    ctx.profile_read()
+    # Timed region: the captured CUDA graphs of the solve, no per-kernel events.
     launches0 = lmb200.launch_count()
     clocks = Clocks(local)
     barrier(world)
@@ -687,10 +725,27 @@ def run_ours(a, world, rank, local):
     clk = clocks.stop()
     t_local = e0.elapsed_time(e1) * 1e-3
     launches = lmb200.launch_count() - launches0
-    phases = ctx.profile_read()
-    ctx.profile(False)
     t = max_over_ranks(t_local, world)
     value = world * a.steps / t
+
+    # Kernel breakdown: the same step with CUDA events around every kernel
+    # group on the launching stream (eager launches), right after the timed
+    # region.  The roofline's achieved rate is the dominant kernel's
+    # algorithmic work divided by its event-timed duration here.
+    phases = None
+    prof_ms = None
+    if a.profile_steps > 0:
+        ctx.profile(True)
+        ctx.profile_read()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record()
+        for _ in range(a.profile_steps):
+            step()
+        p1.record()
+        torch.cuda.synchronize()
+        prof_ms = p0.elapsed_time(p1) / a.profile_steps
+        phases = ctx.profile_read()
+        ctx.profile(False)
 
     # IR: time the plain FP64 LU solve of the same system beside it
     fp64_ref = None
@@ -753,9 +808,16 @@ def run_ours(a, world, rank, local):
 
     if rank != 0:
         return
-    gp = phases["gemm"]
+    ps = max(a.profile_steps, 1)
+    gp = phases["gemm"] if phases else {"flops": 0.0, "ms": 0.0, "launches": 0}
     achieved = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
-    total_ms = sum(p["ms"] for p in phases.values())
+    total_ms = sum(p["ms"] for p in phases.values()) if phases else 0.0
+    if a.workload == "ir":
+        roof_kernel = "sgemm_tf32_kernel (tcgen05 kind::tf32, 3xTF32 split: 3 MMAs per logical product)"
+        peak_src = "cuBLAS TF32 GEMM (FP32 storage, allow_tf32) 8192^3 measured in this run"
+    else:
+        roof_kernel = "dgemm_dmma_kernel (FP64 DMMA)"
+        peak_src = "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)"
     line = {
         "metric": metric_name(a), "value": value, "unit": metric_name(a), "n_gpus": world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * t / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -766,18 +828,22 @@ def run_ours(a, world, rank, local):
         "e2e": {"value": e2e_val, "unit": metric_name(a), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": a.e2e_steps, "api": {"lu": "lm_lu_solve_host", "chol": "lm_chol_solve_host", "gemm": "lm_matmul_host",
                                              "ir": "lm_lu_solve_ir_host"}[a.workload]},
-        "roofline": {"bound": "tensor", "kernel": "dgemm_dmma_kernel (FP64 DMMA trailing updates)",
+        "roofline": {"bound": "tensor", "kernel": roof_kernel,
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
-                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)",
-                     "gemm_launches_per_step": gp["launches"] / a.steps},
-        "phases_ms_per_step": {k: v["ms"] / a.steps for k, v in phases.items()},
-        "phase_share": {k: (v["ms"] / total_ms if total_ms else None) for k, v in phases.items()},
+                     "frac": (achieved / peak) if (achieved and peak) else None,
+                     "traffic": traffic_per_launch(a, gp, ps),
+                     "peak_source": peak_src,
+                     "launches_per_step": gp["launches"] / ps,
+                     "timing": f"CUDA events around each launch of the kernel over {a.profile_steps} profiled "
+                               f"step(s) run after the timed region ({prof_ms and round(prof_ms, 2)} ms per "
+                               f"profiled step, eager launches)"},
+        "phases_ms_per_step": ({k: v["ms"] / ps for k, v in phases.items()} if phases else None),
+        "phase_share": ({k: (v["ms"] / total_ms if total_ms else None) for k, v in phases.items()} if phases else None),
         "tflops_whole_step": (2.0 * n * n * kk if a.workload == "gemm" else FLOPS[a.workload](n, nrhs)) * a.steps / t / 1e12,
         "host_enqueue_ms_per_step": host_enqueue_ms,
-        "profiled": not a.no_profile,
         "accuracy": accuracy,
-        "ir": ({**ir_stats, **(fp64_ref or {})} if a.workload == "ir" else None),
+        "ir": ({**ir_stats, **(fp64_ref or {}), "method": {0: "rbt", 1: "gepp"}.get(ir_method, ir_method)}
+               if a.workload == "ir" else None),
         "clocks": clk,
     }
     if world == 1 and not a.no_cpu_baseline:

@@ -174,6 +174,24 @@ int lm_dgesv_ir(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const do
 int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const double* B, double* X, double tol,
                         int max_iter, int* iters, double* berr, int* info);
 
+/* Factorisation used by the mixed-precision solves of a context (lm_dgesv_ir,
+ * lm_lu_solve_ir_host and the serving loop's large requests).
+ *   LM_IR_RBT (default): A is mixed by two random depth-2 butterfly
+ *     transforms, Ar = U^T A V (Baboulin, Dongarra, Herrmann, Tomov 2013), and
+ *     Ar is factored in FP32 without pivoting, so that everything but the
+ *     128 x 128 diagonal blocks runs on the tensor cores; corrections are
+ *     V Ar^-1 U^T r.  If its refinement stalls (the worst backward error fails
+ *     to halve in one step) or runs out of steps, the solve is redone with
+ *     LM_IR_GEPP, and only that result is reported.
+ *   LM_IR_GEPP: FP32 LU with partial pivoting, as described above.
+ * The stopping test, tolerance and FP64 residual are the same for both. */
+#define LM_IR_RBT 0
+#define LM_IR_GEPP 1
+int lm_ctx_set_ir_method(lm_ctx* ctx, int method);
+/* Method that produced the last mixed-precision result on this context
+ * (LM_IR_RBT, or LM_IR_GEPP after a fallback); -1 before the first solve. */
+int lm_ctx_ir_last_method(lm_ctx* ctx, int* method);
+
 /* ---- factorisation without allocation -----------------------------------------
  * No counterpart in the reference.  lm_dpotrf without any allocation: for
  * callers that cannot call cudaMalloc at call time (a runtime whose memory

@@ -45,6 +45,8 @@ struct Ctx {
   void* ws[kWsSlots] = {};
   size_t ws_bytes[kWsSlots] = {};
   std::mutex mu;
+  int ir_method = LM_IR_RBT;  // lm_ctx_set_ir_method
+  int ir_last = -1;           // method of the last mixed-precision result
   // batch kernel panel width per precision and size bucket (lm_batch_tune)
   int batch_nb[2][BatchLimits::kBuckets] = {{16, 16, 16, 16}, {16, 16, 16, 16}};
 };
@@ -385,6 +387,22 @@ int lm_ctx_check(lm_ctx* ctx) {
   });
 }
 
+int lm_ctx_set_ir_method(lm_ctx* ctx, int method) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (method != LM_IR_RBT && method != LM_IR_GEPP) return LM_ERR_ARG;
+    c.ir_method = method;
+    return LM_OK;
+  });
+}
+
+int lm_ctx_ir_last_method(lm_ctx* ctx, int* method) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (!method) return LM_ERR_ARG;
+    *method = c.ir_last;
+    return LM_OK;
+  });
+}
+
 int lm_ctx_profile(lm_ctx* ctx, int enable) {
   return guarded(ctx, [&](Ctx& c) {
     c.prof = enable != 0;
@@ -522,6 +540,29 @@ int finish_info(Ctx& c, int* info) {
   return r;
 }
 
+// Mixed-precision solve with the context's method: the randomised
+// no-pivoting factor first (LM_IR_RBT), partial pivoting when its refinement
+// stalls.  A zero pivot of the randomised factor only triggers the fallback;
+// the reported info is that of the method whose result is returned.
+int ir_solve(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+             long long ldx, double tol, int max_iter, int* iters, double* berr, const char* tag) {
+  const std::string t(tag);
+  if (c.ir_method == LM_IR_RBT) {
+    const std::string key = lm::gkey(("rbt_ir_" + t).c_str(), {n, (long long)A, lda, nrhs <= 4 ? 1 : 0});
+    int r = lm::dgesv_rbt_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream,
+                             [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+    if (r != LM_ERR_NOT_CONVERGED) {
+      c.ir_last = LM_IR_RBT;
+      return r;
+    }
+    LM_TRY(lm::reset_info(c));
+  }
+  const std::string key = lm::gkey(("sgetrf_ir_" + t).c_str(), {n, (long long)A, lda, nrhs <= 4 ? 1 : 0});
+  c.ir_last = LM_IR_GEPP;
+  return lm::dgesv_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream,
+                      [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+}
+
 }  // namespace
 
 extern "C" {
@@ -631,9 +672,7 @@ int lm_dgesv_ir(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const do
     if (!A || !B || !X || lda < n || ldb < nrhs || ldx < nrhs) return LM_ERR_ARG;
     if (tol <= 0) tol = 1e-15 * n;
     LM_TRY(lm::reset_info(c));
-    const std::string key = lm::gkey("sgetrf_ir", {n, (long long)A, lda});
-    int r = lm::dgesv_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream,
-                         [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+    int r = ir_solve(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, "dev");
     int inf = 0;
     int s = lm::read_status(c, &inf);
     if (s < 0) return s;
@@ -780,9 +819,7 @@ int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const dou
     LM_TRY(h2d_2d(c, hb.B, hb.ldb, B, nrhs, n, nrhs));
     LM_TRY(lm::reset_info(c));
     double* dX = hb.B + nrhs;
-    const std::string key = lm::gkey("sgetrf_ir_host", {n, (long long)hb.A, hb.lda});
-    int r = lm::dgesv_ir(c, n, nrhs, hb.A, hb.lda, hb.B, hb.ldb, dX, hb.ldb, tol, max_iter, iters, berr, c.stream,
-                         [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+    int r = ir_solve(c, n, nrhs, hb.A, hb.lda, hb.B, hb.ldb, dX, hb.ldb, tol, max_iter, iters, berr, "host");
     if (r < 0 && r != LM_ERR_NOT_CONVERGED) return r;
     LM_TRY(d2h_2d(c, X, nrhs, dX, hb.ldb, n, nrhs));
     int inf = 0;

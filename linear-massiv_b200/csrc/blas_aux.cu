@@ -113,6 +113,101 @@ __global__ void __launch_bounds__(kSwapThreads) laswp_kernel(T* A, long long lda
     if (active) A[(long long)list_r[i] * lda + col] = stage[i * 32 + lane];
 }
 
+// The same interchanges split in two launches for wide matrices: one CTA
+// composes the swaps ipiv[k0..k1) into the list of (row, source row) pairs
+// that change (plan[0] = count, then rows, then sources, 2 * kSwapChunk
+// each), so that the column blocks need no serial prologue of their own.
+__global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int nrows, const int* __restrict__ ipiv, int k0,
+                                                                 int k1, int* plan, int* status) {
+  __shared__ int rows[2 * kSwapChunk];
+  __shared__ int src[2 * kSwapChunk];
+  __shared__ int piv[kSwapChunk];
+  __shared__ int hkey[kHash];
+  __shared__ short hval[kHash];
+  __shared__ int m_sh, mm_sh;
+  const int tid = threadIdx.x;
+  const int cnt = k1 - k0;
+  for (int i = tid; i < kHash; i += kSwapThreads) hkey[i] = -1;
+  for (int i = tid; i < cnt; i += kSwapThreads) {
+    rows[i] = k0 + i;
+    src[i] = k0 + i;
+    piv[i] = __ldg(ipiv + k0 + i);
+  }
+  if (tid == 0) mm_sh = 0;
+  __syncthreads();
+  if (tid == 0) {
+    int m = cnt;
+    for (int q = 0; q < cnt; ++q) {
+      const int k = k0 + q;
+      const int p = piv[q];
+      if (p < 0 || p >= nrows) {
+        atomicCAS(status, 0, LM_DEVERR_BOUNDS);
+        continue;
+      }
+      if (p == k) continue;
+      int sp;
+      if (p >= k0 && p < k1) {
+        sp = p - k0;
+      } else {
+        unsigned h = ((unsigned)p * 2654435761u) & (kHash - 1);
+        while (hkey[h] != -1 && hkey[h] != p) h = (h + 1) & (kHash - 1);
+        if (hkey[h] == p) {
+          sp = hval[h];
+        } else {
+          hkey[h] = p;
+          hval[h] = (short)m;
+          rows[m] = p;
+          src[m] = p;
+          sp = m++;
+        }
+      }
+      const int t = src[q];
+      src[q] = src[sp];
+      src[sp] = t;
+    }
+    m_sh = m;
+  }
+  __syncthreads();
+  for (int i = tid; i < m_sh; i += kSwapThreads)
+    if (src[i] != rows[i]) {
+      const int at = atomicAdd(&mm_sh, 1);
+      plan[1 + at] = rows[i];
+      plan[1 + 2 * kSwapChunk + at] = src[i];
+    }
+  __syncthreads();
+  if (tid == 0) plan[0] = mm_sh;
+}
+
+// Gather every changing row's source over a 32-column block into shared
+// memory, then scatter (the plan of swap_plan_kernel).
+template <typename T>
+__global__ void __launch_bounds__(kSwapThreads) swap_apply_kernel(T* A, long long lda, const int* __restrict__ plan,
+                                                                  int ca0, int ca1, int cb0, int cb1) {
+  __shared__ int list_r[2 * kSwapChunk];
+  __shared__ int list_s[2 * kSwapChunk];
+  extern __shared__ __align__(16) unsigned char sm[];
+  T* stage = reinterpret_cast<T*>(sm);  // [2 * kSwapChunk][32]
+  const int tid = threadIdx.x;
+  const int mm = __ldg(plan);
+  for (int i = tid; i < mm; i += kSwapThreads) {
+    list_r[i] = __ldg(plan + 1 + i);
+    list_s[i] = __ldg(plan + 1 + 2 * kSwapChunk + i);
+  }
+  __syncthreads();
+  const int na = ca1 - ca0, ncols = na + (cb1 - cb0);
+  const int lane = tid & 31, warp = tid >> 5;
+  const int t = blockIdx.x * 32 + lane;
+  const bool active = t < ncols;
+  const int col = t < na ? ca0 + t : cb0 + (t - na);
+#pragma unroll 8
+  for (int i = warp; i < mm; i += kSwapThreads / 32)
+    if (active) stage[i * 32 + lane] = A[(long long)list_s[i] * lda + col];
+  __syncthreads();
+#pragma unroll 8
+  for (int i = warp; i < mm; i += kSwapThreads / 32)
+    if (active) A[(long long)list_r[i] * lda + col] = stage[i * 32 + lane];
+}
+
 // op(Tri) X = B for one w x 32 column block of B per CTA (w <= 128).  The
 // triangle of op(Tri) is staged packed in shared memory (w(w+1)/2 entries,
 // so two CTAs fit per SM in FP64) together with the block.  Rows are solved
@@ -259,7 +354,7 @@ int grid_for(long long total, int threads, int sms) {
 
 template <typename T>
 int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int ca0, int ca1, int cb0, int cb1,
-          int* status, cudaStream_t st) {
+          int* status, cudaStream_t st, int* plan) {
   ca1 = std::max(ca0, ca1);
   cb1 = std::max(cb0, cb1);
   const int cols = (ca1 - ca0) + (cb1 - cb0);
@@ -270,13 +365,22 @@ int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int c
   cudaGetDevice(&dev);
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(laswp_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    LM_CUDA_TRY(cudaFuncSetAttribute(swap_apply_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set[dev] = true;
   }
+  // wide: plan once, then the column blocks; narrow: one self-contained launch
+  const bool planned = plan != nullptr && cols > 4 * 32;
   for (int s0 = k0; s0 < k1; s0 += kSwapChunk) {
     const int s1 = std::min(k1, s0 + kSwapChunk);
-    laswp_kernel<T><<<cdiv(cols, 32), kSwapThreads, smem, st>>>(A, lda, nrows, ipiv, s0, s1, ca0, ca1, cb0, cb1,
-                                                                status);
-    count_launch(1);
+    if (planned) {
+      swap_plan_kernel<<<1, kSwapThreads, 0, st>>>(nrows, ipiv, s0, s1, plan, status);
+      swap_apply_kernel<T><<<cdiv(cols, 32), kSwapThreads, smem, st>>>(A, lda, plan, ca0, ca1, cb0, cb1);
+      count_launch(2);
+    } else {
+      laswp_kernel<T><<<cdiv(cols, 32), kSwapThreads, smem, st>>>(A, lda, nrows, ipiv, s0, s1, ca0, ca1, cb0, cb1,
+                                                                  status);
+      count_launch(1);
+    }
     LM_CUDA_TRY(cudaGetLastError());
   }
   return LM_OK;
@@ -364,8 +468,9 @@ int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const dou
   return dgemm(c, d, st);
 }
 
-template int laswp<double>(double*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t);
-template int laswp<float>(float*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t);
+template int laswp<double>(double*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t,
+                           int*);
+template int laswp<float>(float*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t, int*);
 template int trsm_left<double>(const double*, long long, int, bool, bool, bool, double*, long long, int,
                                cudaStream_t);
 template int trsm_left<float>(const float*, long long, int, bool, bool, bool, float*, long long, int,

@@ -8,6 +8,11 @@
 //     right half -> swap left half.
 //   Row interchanges are applied to every column of A, matching the
 //   reference's full-row rawSwapRows (fromCol = 0, LU.hs:324-325).
+//   Every U12 = L11^-1 A12 (rawTriSolvePanelTrail, LU.hs:364-407) runs as
+//   inv(L11) (one CTA, blocked inversion in shared memory) times a copy of A12
+//   on the DMMA GEMM: the multipliers are bounded by 1 under partial
+//   pivoting, so the explicit inverse of the unit-lower block is well scaled,
+//   and the block solve leaves the latency-bound substitution kernel.
 // dpotrf — right-looking blocked Cholesky, kNB = 128: diagonal block in SMEM,
 //   L21 = A21 L11^-T (inverse block times the panel, on the tensor cores), then
 //   A22 -= L21 L21^T as a lower-triangle-only GEMM (SYRK tile skip).  Same
@@ -28,8 +33,40 @@ namespace {
 
 constexpr int kNB = 128;
 
+// Scratch of the inverse-based block solves: inv(L11) (kNB x kNB) and the
+// row-interchange plan.
+struct TrsmScratch {
+  double* Linv;
+  int* plan;  // kSwapPlanInts
+};
+
+// B (w x ncols, ldb) <- inv(unit lower L11) B.  Small blocks (inside a panel)
+// in one fused launch; the panel's row block as inv(L11) times B on the
+// tensor cores, written in place: with m = w <= 128 there is one row of
+// output tiles, so each CTA reads exactly the columns of B that it later
+// overwrites, all of them before its epilogue, and no other CTA reads them.
+int trsm_unit_lower_gemm(Ctx& c, const double* L11, long long lda, int w, double* B, long long ldb, int ncols,
+                         const TrsmScratch& s, cudaStream_t st) {
+  if (w <= 0 || ncols <= 0) return LM_OK;
+  if (w <= 64 && ncols <= 128) {
+    Prof p(c, kPhaseTrsm, (double)w * w * ncols, 8.0 * ((double)w * w / 2 + 2.0 * w * ncols), st);
+    return trsm_lower_small<double>(L11, lda, w, true, B, ldb, ncols, st);
+  }
+  {
+    Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 8.0 * (double)w * w, st);
+    LM_TRY(tri_inv_lower<double>(L11, lda, w, true, s.Linv, kNB, nullptr, st));
+  }
+  GemmDesc d;
+  d.m = w; d.n = ncols; d.k = w;
+  d.alpha = 1.0; d.beta = 0.0;
+  d.A = s.Linv; d.lda = kNB;
+  d.B = B; d.ldb = ldb;
+  d.C = B; d.ldc = ldb;
+  return dgemm(c, d, st);
+}
+
 int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv,
-                    cudaStream_t st) {
+                    const TrsmScratch& s, cudaStream_t st) {
   const int R = n - c0;
   const int wmax = panel_leaf_max_width_for(c, R);
   if (wmax <= 0) return LM_ERR_UNSUPPORTED;
@@ -42,12 +79,9 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int 
   int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
   if (w1 >= w) w1 = w - 4;
   const int w2 = w - w1;
-  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, st));
+  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st));
   double* A11 = A + (long long)c0 * lda + c0;
-  {
-    Prof p(c, kPhaseTrsm, (double)w1 * w1 * w2, 8.0 * ((double)w1 * w1 / 2 + 2.0 * w1 * w2), st);
-    LM_TRY(trsm_left<double>(A11, lda, w1, true, true, false, A11 + w1, lda, w2, st));
-  }
+  LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w1, A11 + w1, lda, w2, s, st));
   GemmDesc d;
   d.m = R - w1; d.n = w2; d.k = w1;
   d.alpha = -1.0; d.beta = 1.0;
@@ -55,27 +89,30 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int 
   d.B = A11 + w1; d.ldb = lda;
   d.C = A11 + (long long)w1 * lda + w1; d.ldc = lda;
   LM_TRY(dgemm(c, d, st));
-  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, st);
+  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st);
 }
 
 }  // namespace
 
 int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) {
+  TrsmScratch s;
+  {
+    void* ws = nullptr;
+    LM_TRY(ctx_workspace(c, 1, sizeof(double) * (size_t)kNB * kNB + sizeof(int) * kSwapPlanInts, &ws));
+    s.Linv = static_cast<double*>(ws);
+    s.plan = reinterpret_cast<int*>(s.Linv + (size_t)kNB * kNB);
+  }
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
-    LM_TRY(getrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, st));
+    LM_TRY(getrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, s, st));
     // this panel's interchanges on the columns left and right of it
     {
       Prof p(c, kPhaseSwap, 0.0, 32.0 * w * (n - w), st);
-      LM_TRY(laswp<double>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st));
+      LM_TRY(laswp<double>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st, s.plan));
     }
     if (k0 + w < n) {
       double* A11 = A + (long long)k0 * lda + k0;
-      {
-        const double nc = n - k0 - w;
-        Prof p(c, kPhaseTrsm, (double)w * w * nc, 8.0 * ((double)w * w / 2 + 2.0 * w * nc), st);
-        LM_TRY(trsm_left<double>(A11, lda, w, true, true, false, A11 + w, lda, n - k0 - w, st));
-      }
+      LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w, A11 + w, lda, n - k0 - w, s, st));
       GemmDesc d;
       d.m = n - k0 - w; d.n = n - k0 - w; d.k = w;
       d.alpha = -1.0; d.beta = 1.0;
@@ -104,9 +141,8 @@ int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st) {
       double* W21 = Linv + (size_t)kNB * kNB;
       double* A21 = A11 + (long long)w * lda;
       {
-        Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 24.0 * w * w, st);
-        LM_TRY(set_identity<double>(Linv, kNB, w, w, st));
-        LM_TRY(trsm_left<double>(A11, lda, w, true, false, false, Linv, kNB, w, st));
+        Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 16.0 * w * w, st);
+        LM_TRY(tri_inv_lower<double>(A11, lda, w, false, Linv, kNB, nullptr, st));
       }
       {
         Prof p(c, kPhaseOther, 0.0, 16.0 * R * w, st);

@@ -80,9 +80,12 @@ int dgemm(Ctx& c, const GemmDesc& d, cudaStream_t st);
 // Apply row interchanges ipiv[k0..k1) in order (row s <-> row ipiv[s]) to the
 // columns [ca0, ca1) and [cb0, cb1) of A (nrows rows).  A pivot row outside
 // [0, nrows) is skipped and recorded as LM_DEVERR_BOUNDS in status[0].
+// `plan` (kSwapPlanInts ints of device scratch, or null) lets wide updates
+// compose the interchanges once instead of in every column block.
+constexpr int kSwapPlanInts = 1 + 2 * 256 + 15;
 template <typename T>
 int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int ca0, int ca1, int cb0, int cb1,
-          int* status, cudaStream_t st);
+          int* status, cudaStream_t st, int* plan = nullptr);
 
 // In-place triangular solve with a w x w block (w <= 128) of Tri (ldt) on the
 // w x ncols block B (ldb):  op(Tri) X = B.
@@ -90,6 +93,26 @@ int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int c
 template <typename T>
 int trsm_left(const T* Tri, long long ldt, int w, bool lower, bool unit, bool trans, T* B,
               long long ldb, int ncols, cudaStream_t st);
+
+// Inverse of a lower-triangular block of order w <= 128 (diag.cu): Xout
+// (w x w, ldx) <- inv(L) with zeros above the diagonal; `unit` ignores the
+// stored diagonal.  For float with `lo` given, Xout receives the TF32 high
+// part and lo the remainder (the 3xTF32 operand split).  One CTA.
+template <typename T>
+int tri_inv_lower(const T* L, long long ldl, int w, bool unit, T* Xout, long long ldx, T* lo, cudaStream_t st);
+
+// B (w x ncols, ldb) <- inv(lower triangle of L) B in one launch, for
+// w <= 64 and ncols <= 128 (the block solves inside a panel; diag.cu).
+template <typename T>
+int trsm_lower_small(const T* L, long long ldl, int w, bool unit, T* B, long long ldb, int ncols, cudaStream_t st);
+
+// LU without pivoting of the w x w (w <= 128) FP32 block A11 in place, with
+// split(inv(L11)) into Lhi/Llo and split(inv(U11)^T) into UThi/UTlo (w x w,
+// ld ldi), and inv(L11) / inv(U11) as 128 x 128 identity-padded blocks into
+// DinvL / DinvU; the first zero or NaN pivot is recorded as base + k + 1 in
+// status[1] (diag.cu).
+int nopiv_diag(float* A11, long long lda, int w, int base, float* Lhi, float* Llo, float* UThi, float* UTlo,
+               long long ldi, float* DinvL, float* DinvU, int* status, cudaStream_t st);
 
 // 2D copy (rows x cols) between strided buffers on the device.
 template <typename T>
@@ -134,6 +157,20 @@ int sgetrs(Ctx& c, int n, int nrhs, const float* LU, long long lda, const int* i
 int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
              const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner);
+
+// Randomised variant (ir.cu, rbt.cu): depth-2 random butterflies on both
+// sides, FP32 LU without pivoting on the tensor cores, FP64 refinement.
+// Returns LM_ERR_NOT_CONVERGED when refinement stalls (the caller falls back
+// to dgesv_ir).
+int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+                 long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
+                 const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner);
+int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, cudaStream_t st);
+// Depth-2 recursive butterflies (rbt.cu); np is a multiple of 4.
+int rbt_diagonals(double* du, double* dv, int np, cudaStream_t st);
+int rbt_transform(float* Ar, long long ldr, const double* A, long long lda, int n, int np, const double* du,
+                  const double* dv, cudaStream_t st);
+int rbt_rows(float* D, long long ldd, int np, int nrhs, const double* d, bool transposed, cudaStream_t st);
 
 // Run dpotrf with caller-provided device scratch (workspace slot 1) and
 // status words instead of a context's own allocations (api.cu).

@@ -142,14 +142,41 @@ __global__ void colmax_abs_kernel(const double* V, long long ldv, int rows, int 
   }
 }
 
+__global__ void iota_kernel(int* p, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
+}
+
 int grid_of(long long total) { return (int)std::max<long long>(1, std::min<long long>(cdivll(total, 256), 2048)); }
 
 // Scratch for the split operands of the 3xTF32 update: L21 -> Ahi/Alo
-// (m x k), U12^T -> Bhi/Blo (n x k); all with leading dimension 128 (k <= 128).
+// (m x k), U12^T -> Bhi/Blo (n x k); all with leading dimension 128 (k <= 128);
+// Lhi/Llo hold split(inv(L11)) for the block solves (128 x 128).
 struct SScratch {
-  float *Ahi, *Alo, *Bhi, *Blo;
+  float *Ahi, *Alo, *Bhi, *Blo, *Lhi, *Llo;
   long long ld;
+  int* plan;  // row-interchange plan (kSwapPlanInts)
 };
+
+// B (w x ncols, ldb) <- inv(unit lower L11) B: small blocks (inside a panel)
+// in one fused FP32 launch; otherwise the inverse of the diagonal block (one
+// CTA) times B on the tensor cores as 3xTF32.
+int s_trsm_unit_lower(Ctx& c, const float* L11, long long lda, int w, float* B, long long ldb, int ncols,
+                      SScratch& s, cudaStream_t st) {
+  if (w <= 0 || ncols <= 0) return LM_OK;
+  if (w <= 64 && ncols <= 128) {
+    Prof p(c, kPhaseTrsm, (double)w * w * ncols, 4.0 * ((double)w * w / 2 + 2.0 * w * ncols), st);
+    return trsm_lower_small<float>(L11, lda, w, true, B, ldb, ncols, st);
+  }
+  {
+    Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 12.0 * (double)w * w, st);
+    LM_TRY(tri_inv_lower<float>(L11, lda, w, true, s.Lhi, kNB, s.Llo, st));
+  }
+  dim3 tb(32, 8), tg(cdiv(ncols, 32), cdiv(w, 32));
+  transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, B, ldb, w, ncols);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return sgemm_tf32(c, w, ncols, w, 1.0f, s.Lhi, kNB, s.Bhi, s.ld, 0.0f, B, ldb, st, s.Llo, s.Blo);
+}
 
 int s_update(Ctx& c, int m, int n, int k, float* A21, long long lda, const float* U12, float* C, SScratch& s,
              cudaStream_t st) {
@@ -176,10 +203,7 @@ int sgetrf_panel_rec(Ctx& c, float* A, long long lda, int n, int c0, int w, int 
   const int w2 = w - w1;
   LM_TRY(sgetrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st));
   float* A11 = A + (long long)c0 * lda + c0;
-  {
-    Prof p(c, kPhaseTrsm, (double)w1 * w1 * w2, 4.0 * ((double)w1 * w1 / 2 + 2.0 * w1 * w2), st);
-    LM_TRY(trsm_left<float>(A11, lda, w1, true, true, false, A11 + w1, lda, w2, st));
-  }
+  LM_TRY(s_trsm_unit_lower(c, A11, lda, w1, A11 + w1, lda, w2, s, st));
   LM_TRY(s_update(c, R - w1, w2, w1, A11 + (long long)w1 * lda, lda, A11 + w1, A11 + (long long)w1 * lda + w1, s, st));
   return sgetrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st);
 }
@@ -190,25 +214,25 @@ int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
   void* ws = nullptr;
   SScratch s;
   s.ld = kNB;
-  LM_TRY(ctx_workspace(c, 1, 4 * sizeof(float) * (size_t)n * kNB, &ws));
+  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * kNB + 2 * (size_t)kNB * kNB) + sizeof(int) * kSwapPlanInts,
+                       &ws));
   s.Ahi = static_cast<float*>(ws);
   s.Alo = s.Ahi + (size_t)n * kNB;
   s.Bhi = s.Alo + (size_t)n * kNB;
   s.Blo = s.Bhi + (size_t)n * kNB;
+  s.Lhi = s.Blo + (size_t)n * kNB;
+  s.Llo = s.Lhi + (size_t)kNB * kNB;
+  s.plan = reinterpret_cast<int*>(s.Llo + (size_t)kNB * kNB);
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
     LM_TRY(sgetrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, s, st));
     {
       Prof p(c, kPhaseSwap, 0.0, 16.0 * w * (n - w), st);
-      LM_TRY(laswp<float>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st));
+      LM_TRY(laswp<float>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st, s.plan));
     }
     if (k0 + w < n) {
       float* A11 = A + (long long)k0 * lda + k0;
-      {
-        const double nc = n - k0 - w;
-        Prof p(c, kPhaseTrsm, (double)w * w * nc, 4.0 * ((double)w * w / 2 + 2.0 * w * nc), st);
-        LM_TRY(trsm_left<float>(A11, lda, w, true, true, false, A11 + w, lda, n - k0 - w, st));
-      }
+      LM_TRY(s_trsm_unit_lower(c, A11, lda, w, A11 + w, lda, n - k0 - w, s, st));
       LM_TRY(s_update(c, n - k0 - w, n - k0 - w, w, A11 + (long long)w * lda, lda, A11 + w,
                       A11 + (long long)w * lda + w, s, st));
     }
@@ -266,6 +290,79 @@ int convert_d2s(float* dst, long long ldd, const double* src, long long lds, int
   return LM_OK;
 }
 
+namespace {
+
+int identity_pivots(int* ipiv, int n, cudaStream_t st) {
+  iota_kernel<<<grid_of(n), 256, 0, st>>>(ipiv, n);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+// Refinement loop shared by both low-precision factorisations.  R (n x ldr
+// FP64), D (np x ldr FP32, np >= n) and nrm (2 + 3 * 64 words, nrm[0] and
+// nrm[1..] already hold ||A||_inf and ||B_c||_inf) are device scratch.
+// `correct(D, s)` turns D = fl32(r) (rows n..np-1 zero) into the correction.
+// With stall_exit the loop gives up as soon as the worst backward error fails
+// to halve, so that a poor factor hands over to the next method early.
+int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+           long long ldx, double tol, int max_iter, bool stall_exit, double* R, long long ldr, float* D,
+           unsigned long long* nrm, int* iters_out, double* berr_out, cudaStream_t st,
+           const std::function<int(float*, cudaStream_t)>& correct) {
+  // x = 0, r = b
+  LM_CUDA_TRY(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * nrhs, n, st));
+  LM_TRY(copy2d<double>(R, ldr, B, ldb, n, nrhs, st));
+  std::vector<unsigned long long> h(1 + 3 * 64);
+  int it = 0;
+  double worst = 0.0, prev = 1e300;
+  for (it = 1; it <= max_iter; ++it) {
+    LM_TRY(convert_d2s(D, ldr, R, ldr, n, nrhs, st));
+    if (np > n) LM_CUDA_TRY(cudaMemsetAsync(D + (size_t)n * ldr, 0, sizeof(float) * (size_t)(np - n) * ldr, st));
+    LM_TRY(correct(D, st));
+    add_s2d_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, D, ldr, n, nrhs);
+    count_launch(1);
+    LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, st));
+    LM_CUDA_TRY(cudaMemsetAsync(nrm + 1 + 64, 0, sizeof(unsigned long long) * 128, st));
+    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(R, ldr, n, nrhs, nrm + 1 + 64);
+    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, n, nrhs, nrm + 1 + 128);
+    count_launch(2);
+    LM_CUDA_TRY(cudaMemcpyAsync(h.data(), nrm, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
+    LM_CUDA_TRY(cudaStreamSynchronize(st));
+    auto dbl = [](unsigned long long u) {
+      double d;
+      std::memcpy(&d, &u, sizeof d);
+      return d;
+    };
+    const double anorm = dbl(h[0]);
+    worst = 0.0;
+    for (int col = 0; col < nrhs; ++col) {
+      const double rn = dbl(h[1 + 64 + col]), xn = dbl(h[1 + 128 + col]), bn = dbl(h[1 + col]);
+      const double den = anorm * xn + bn;
+      const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
+      worst = std::max(worst, (be != be) ? 1e300 : be);
+    }
+    if (worst <= tol) break;
+    if (stall_exit && it >= 2 && !(worst < 0.5 * prev)) break;
+    prev = worst;
+  }
+  if (iters_out) *iters_out = std::min(it, max_iter);
+  if (berr_out) *berr_out = worst;
+  return worst <= tol ? LM_OK : LM_ERR_NOT_CONVERGED;
+}
+
+// ||A||_inf and ||B_c||_inf (FP64, from the original data) into nrm.
+int input_norms(int n, int nrhs, const double* A, long long lda, const double* B, long long ldb,
+                unsigned long long* nrm, size_t nrm_bytes, cudaStream_t st) {
+  LM_CUDA_TRY(cudaMemsetAsync(nrm, 0, nrm_bytes, st));
+  norm_inf_rows_kernel<<<cdiv(n, 8), 256, 0, st>>>(A, lda, n, nrm);
+  colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(B, ldb, n, nrhs, nrm + 1);
+  count_launch(2);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+}  // namespace
+
 // Iterative refinement driver.  A, B, X are FP64 device buffers; X receives
 // the solution.  Returns info (> 0 if the FP32 factor hit a zero pivot),
 // LM_ERR_NOT_CONVERGED if some column misses tol after max_iter steps.
@@ -296,11 +393,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   const bool fast_trsv = nrhs <= 4;
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
 
-  // ||A||_inf and ||B_c||_inf (FP64, from the original data)
-  LM_CUDA_TRY(cudaMemsetAsync(nrm, 0, nrm_bytes, st));
-  norm_inf_rows_kernel<<<cdiv(n, 8), 256, 0, st>>>(A, lda, n, nrm);
-  colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(B, ldb, n, nrhs, nrm + 1);
-  count_launch(2);
+  LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
   // factor fl32(A)
   LM_TRY(factor_runner([&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
@@ -308,51 +401,140 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
     if (!fast_trsv) return LM_OK;
     return tri_inv_blocks<float>(A32, lda32, n, DinvL, DinvU, s);
   }));
-  // x = 0, r = b
-  LM_CUDA_TRY(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * nrhs, n, st));
-  LM_TRY(copy2d<double>(R, ldr, B, ldb, n, nrhs, st));
-  std::vector<unsigned long long> h(1 + 3 * 64);
-  int it = 0;
-  double worst = 0.0;
-  for (it = 1; it <= max_iter; ++it) {
-    LM_TRY(convert_d2s(D, ldr, R, ldr, n, nrhs, st));
-    if (fast_trsv) {
-      {
-        Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, st);
-        LM_TRY(laswp<float>(D, ldr, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
-      }
-      Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, st);
-      LM_TRY(trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, D, ldr, tsync, ctx_status(c), st));
-    } else {
-      LM_TRY(sgetrs(c, n, nrhs, A32, lda32, ipiv, D, ldr, st));
+  return refine(c, n, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, false, R, ldr, D, nrm, iters_out, berr_out, st,
+                [&](float* Dd, cudaStream_t s) {
+                  if (fast_trsv) {
+                    {
+                      Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
+                      LM_TRY(laswp<float>(Dd, ldr, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), s));
+                    }
+                    Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, s);
+                    return trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s);
+                  }
+                  return sgetrs(c, n, nrhs, A32, lda32, ipiv, Dd, ldr, s);
+                });
+}
+
+// LU without pivoting of the FP32 matrix A (n x n, lda), right-looking with
+// 128-wide steps in which everything but the 128 x 128 diagonal block runs
+// on the tensor cores (3xTF32):
+//   diagonal block: LU and both inverses in one CTA (nopiv_diag);
+//   L21 = A21 inv(U11);  U12 = inv(L11) A12;  A22 -= L21 U12.
+// DinvL / DinvU receive the diagonal-block inverses in the layout of the
+// persistent substitutions.  A zero pivot is recorded in status[1].
+int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, cudaStream_t st) {
+  void* ws = nullptr;
+  SScratch s;
+  s.ld = kNB;
+  const size_t blk = (size_t)kNB * kNB;
+  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * kNB + 4 * blk) + sizeof(int) * kSwapPlanInts, &ws));
+  s.Ahi = static_cast<float*>(ws);
+  s.Alo = s.Ahi + (size_t)n * kNB;
+  s.Bhi = s.Alo + (size_t)n * kNB;
+  s.Blo = s.Bhi + (size_t)n * kNB;
+  s.Lhi = s.Blo + (size_t)n * kNB;
+  s.Llo = s.Lhi + blk;
+  float* UThi = s.Llo + blk;
+  float* UTlo = UThi + blk;
+  s.plan = nullptr;
+  for (int k0 = 0; k0 < n; k0 += kNB) {
+    const int w = std::min(kNB, n - k0);
+    const int m = n - k0 - w;
+    float* A11 = A + (long long)k0 * lda + k0;
+    {
+      Prof p(c, kPhasePanel, 2.0 / 3.0 * w * w * w, 8.0 * w * w, st);
+      LM_TRY(nopiv_diag(A11, lda, w, k0, s.Lhi, s.Llo, UThi, UTlo, kNB, DinvL + (size_t)(k0 / kNB) * blk,
+                        DinvU + (size_t)(k0 / kNB) * blk, ctx_status(c), st));
     }
-    add_s2d_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, D, ldr, n, nrhs);
-    count_launch(1);
-    LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, st));
-    LM_CUDA_TRY(cudaMemsetAsync(nrm + 1 + 64, 0, sizeof(unsigned long long) * 128, st));
-    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(R, ldr, n, nrhs, nrm + 1 + 64);
-    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, n, nrhs, nrm + 1 + 128);
-    count_launch(2);
-    LM_CUDA_TRY(cudaMemcpyAsync(h.data(), nrm, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
-    LM_CUDA_TRY(cudaStreamSynchronize(st));
-    auto dbl = [](unsigned long long u) {
-      double d;
-      std::memcpy(&d, &u, sizeof d);
-      return d;
-    };
-    const double anorm = dbl(h[0]);
-    worst = 0.0;
-    for (int col = 0; col < nrhs; ++col) {
-      const double rn = dbl(h[1 + 64 + col]), xn = dbl(h[1 + 128 + col]), bn = dbl(h[1 + col]);
-      const double den = anorm * xn + bn;
-      const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
-      worst = std::max(worst, (be != be) ? 1e300 : be);
+    if (m <= 0) continue;
+    float* A21 = A11 + (long long)w * lda;
+    float* A12 = A11 + w;
+    {
+      // L21 = A21 inv(U11): A21 split into scratch, the product written back in place
+      Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 4.0 * 2.0 * m * w, st);
+      split_kernel<<<grid_of((long long)m * w), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, w);
+      count_launch(1);
+      LM_CUDA_TRY(cudaGetLastError());
     }
-    if (worst <= tol) break;
+    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, s.Ahi, s.ld, UThi, kNB, 0.0f, A21, lda, st, s.Alo, UTlo));
+    {
+      // U12 = inv(L11) A12 from the transposed split of A12
+      Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 4.0 * 2.0 * m * w, st);
+      dim3 tb(32, 8), tg(cdiv(m, 32), cdiv(w, 32));
+      transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, A12, lda, w, m);
+      count_launch(1);
+      LM_CUDA_TRY(cudaGetLastError());
+    }
+    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, s.Lhi, kNB, s.Bhi, s.ld, 0.0f, A12, lda, st, s.Llo, s.Blo));
+    LM_TRY(s_update(c, m, m, w, A21, lda, A12, A21 + w, s, st));
   }
-  if (iters_out) *iters_out = std::min(it, max_iter);
-  if (berr_out) *berr_out = worst;
-  return worst <= tol ? LM_OK : LM_ERR_NOT_CONVERGED;
+  return LM_OK;
+}
+
+// Randomised mixed-precision solve: Ar = fl32(U^T A V) with depth-2 random
+// butterflies U, V (rbt.cu), Ar = L U without pivoting (sgetrf_nopiv), then
+// FP64 refinement with the original A where each correction is
+// V U^-1 L^-1 U^T fl32(r).  Returns LM_ERR_NOT_CONVERGED when the refinement
+// stalls or runs out of steps; the caller then falls back to partial pivoting.
+int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+                 long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
+                 const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner) {
+  if (nrhs > 64) return LM_ERR_UNSUPPORTED;
+  const int np = (n + 3) / 4 * 4;
+  const long long lda32 = (np + 31) / 32 * 32;
+  const long long ldr = (nrhs + 7) / 8 * 8;
+  const size_t a32_bytes = sizeof(float) * (size_t)np * lda32;
+  const size_t piv_bytes = sizeof(int) * (size_t)((np + 63) / 64 * 64);
+  const size_t r_bytes = sizeof(double) * (size_t)n * ldr;
+  const size_t d_bytes = (sizeof(float) * (size_t)np * ldr + 15) / 16 * 16;
+  const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(2 + 3 * 64);
+  const size_t inv_elems = trsv_inv_elems<float>(np);
+  const size_t inv_bytes = 2 * sizeof(float) * inv_elems;
+  const size_t diag_bytes = 4 * sizeof(double) * (size_t)np;
+  const size_t sync_bytes = 64;
+  void* ws = nullptr;
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + diag_bytes + sync_bytes,
+                       &ws));
+  char* p = static_cast<char*>(ws);
+  float* A32 = reinterpret_cast<float*>(p);
+  p += a32_bytes;
+  int* ipiv = reinterpret_cast<int*>(p);
+  p += piv_bytes;
+  double* R = reinterpret_cast<double*>(p);
+  p += r_bytes;
+  float* D = reinterpret_cast<float*>(p);
+  p += d_bytes;
+  unsigned long long* nrm = reinterpret_cast<unsigned long long*>(p);
+  p += nrm_bytes;
+  float* DinvL = reinterpret_cast<float*>(p);
+  float* DinvU = DinvL + inv_elems;
+  p += inv_bytes;
+  double* du = reinterpret_cast<double*>(p);
+  double* dv = du + 2 * (size_t)np;
+  p += diag_bytes;
+  int* tsync = reinterpret_cast<int*>(p);
+  const bool fast_trsv = nrhs <= 4;
+
+  LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
+  LM_TRY(factor_runner([&](cudaStream_t s) {
+    LM_TRY(rbt_diagonals(du, dv, np, s));
+    LM_TRY(rbt_transform(A32, lda32, A, lda, n, np, du, dv, s));
+    LM_TRY(sgetrf_nopiv(c, np, A32, lda32, DinvL, DinvU, s));
+    if (fast_trsv) return LM_OK;
+    // identity swap list for the blocked substitutions
+    return identity_pivots(ipiv, np, s);
+  }));
+  return refine(c, n, np, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, true, R, ldr, D, nrm, iters_out, berr_out, st,
+                [&](float* Dd, cudaStream_t s) {
+                  LM_TRY(rbt_rows(Dd, ldr, np, nrhs, du, true, s));
+                  if (fast_trsv) {
+                    Prof pt(c, kPhaseTrsm, 2.0 * np * np * nrhs, 4.0 * np * np, s);
+                    LM_TRY(trsv_lu<float>(A32, lda32, np, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s));
+                  } else {
+                    LM_TRY(sgetrs(c, np, nrhs, A32, lda32, ipiv, Dd, ldr, s));
+                  }
+                  return rbt_rows(Dd, ldr, np, nrhs, dv, false, s);
+                });
 }
 
 }  // namespace lm

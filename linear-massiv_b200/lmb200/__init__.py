@@ -38,13 +38,15 @@ EXPORTS = [
     "lm_dgetrf", "lm_dgetrs", "lm_dgesv", "lm_dpotrf", "lm_dpotrs", "lm_dposv",
     "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
     "lm_lu_host", "lm_cholesky_host", "lm_det_host", "lm_ipiv_to_perm", "lm_dresidual",
-    "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_dpotrf_noalloc",
+    "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_ctx_set_ir_method", "lm_ctx_ir_last_method", "lm_dpotrf_noalloc",
     "lm_batch_create", "lm_batch_destroy", "lm_batch_offsets", "lm_batch_solve", "lm_batch_results",
     "lm_batch_factors", "lm_batch_solve_host", "lm_batch_tune", "lm_batch_tune_get", "lm_batch_tune_set",
     "lm_server_default_config", "lm_server_create", "lm_server_submit", "lm_server_test", "lm_server_wait",
     "lm_server_cancel", "lm_server_drain", "lm_server_stats", "lm_server_reset_stats", "lm_server_destroy",
 ]
 
+IR_RBT = 0
+IR_GEPP = 1
 BATCH_GENERAL = 0
 BATCH_SPD = 1
 PREC_FP64 = 0
@@ -88,6 +90,8 @@ def _lib():
                 "lm_ctx_synchronize": ([vp], i),
                 "lm_ctx_check": ([vp], i),
                 "lm_ctx_profile": ([vp, i], i),
+                "lm_ctx_set_ir_method": ([vp, i], i),
+                "lm_ctx_ir_last_method": ([vp, ip], i),
                 "lm_ctx_profile_read": ([vp, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp], i),
                 "lm_status_string": ([i], ctypes.c_char_p),
                 "lm_last_error": ([], ctypes.c_char_p),
@@ -194,6 +198,15 @@ class Context:
         _check(_lib().lm_ctx_check(self.h), "device status")
 
     PHASES = ("gemm", "panel", "swap", "trsm", "other")
+
+    def set_ir_method(self, method: int):
+        """IR_RBT (randomised, no pivoting; default) or IR_GEPP for the mixed-precision solves."""
+        _check(_lib().lm_ctx_set_ir_method(self.h, int(method)), "lm_ctx_set_ir_method")
+
+    def ir_last_method(self) -> int:
+        m = ctypes.c_int(-1)
+        _check(_lib().lm_ctx_ir_last_method(self.h, ctypes.byref(m)), "lm_ctx_ir_last_method")
+        return m.value
 
     def profile(self, enable: bool = True):
         _check(_lib().lm_ctx_profile(self.h, 1 if enable else 0), "lm_ctx_profile")
