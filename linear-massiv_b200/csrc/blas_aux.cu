@@ -208,6 +208,43 @@ __global__ void __launch_bounds__(kSwapThreads) swap_apply_kernel(T* A, long lon
     if (active) A[(long long)list_r[i] * lda + col] = stage[i * 32 + lane];
 }
 
+// All interchanges ipiv[0..n) on a narrow block B (n x nrhs) at once:
+// W(i, :) = B(sigma(i), :) with sigma(i) = tau_0(tau_1(... tau_{n-1}(i))),
+// tau_k the transposition (k, ipiv[k]).  Thread i walks the swap list
+// backwards (ipiv staged through shared memory, read as broadcasts), so the
+// n sequential swaps of applyPivotsForward (LU.hs:493-507) become one
+// parallel gather; an out-of-range pivot row records LM_DEVERR_BOUNDS.
+template <typename T>
+__global__ void __launch_bounds__(128) perm_gather_kernel(const T* __restrict__ B, long long ldb, int n, int nrhs,
+                                                          const int* __restrict__ ipiv, T* W, long long ldw,
+                                                          int* status) {
+  constexpr int CH = 4096;
+  __shared__ int sp[CH];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = i;
+  bool bad = false;
+  for (int c0 = ((n - 1) / CH) * CH; c0 >= 0; c0 -= CH) {
+    const int cnt = min(CH, n - c0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) sp[e] = __ldg(ipiv + c0 + e);
+    __syncthreads();
+#pragma unroll 8
+    for (int k = cnt - 1; k >= 0; --k) {
+      const int p = sp[k];
+      const int kk = c0 + k;
+      r = (r == kk) ? p : ((r == p) ? kk : r);
+    }
+  }
+  if (i < n) {
+    if (r < 0 || r >= n) bad = true;
+    if (bad) {
+      atomicCAS(status, 0, LM_DEVERR_BOUNDS);
+      r = i;
+    }
+    for (int c = 0; c < nrhs; ++c) W[(long long)i * ldw + c] = B[(long long)r * ldb + c];
+  }
+}
+
 // op(Tri) X = B for one w x 32 column block of B per CTA (w <= 128).  The
 // triangle of op(Tri) is staged packed in shared memory (w(w+1)/2 entries,
 // so two CTAs fit per SM in FP64) together with the block.  Rows are solved
@@ -328,6 +365,7 @@ __global__ void residual_kernel(int n, int nrhs, const double* __restrict__ A, l
 #pragma unroll
   for (int r = 0; r < NR; ++r) acc[r] = 0.0;
   const double* arow = A + (long long)row * lda;
+#pragma unroll 8
   for (int j = lane; j < n; j += 32) {
     const double a = arow[j];
 #pragma unroll
@@ -384,6 +422,15 @@ int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int c
     LM_CUDA_TRY(cudaGetLastError());
   }
   return LM_OK;
+}
+
+template <typename T>
+int laswp_narrow(T* B, long long ldb, int n, int nrhs, const int* ipiv, T* W, int* status, cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0) return LM_OK;
+  perm_gather_kernel<T><<<cdiv(n, 128), 128, 0, st>>>(B, ldb, n, nrhs, ipiv, W, nrhs, status);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return copy2d<T>(B, ldb, W, nrhs, n, nrhs, st);
 }
 
 template <typename T>
@@ -471,6 +518,8 @@ int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const dou
 template int laswp<double>(double*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t,
                            int*);
 template int laswp<float>(float*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t, int*);
+template int laswp_narrow<double>(double*, long long, int, int, const int*, double*, int*, cudaStream_t);
+template int laswp_narrow<float>(float*, long long, int, int, const int*, float*, int*, cudaStream_t);
 template int trsm_left<double>(const double*, long long, int, bool, bool, bool, double*, long long, int,
                                cudaStream_t);
 template int trsm_left<float>(const float*, long long, int, bool, bool, bool, float*, long long, int,

@@ -25,8 +25,8 @@ void count_launch(int n);
 namespace {
 
 constexpr int DB = 128;       // block order handled by one CTA
-constexpr int DLD = DB + 1;   // shared-memory leading dimension
-constexpr int TLD = 64 + 1;   // scratch leading dimension
+constexpr int DLD = DB + 4;   // shared-memory leading dimension (rows 16-byte aligned)
+constexpr int TLD = 64 + 4;   // scratch leading dimension
 
 __device__ __forceinline__ void group_bar(int id, int nthreads) {
   if (id == 0)
@@ -35,41 +35,93 @@ __device__ __forceinline__ void group_bar(int id, int nthreads) {
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// Four consecutive elements of a shared-memory row (16-byte aligned for
+// FP32, 32 bytes as two 16-byte loads for FP64).
+template <typename T>
+__device__ __forceinline__ void lds4(T (&v)[4], const T* p) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  } else {
+    const double2 q0 = *reinterpret_cast<const double2*>(p);
+    const double2 q1 = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = q0.x; v[1] = q0.y; v[2] = q1.x; v[3] = q1.y;
+  }
+}
+
+// C (m x n) = C0 + sign * A (m x kdim) B (kdim x n), all row-major in shared
+// memory, m and n multiples of 4 and every row start 16-byte aligned.
+// 4 x 4 register tiles, nthreads threads from t = 0; consecutive threads take
+// consecutive column tiles, so a warp reads A as broadcasts and B as
+// contiguous 16-byte vectors (about half a shared-memory wavefront per FMA
+// instruction instead of two).  With `acc_c` C0 = C, else C0 = 0.
+template <typename T>
+__device__ __forceinline__ void smem_mm4(T* C, int ldc, const T* A, int lda, const T* B, int ldb, int m, int n,
+                                         int kdim, T sign, bool acc_c, int t, int nthreads) {
+  const int tn = n / 4, tiles = (m / 4) * tn;
+  for (int tt = t; tt < tiles; tt += nthreads) {
+    const int r0 = (tt / tn) * 4, c0 = (tt % tn) * 4;
+    T acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[p][q] = T(0);
+#pragma unroll 4
+    for (int k = 0; k < kdim; ++k) {
+      T b[4];
+      lds4<T>(b, B + k * ldb + c0);
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const T a = A[(r0 + p) * lda + k];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = fma(a, b[q], acc[p][q]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+      T* cr = C + (r0 + p) * ldc + c0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) cr[q] = acc_c ? fma(sign, acc[p][q], cr[q]) : sign * acc[p][q];
+    }
+  }
+}
+
 // One doubling level of the blocked inversion: for each 2H x 2H diagonal
-// block p, X21 = -X22 (L21 X11), with tmp receiving L21 X11.  Thread t owns
-// column j = t % H and the rows ig + 8 r (r < H / 8) of its block, so every
-// k step loads one value of the right operand and H / 8 broadcast values of
-// the left one for H / 8 independent accumulations.  Upper triangles of the
-// diagonal blocks must hold zeros.
+// block p, X21 = -X22 (L21 X11), with tmp receiving L21 X11 (register-tiled
+// products).  Upper triangles of the diagonal blocks must hold zeros.
 template <typename T, int H>
 __device__ __forceinline__ void inv_combine(T* S, T* tmp, int t, int bar) {
-  constexpr int R = H / 8;
-  const int j = t % H, rest = t / H;
-  const int p = rest / 8, ig = rest % 8;
+  constexpr int NB = DB / (2 * H);
+  constexpr int PER = 512 / NB;  // the blocks split the threads evenly
+  const int p = t / PER, tl = t % PER;
   const int q0 = p * 2 * H;
-  T acc[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) acc[r] = T(0);
-#pragma unroll 8
-  for (int k = 0; k < H; ++k) {
-    const T b = S[(q0 + k) * DLD + q0 + j];  // X11(k, j)
-#pragma unroll
-    for (int r = 0; r < R; ++r) acc[r] = fma(S[(q0 + H + ig + 8 * r) * DLD + q0 + k], b, acc[r]);
-  }
-#pragma unroll
-  for (int r = 0; r < R; ++r) tmp[(p * H + ig + 8 * r) * TLD + j] = acc[r];
+  smem_mm4<T>(tmp + p * H * TLD, TLD, S + (q0 + H) * DLD + q0, DLD, S + q0 * DLD + q0, DLD, H, H, H, T(1), false, tl,
+              PER);
   group_bar(bar, 512);
-#pragma unroll
-  for (int r = 0; r < R; ++r) acc[r] = T(0);
-#pragma unroll 8
-  for (int k = 0; k < H; ++k) {
-    const T b = tmp[(p * H + k) * TLD + j];  // (L21 X11)(k, j)
-#pragma unroll
-    for (int r = 0; r < R; ++r) acc[r] = fma(S[(q0 + H + ig + 8 * r) * DLD + q0 + H + k], b, acc[r]);
-  }
-#pragma unroll
-  for (int r = 0; r < R; ++r) S[(q0 + H + ig + 8 * r) * DLD + q0 + j] = -acc[r];
+  smem_mm4<T>(S + (q0 + H) * DLD + q0, DLD, S + (q0 + H) * DLD + q0 + H, DLD, tmp + p * H * TLD, TLD, H, H, H, T(-1),
+              false, tl, PER);
   group_bar(bar, 512);
+}
+
+// Inverse of the lower-triangular 32 x 32 block at blk (leading dimension
+// DLD) in place, by one warp: lane j computes column j column-oriented (once
+// x[k] is final it is applied to every later row at once).  Out of line so
+// that x[] is register-allocated apart from the caller.
+template <typename T>
+__device__ __noinline__ void inv32_warp(T* blk, bool unit, int j) {
+  T x[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) x[i] = (i == j) ? T(1) : T(0);
+#pragma unroll 32
+  for (int k = 0; k < 32; ++k) {
+    if (!unit) x[k] = x[k] / blk[k * DLD + k];
+#pragma unroll 32
+    for (int i = k + 1; i < 32; ++i) x[i] = fma(-blk[i * DLD + k], x[k], x[i]);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int i = 0; i < 32; ++i)
+    if (i >= j) blk[i * DLD + j] = x[i];
 }
 
 // In-place inverse of the lower triangle of S (DB x DB, leading dimension
@@ -82,22 +134,7 @@ __device__ __forceinline__ void inv_combine(T* S, T* tmp, int t, int bar) {
 template <typename T>
 __device__ void inv_lower_smem(T* S, T* tmp, bool unit, bool half, int t, int bar) {
   const int lane = t & 31, warp = t >> 5;
-  if (warp < (half ? 2 : 4)) {
-    const int b0 = warp * 32, j = lane;
-    T x[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-      T acc = (i == j) ? T(1) : T(0);
-#pragma unroll
-      for (int k = 0; k < i; ++k) acc = fma(-S[(b0 + i) * DLD + b0 + k], x[k], acc);
-      if (!unit) acc = acc / S[(b0 + i) * DLD + b0 + i];
-      x[i] = (i < j) ? T(0) : acc;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < 32; ++i)
-      if (i >= j) S[(b0 + i) * DLD + b0 + j] = x[i];
-  }
+  if (warp < (half ? 2 : 4)) inv32_warp<T>(S + warp * 32 * DLD + warp * 32, unit, lane);
   group_bar(bar, 512);
   inv_combine<T, 32>(S, tmp, t, bar);
   if (!half) inv_combine<T, 64>(S, tmp, t, bar);
@@ -131,7 +168,6 @@ __global__ void __launch_bounds__(512, 1)
   inv_lower_smem<T>(S, tmp, unit != 0, w <= 64, t, 0);
   if (B) {
     // X = inv(L) B, 64 columns at a time through tmp
-    const int j = t % 64, ig = t / 64;
     for (int c0 = 0; c0 < ncols; c0 += 64) {
 #pragma unroll 8
       for (int e = t; e < 64 * 64; e += 512) {
@@ -139,19 +175,30 @@ __global__ void __launch_bounds__(512, 1)
         tmp[r * TLD + c] = (r < w && c0 + c < ncols) ? B[(long long)r * ldb + c0 + c] : T(0);
       }
       __syncthreads();
-      T acc[8];
+      // X = inv(L)[0:64, 0:64] tmp: 4 x 4 register tiles, written to B directly
+      if (t < 256) {
+        const int r0 = (t / 16) * 4, cq = (t % 16) * 4;
+        T acc[4][4];
 #pragma unroll
-      for (int r = 0; r < 8; ++r) acc[r] = T(0);
-#pragma unroll 8
-      for (int k = 0; k < 64; ++k) {
-        const T b = tmp[k * TLD + j];
+        for (int p = 0; p < 4; ++p)
 #pragma unroll
-        for (int r = 0; r < 8; ++r) acc[r] = fma(S[(ig + 8 * r) * DLD + k], b, acc[r]);
-      }
+          for (int q = 0; q < 4; ++q) acc[p][q] = T(0);
+#pragma unroll 4
+        for (int k = 0; k < 64; ++k) {
+          T b[4];
+          lds4<T>(b, tmp + k * TLD + cq);
 #pragma unroll
-      for (int r = 0; r < 8; ++r) {
-        const int i = ig + 8 * r;
-        if (i < w && c0 + j < ncols) B[(long long)i * ldb + c0 + j] = acc[r];
+          for (int p = 0; p < 4; ++p) {
+            const T a = S[(r0 + p) * DLD + k];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[p][q] = fma(a, b[q], acc[p][q]);
+          }
+        }
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (r0 + p < w && c0 + cq + q < ncols) B[(long long)(r0 + p) * ldb + c0 + cq + q] = acc[p][q];
       }
       __syncthreads();
     }
@@ -173,23 +220,87 @@ __global__ void __launch_bounds__(512, 1)
   }
 }
 
+// x U = row (U the upper triangle of the 32 x 32 block d, leading dimension
+// DLD), in place on the row: column-oriented in registers.
+__device__ __noinline__ void row_solve32(float* row, const float* d) {
+  float x[32];
+#pragma unroll
+  for (int j = 0; j < 32; j += 4) {
+    const float4 q = *reinterpret_cast<const float4*>(row + j);
+    x[j] = q.x; x[j + 1] = q.y; x[j + 2] = q.z; x[j + 3] = q.w;
+  }
+#pragma unroll 32
+  for (int j = 0; j < 32; ++j) {
+    x[j] = x[j] / d[j * DLD + j];
+#pragma unroll 32
+    for (int jj = j + 1; jj < 32; ++jj) x[jj] = fmaf(-x[j], d[j * DLD + jj], x[jj]);
+  }
+#pragma unroll
+  for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(row + j) = make_float4(x[j], x[j + 1], x[j + 2], x[j + 3]);
+}
+
+// L y = col (L the unit lower triangle of d), in place on a column of
+// stride DLD: column-oriented in registers.
+__device__ __noinline__ void col_solve32(float* col, const float* d) {
+  float y[32];
+#pragma unroll
+  for (int i = 0; i < 32; ++i) y[i] = col[i * DLD];
+#pragma unroll 32
+  for (int i = 0; i < 32; ++i) {
+#pragma unroll 32
+    for (int ii = i + 1; ii < 32; ++ii) y[ii] = fmaf(-d[ii * DLD + i], y[i], y[ii]);
+  }
+#pragma unroll
+  for (int i = 1; i < 32; ++i) col[i * DLD] = y[i];
+}
+
+// LU without pivoting of a 32 x 32 block (leading dimension DLD) by one
+// warp: lane i holds row i in registers, row k reaches the other lanes by
+// shuffles.  Kept out of line so that its registers are allocated apart from
+// the rest of the kernel.  The first zero or NaN pivot (global column
+// base + o + k < base + w) is recorded in status[1].
+__device__ __noinline__ void lu32_warp(float* blk, int o, int w, int base, int* status) {
+  const int i = threadIdx.x & 31;
+  float* ri = blk + i * DLD;
+  float r[32];
+#pragma unroll
+  for (int j = 0; j < 32; j += 4) {
+    const float4 q = *reinterpret_cast<const float4*>(ri + j);
+    r[j] = q.x; r[j + 1] = q.y; r[j + 2] = q.z; r[j + 3] = q.w;
+  }
+#pragma unroll 32
+  for (int k = 0; k < 32; ++k) {
+    const float piv = __shfl_sync(0xffffffffu, r[k], k);
+    if (i == 0 && o + k < w && (piv == 0.f || piv != piv)) atomicCAS(status + 1, 0, base + o + k + 1);
+    const float l = r[k] / piv;
+    if (i > k) r[k] = l;
+#pragma unroll 32
+    for (int j = k + 1; j < 32; ++j) {
+      const float u = __shfl_sync(0xffffffffu, r[j], k);
+      if (i > k) r[j] = fmaf(-l, u, r[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 32; j += 4) *reinterpret_cast<float4*>(ri + j) = make_float4(r[j], r[j + 1], r[j + 2], r[j + 3]);
+}
+
 // LU without pivoting of the w x w block A11 (w <= 128) in place, then
 //   Lhi/Llo   = split(inv(L11))        (w x w, ld ldi, zeros above the diagonal)
 //   UThi/UTlo = split(inv(U11)^T)      (w x w, ld ldi, zeros above the diagonal)
 //   DinvL / DinvU = inv(L11) / inv(U11) as DB x DB blocks padded with the
 //                   identity (the layout of the persistent substitutions).
 // The first zero or NaN pivot is recorded as base + k + 1 in status[1].
-// 1024 threads: the factorisation uses all of them; then threads 0..511
-// invert L and 512..1023 invert U^T concurrently (named barriers 1 and 2).
-__global__ void __launch_bounds__(1024, 1)
+// 512 threads; L and U^T are inverted one after the other.
+__global__ void __launch_bounds__(512, 1)
     nopiv_diag_kernel(float* A11, long long lda, int w, int base, float* Lhi, float* Llo, float* UThi, float* UTlo,
                       long long ldi, float* DinvL, float* DinvU, int* status) {
   extern __shared__ __align__(16) unsigned char dsm[];
   float* S = reinterpret_cast<float*>(dsm);   // L \ U, then inv(L)
   float* S2 = S + DB * DLD;                    // U^T, then inv(U^T)
-  float* tmp = S2 + DB * DLD;                  // 2 x 64 x TLD
+  float* tmp = S2 + DB * DLD;                  // 64 x TLD
   const int t = threadIdx.x;
-  for (int e = t; e < DB * DB; e += 1024) {
+#pragma unroll 8
+  for (int e = t; e < DB * DB; e += 512) {
     const int i = e / DB, j = e % DB;
     float v = 0.f;
     if (i < w && j < w)
@@ -199,39 +310,47 @@ __global__ void __launch_bounds__(1024, 1)
     S[i * DLD + j] = v;
   }
   __syncthreads();
-  for (int k = 0; k < w; ++k) {
-    const float piv = S[k * DLD + k];
-    if (t == 0 && (piv == 0.f || piv != piv)) atomicCAS(status + 1, 0, base + k + 1);
-    const int m = DB - k - 1;
-    for (int i = t; i < m; i += 1024) S[(k + 1 + i) * DLD + k] = S[(k + 1 + i) * DLD + k] / piv;
+  // Blocked right-looking LU in 32-column steps:
+  //   (a) one warp factors the 32 x 32 diagonal block (lane i owns row i);
+  //   (b) L10 = A10 U00^-1 row by row and U01 = L00^-1 A01 column by column,
+  //       one thread per row / column;
+  //   (c) A11 -= L10 U01 over the whole CTA.
+  for (int kb = 0; kb < DB / 32; ++kb) {
+    const int o = kb * 32;
+    const int rem = DB - o - 32;
+    if (t < 32) lu32_warp(S + o * DLD + o, o, w, base, status);
     __syncthreads();
-    for (int e = t; e < m * m; e += 1024) {
-      const int i = k + 1 + e / m, j = k + 1 + e % m;
-      S[i * DLD + j] = fmaf(-S[i * DLD + k], S[k * DLD + j], S[i * DLD + j]);
-    }
+    if (rem <= 0) break;
+    // both solves column-oriented in registers: each finished unknown is
+    // applied to all later ones at once (independent FMAs per step)
+    if (t < rem)
+      row_solve32(S + (o + 32 + t) * DLD + o, S + o * DLD + o);
+    else if (t >= 256 && t < 256 + rem)
+      col_solve32(S + o * DLD + o + 32 + (t - 256), S + o * DLD + o);
+    __syncthreads();
+    smem_mm4<float>(S + (o + 32) * DLD + o + 32, DLD, S + (o + 32) * DLD + o, DLD, S + o * DLD + o + 32, DLD, rem,
+                    rem, 32, -1.f, true, t, 512);
     __syncthreads();
   }
-  for (int e = t; e < w * w; e += 1024) {
+  for (int e = t; e < w * w; e += 512) {
     const int i = e / w, j = e % w;
     A11[(long long)i * lda + j] = S[i * DLD + j];
   }
   // S2 = U^T (lower, with U's diagonal); then S keeps only L (zero upper)
-  for (int e = t; e < DB * DB; e += 1024) {
+  for (int e = t; e < DB * DB; e += 512) {
     const int i = e / DB, j = e % DB;
     S2[i * DLD + j] = (j <= i) ? S[j * DLD + i] : 0.f;
   }
   __syncthreads();
-  for (int e = t; e < DB * DB; e += 1024) {
+  for (int e = t; e < DB * DB; e += 512) {
     const int i = e / DB, j = e % DB;
     if (j > i) S[i * DLD + j] = 0.f;
   }
   __syncthreads();
-  if (t < 512)
-    inv_lower_smem<float>(S, tmp, true, false, t, 1);
-  else
-    inv_lower_smem<float>(S2, tmp + 64 * TLD, false, false, t - 512, 2);
+  inv_lower_smem<float>(S, tmp, true, false, t, 0);
+  inv_lower_smem<float>(S2, tmp, false, false, t, 0);
   __syncthreads();
-  for (int e = t; e < DB * DB; e += 1024) {
+  for (int e = t; e < DB * DB; e += 512) {
     const int i = e / DB, j = e % DB;
     const float li = (j <= i) ? S[i * DLD + j] : 0.f;    // inv(L)(i, j)
     const float ut = (j <= i) ? S2[i * DLD + j] : 0.f;   // inv(U)^T(i, j) = inv(U)(j, i)
@@ -252,7 +371,7 @@ template <typename T>
 constexpr size_t inv_smem_bytes() {
   return sizeof(T) * ((size_t)DB * DLD + (size_t)64 * TLD);
 }
-constexpr size_t nopiv_smem_bytes() { return sizeof(float) * (2 * (size_t)DB * DLD + 2 * (size_t)64 * TLD); }
+constexpr size_t nopiv_smem_bytes() { return sizeof(float) * (2 * (size_t)DB * DLD + (size_t)64 * TLD); }
 
 }  // namespace
 
@@ -306,7 +425,7 @@ int nopiv_diag(float* A11, long long lda, int w, int base, float* Lhi, float* Ll
                                      (int)nopiv_smem_bytes()));
     attr_set[dev] = true;
   }
-  nopiv_diag_kernel<<<1, 1024, nopiv_smem_bytes(), st>>>(A11, lda, w, base, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
+  nopiv_diag_kernel<<<1, 512, nopiv_smem_bytes(), st>>>(A11, lda, w, base, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
                                                          status);
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());

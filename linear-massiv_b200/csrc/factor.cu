@@ -228,10 +228,11 @@ int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* 
   if (nrhs <= 4) {
     // few right-hand sides: P b, then one persistent launch per direction
     void* ws = nullptr;
-    LM_TRY(ctx_workspace(c, 2, 64, &ws));
+    LM_TRY(ctx_workspace(c, 2, 64 + sizeof(double) * (size_t)n * nrhs, &ws));
     {
       Prof p(c, kPhaseSwap, 0.0, 32.0 * n * nrhs, st);
-      LM_TRY(laswp<double>(B, ldb, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), st));
+      LM_TRY(laswp_narrow<double>(B, ldb, n, nrhs, ipiv, reinterpret_cast<double*>(static_cast<char*>(ws) + 64),
+                                  ctx_status(c), st));
     }
     Prof p(c, kPhaseTrsm, 2.0 * n * n * nrhs, 8.0 * n * n, st);
     return trsv_lu<double>(LU, lda, n, nrhs, nullptr, nullptr, B, ldb, static_cast<int*>(ws), ctx_status(c), st);

@@ -87,6 +87,11 @@ template <typename T>
 int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int ca0, int ca1, int cb0, int cb1,
           int* status, cudaStream_t st, int* plan = nullptr);
 
+// All interchanges ipiv[0..n) on a narrow n x nrhs block B at once (one
+// parallel gather into W, n x nrhs scratch, then copied back).
+template <typename T>
+int laswp_narrow(T* B, long long ldb, int n, int nrhs, const int* ipiv, T* W, int* status, cudaStream_t st);
+
 // In-place triangular solve with a w x w block (w <= 128) of Tri (ldt) on the
 // w x ncols block B (ldb):  op(Tri) X = B.
 //   lower/unit describe Tri as stored; trans solves with Tri^T.

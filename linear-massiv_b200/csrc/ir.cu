@@ -13,6 +13,7 @@
 // The stopping metric is the reference test suite's scaledResidualLinear
 // without the n*eps guard (test/Test/Residuals.hs:69-78).
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <functional>
 #include <vector>
@@ -303,8 +304,10 @@ int identity_pivots(int* ipiv, int n, cudaStream_t st) {
 // FP64), D (np x ldr FP32, np >= n) and nrm (2 + 3 * 64 words, nrm[0] and
 // nrm[1..] already hold ||A||_inf and ||B_c||_inf) are device scratch.
 // `correct(D, s)` turns D = fl32(r) (rows n..np-1 zero) into the correction.
-// With stall_exit the loop gives up as soon as the worst backward error fails
-// to halve, so that a poor factor hands over to the next method early.
+// With stall_exit the loop gives up as soon as an iteration fails to reduce
+// the worst backward error, or the observed contraction rate could not reach
+// tol within max_iter, so that a poor factor hands over to the next method
+// early.
 int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
            long long ldx, double tol, int max_iter, bool stall_exit, double* R, long long ldr, float* D,
            unsigned long long* nrm, int* iters_out, double* berr_out, cudaStream_t st,
@@ -342,7 +345,13 @@ int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, cons
       worst = std::max(worst, (be != be) ? 1e300 : be);
     }
     if (worst <= tol) break;
-    if (stall_exit && it >= 2 && !(worst < 0.5 * prev)) break;
+    if (stall_exit && it >= 2) {
+      // give up when an iteration makes no progress, or when the observed
+      // contraction cannot reach tol within max_iter
+      const double rate = worst / prev;
+      if (!(rate < 1.0)) break;
+      if (rate > 0.5 && it + std::log(tol / worst) / std::log(rate) > max_iter) break;
+    }
     prev = worst;
   }
   if (iters_out) *iters_out = std::min(it, max_iter);
@@ -379,8 +388,10 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   const size_t inv_elems = trsv_inv_elems<float>(n);
   const size_t inv_bytes = 2 * sizeof(float) * inv_elems;  // diagonal-block inverses of L and U
   const size_t sync_bytes = 64;
+  const size_t w_bytes = sizeof(float) * (size_t)n * ldr;  // gather scratch of the interchanges
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + sync_bytes, &ws));
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + sync_bytes + w_bytes,
+                       &ws));
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   int* ipiv = reinterpret_cast<int*>(p + a32_bytes);
@@ -390,6 +401,8 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   float* DinvL = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes);
   float* DinvU = DinvL + inv_elems;
   int* tsync = reinterpret_cast<int*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes);
+  float* Wg = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes +
+                                       sync_bytes);
   const bool fast_trsv = nrhs <= 4;
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
 
@@ -406,7 +419,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
                   if (fast_trsv) {
                     {
                       Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
-                      LM_TRY(laswp<float>(Dd, ldr, n, ipiv, 0, n, 0, nrhs, 0, 0, ctx_status(c), s));
+                      LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
                     }
                     Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, s);
                     return trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s);
