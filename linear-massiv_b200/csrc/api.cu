@@ -33,6 +33,8 @@ struct Ctx {
   std::vector<GraphEntry> gcache;
   long long ws_generation = 0;
   cudaStream_t side = nullptr;  // capture stream when the caller's stream is the legacy default
+  cudaStream_t aux = nullptr;   // look-ahead stream of the factorisations (ctx_aux)
+  cudaEvent_t ev_la[2] = {};    // its fork / join events
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   bool prof = false;
   std::vector<ProfRec> recs;
@@ -107,6 +109,20 @@ Prof::~Prof() {
 
 int* ctx_status(Ctx& c) { return c.d_status; }
 int ctx_num_sms(Ctx& c) { return c.num_sms; }
+
+int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join) {
+  if (!c.aux) {
+    int lo = 0, hi = 0;
+    LM_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    LM_CUDA_TRY(cudaStreamCreateWithPriority(&c.aux, cudaStreamNonBlocking, hi));
+    LM_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_la[0], cudaEventDisableTiming));
+    LM_CUDA_TRY(cudaEventCreateWithFlags(&c.ev_la[1], cudaEventDisableTiming));
+  }
+  *aux = c.aux;
+  *fork = c.ev_la[0];
+  *join = c.ev_la[1];
+  return LM_OK;
+}
 int ctx_device(Ctx& c) { return c.device; }
 
 int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr) {
@@ -350,6 +366,9 @@ int lm_ctx_destroy(lm_ctx* ctx) {
     for (auto& g : ctx->c.gcache)
       if (g.exec) cudaGraphExecDestroy(g.exec);
     if (ctx->c.side) cudaStreamDestroy(ctx->c.side);
+    if (ctx->c.aux) cudaStreamDestroy(ctx->c.aux);
+    for (auto e : ctx->c.ev_la)
+      if (e) cudaEventDestroy(e);
     if (ctx->c.ev_in) cudaEventDestroy(ctx->c.ev_in);
     if (ctx->c.ev_out) cudaEventDestroy(ctx->c.ev_out);
     if (ctx->c.d_status) cudaFree(ctx->c.d_status);

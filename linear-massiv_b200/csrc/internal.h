@@ -22,6 +22,9 @@ int ctx_device(Ctx& c);
 // Grow-only device workspace owned by the context (slot 0..kWsSlots-1).
 constexpr int kWsSlots = 4;
 int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr);
+// The context's look-ahead stream (highest priority, created on first use,
+// which must not be inside a stream capture) and its fork / join events.
+int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join);
 
 // Per-phase CUDA-event tracing (enabled by lm_ctx_profile).  A Prof scope
 // brackets the kernels launched inside it with events on stream `st`.

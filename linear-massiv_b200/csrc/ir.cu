@@ -24,9 +24,11 @@
 namespace lm {
 
 void count_launch(int n);
+// C = alpha A Bt^T + beta C on tcgen05 (sgemm_tc.cu); max_ctas caps the
+// persistent grid (0 = one CTA per SM).
 int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
                long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
-               const float* Btlo);
+               const float* Btlo, int max_ctas = 0);
 
 
 namespace {
@@ -440,46 +442,79 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
   SScratch s;
   s.ld = kNB;
   const size_t blk = (size_t)kNB * kNB;
-  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * kNB + 4 * blk) + sizeof(int) * kSwapPlanInts, &ws));
+  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * kNB + 8 * blk) + sizeof(int) * kSwapPlanInts, &ws));
   s.Ahi = static_cast<float*>(ws);
   s.Alo = s.Ahi + (size_t)n * kNB;
   s.Bhi = s.Alo + (size_t)n * kNB;
   s.Blo = s.Bhi + (size_t)n * kNB;
-  s.Lhi = s.Blo + (size_t)n * kNB;
-  s.Llo = s.Lhi + blk;
-  float* UThi = s.Llo + blk;
-  float* UTlo = UThi + blk;
+  // two sets of diagonal-block operands: the look-ahead factors block k + 1
+  // while block k's are still being read
+  float* inv[2][4];
+  for (int b = 0; b < 2; ++b)
+    for (int q = 0; q < 4; ++q) inv[b][q] = s.Blo + (size_t)n * kNB + (size_t)(4 * b + q) * blk;
   s.plan = nullptr;
+  cudaStream_t aux;
+  cudaEvent_t ev_fork, ev_join;
+  LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
+  const int nsm = ctx_num_sms(c);
+  auto diag = [&](int k0, cudaStream_t ds) {
+    const int w = std::min(kNB, n - k0);
+    float** d = inv[(k0 / kNB) & 1];
+    Prof p(c, kPhasePanel, 2.0 / 3.0 * w * w * w, 8.0 * w * w, ds);
+    return nopiv_diag(A + (long long)k0 * lda + k0, lda, w, k0, d[0], d[1], d[2], d[3], kNB,
+                      DinvL + (size_t)(k0 / kNB) * blk, DinvU + (size_t)(k0 / kNB) * blk, ctx_status(c), ds);
+  };
+  LM_TRY(diag(0, st));
+  // Step k: with the diagonal block factored, L21 = A21 inv(U11) and
+  // U12 = inv(L11) A12 (3xTF32), then A22 -= L21 U12 in three pieces: the next
+  // diagonal block first, whose factorisation then runs on the look-ahead
+  // stream (one CTA on the SM the other pieces leave free) while the rest of
+  // A22 is updated.
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
     const int m = n - k0 - w;
+    if (m <= 0) break;
+    float** d = inv[(k0 / kNB) & 1];
     float* A11 = A + (long long)k0 * lda + k0;
-    {
-      Prof p(c, kPhasePanel, 2.0 / 3.0 * w * w * w, 8.0 * w * w, st);
-      LM_TRY(nopiv_diag(A11, lda, w, k0, s.Lhi, s.Llo, UThi, UTlo, kNB, DinvL + (size_t)(k0 / kNB) * blk,
-                        DinvU + (size_t)(k0 / kNB) * blk, ctx_status(c), st));
-    }
-    if (m <= 0) continue;
     float* A21 = A11 + (long long)w * lda;
     float* A12 = A11 + w;
+    float* A22 = A21 + w;
     {
-      // L21 = A21 inv(U11): A21 split into scratch, the product written back in place
       Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 4.0 * 2.0 * m * w, st);
       split_kernel<<<grid_of((long long)m * w), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, w);
       count_launch(1);
       LM_CUDA_TRY(cudaGetLastError());
     }
-    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, s.Ahi, s.ld, UThi, kNB, 0.0f, A21, lda, st, s.Alo, UTlo));
+    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, s.Ahi, s.ld, d[2], kNB, 0.0f, A21, lda, st, s.Alo, d[3]));
     {
-      // U12 = inv(L11) A12 from the transposed split of A12
       Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 4.0 * 2.0 * m * w, st);
       dim3 tb(32, 8), tg(cdiv(m, 32), cdiv(w, 32));
       transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, A12, lda, w, m);
       count_launch(1);
       LM_CUDA_TRY(cudaGetLastError());
     }
-    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, s.Lhi, kNB, s.Bhi, s.ld, 0.0f, A12, lda, st, s.Llo, s.Blo));
-    LM_TRY(s_update(c, m, m, w, A21, lda, A12, A21 + w, s, st));
+    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, s.Bhi, s.ld, 0.0f, A12, lda, st, d[1], s.Blo));
+    // split operands of the update: L21 -> Ahi/Alo, U12^T -> Bhi/Blo
+    {
+      dim3 tb(32, 8), tg(cdiv(m, 32), cdiv(w, 32));
+      transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, A12, lda, w, m);
+      split_kernel<<<grid_of((long long)m * w), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, w);
+      count_launch(2);
+      LM_CUDA_TRY(cudaGetLastError());
+    }
+    const int w2 = std::min(kNB, m);
+    LM_TRY(sgemm_tf32(c, w2, w2, w, -1.0f, s.Ahi, s.ld, s.Bhi, s.ld, 1.0f, A22, lda, st, s.Alo, s.Blo));
+    LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
+    LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
+    LM_TRY(diag(k0 + w, aux));
+    LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
+    if (m > w2) {
+      LM_TRY(sgemm_tf32(c, w2, m - w2, w, -1.0f, s.Ahi, s.ld, s.Bhi + (size_t)w2 * s.ld, s.ld, 1.0f, A22 + w2, lda, st,
+                        s.Alo, s.Blo + (size_t)w2 * s.ld, nsm - 1));
+      LM_TRY(sgemm_tf32(c, m - w2, m, w, -1.0f, s.Ahi + (size_t)w2 * s.ld, s.ld, s.Bhi, s.ld, 1.0f,
+                        A22 + (long long)w2 * lda, lda, st, s.Alo + (size_t)w2 * s.ld, s.Blo, nsm - 1));
+    }
+    LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
   }
   return LM_OK;
 }

@@ -282,7 +282,7 @@ void count_launch(int n);
 
 int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
                long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
-               const float* Btlo) {
+               const float* Btlo, int max_ctas) {
   if (m <= 0 || n <= 0) return LM_OK;
   if (k <= 0) return LM_ERR_ARG;
   const bool split = Alo != nullptr && Btlo != nullptr;
@@ -320,7 +320,7 @@ int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long 
   g.tiles_n = cdiv(n, TBN);
   g.num_tiles = g.tiles_m * g.tiles_n;
   g.status = ctx_status(ctx);
-  const int grid = std::min(g.num_tiles, ctx_num_sms(ctx));
+  const int grid = std::min(g.num_tiles, max_ctas > 0 ? std::min(max_ctas, ctx_num_sms(ctx)) : ctx_num_sms(ctx));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(T_THREADS, 1, 1);
