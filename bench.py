@@ -67,6 +67,7 @@ def parse():
     p.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
     p.add_argument("--pool", type=int, default=48, help="serve: distinct pregenerated systems")
     p.add_argument("--max-n", type=int, default=4096, help="serve: largest order")
+    p.add_argument("--workers", type=int, default=8, help="serve: concurrent large solves")
     p.add_argument("--count", type=int, default=10000, help="batch: number of instances")
     p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
     p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
@@ -283,7 +284,7 @@ def run_serve(a, world, rank, local):
     g = np.random.Generator(np.random.Philox(a.seed + 99 + 7919 * rank))
     rhs = {r: torch.from_numpy(g.uniform(-1.0, 1.0, (a.max_n, r))).pin_memory() for r in (1, 8, 32)}
     free_b, _ = torch.cuda.mem_get_info()
-    srv = lmb200.Server(local, max_n=a.max_n, max_nrhs=32, large_workers=4, batch_lanes=2,
+    srv = lmb200.Server(local, max_n=a.max_n, max_nrhs=32, large_workers=a.workers, batch_lanes=2,
                         hbm_budget=int(min(free_b // 3, 48 << 30)))
     # arrival schedule and request draws (seeded, fixed before the run)
     total = int(a.rate * a.duration)

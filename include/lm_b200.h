@@ -263,15 +263,17 @@ int lm_batch_tune_set(lm_ctx* ctx, const int* nb /* [2][4] */);
  * the persistent batch kernel (batch_lanes streams, each micro-batch taking
  * every small request queued when its lane frees up), larger ones each take
  * one of `large_workers` contexts (own stream; workspaces pre-grown at start-up
- * for max_n x max_nrhs): mixed-precision LU + FP64 refinement for general
- * matrices (large_precision LM_PREC_FP32_IR), FP64 LU when refinement does not
- * converge, FP64 Cholesky for SPD ones.  A, B (read) and X (written) are the
+ * for max_n x max_nrhs): with large_precision LM_PREC_FP32_IR the
+ * mixed-precision solve of lm_dgesv_ir (FP32 factor + FP64 refinement, for
+ * general and SPD matrices alike), then FP64 LU (general) or FP64 Cholesky
+ * (SPD) when refinement does not converge; with LM_PREC_FP64 FP64 LU or
+ * Cholesky directly.  A, B (read) and X (written) are the
  * caller's host buffers (pinned for asynchronous copies) and must stay valid
  * until the request completes.  Status of a completed request: 0, LAPACK-style
  * info > 0, or < 0 on error / cancellation. */
 typedef struct {
   size_t hbm_budget;    /* bytes of the request arena (0 = 1/4 of free memory) */
-  int large_workers;    /* concurrent large solves (default 4) */
+  int large_workers;    /* concurrent large solves (default 8) */
   int batch_lanes;      /* concurrent micro-batches (default 2) */
   int small_max_n;      /* largest n sent to the batch kernel (default 256, <= 256) */
   int small_precision;  /* LM_PREC_FP64 (default) or LM_PREC_FP32_IR */

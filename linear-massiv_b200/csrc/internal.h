@@ -53,8 +53,9 @@ size_t trsv_inv_elems(int n);
 // unit-lower L and upper U (16-byte aligned, trsv_inv_elems<T>(n) each).
 template <typename T>
 int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaStream_t st);
-// X (n x nrhs, nrhs <= 4) <- U^-1 L^-1 X in two persistent launches; `sync`
-// is 4 ints of device scratch.
+// X (n x nrhs) <- U^-1 L^-1 X, two persistent launches per pass (FP64:
+// nrhs <= 4; FP32: any nrhs, in passes of 16 beyond 4); `sync` is 4 ints of
+// device scratch.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
             int* sync, int* status, cudaStream_t st);

@@ -145,10 +145,6 @@ __global__ void colmax_abs_kernel(const double* V, long long ldv, int rows, int 
   }
 }
 
-__global__ void iota_kernel(int* p, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = i;
-}
-
 int grid_of(long long total) { return (int)std::max<long long>(1, std::min<long long>(cdivll(total, 256), 2048)); }
 
 // Scratch for the split operands of the 3xTF32 update: L21 -> Ahi/Alo
@@ -295,13 +291,6 @@ int convert_d2s(float* dst, long long ldd, const double* src, long long lds, int
 
 namespace {
 
-int identity_pivots(int* ipiv, int n, cudaStream_t st) {
-  iota_kernel<<<grid_of(n), 256, 0, st>>>(ipiv, n);
-  count_launch(1);
-  LM_CUDA_TRY(cudaGetLastError());
-  return LM_OK;
-}
-
 // Refinement loop shared by both low-precision factorisations.  R (n x ldr
 // FP64), D (np x ldr FP32, np >= n) and nrm (2 + 3 * 64 words, nrm[0] and
 // nrm[1..] already hold ||A||_inf and ||B_c||_inf) are device scratch.
@@ -405,7 +394,6 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   int* tsync = reinterpret_cast<int*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes);
   float* Wg = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes +
                                        sync_bytes);
-  const bool fast_trsv = nrhs <= 4;
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
 
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
@@ -413,20 +401,16 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   LM_TRY(factor_runner([&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
     LM_TRY(sgetrf(c, n, A32, lda32, ipiv, s));
-    if (!fast_trsv) return LM_OK;
     return tri_inv_blocks<float>(A32, lda32, n, DinvL, DinvU, s);
   }));
   return refine(c, n, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, false, R, ldr, D, nrm, iters_out, berr_out, st,
                 [&](float* Dd, cudaStream_t s) {
-                  if (fast_trsv) {
-                    {
-                      Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
-                      LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
-                    }
-                    Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, s);
-                    return trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s);
+                  {
+                    Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
+                    LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
                   }
-                  return sgetrs(c, n, nrhs, A32, lda32, ipiv, Dd, ldr, s);
+                  Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, s);
+                  return trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s);
                 });
 }
 
@@ -532,7 +516,6 @@ int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
   const long long lda32 = (np + 31) / 32 * 32;
   const long long ldr = (nrhs + 7) / 8 * 8;
   const size_t a32_bytes = sizeof(float) * (size_t)np * lda32;
-  const size_t piv_bytes = sizeof(int) * (size_t)((np + 63) / 64 * 64);
   const size_t r_bytes = sizeof(double) * (size_t)n * ldr;
   const size_t d_bytes = (sizeof(float) * (size_t)np * ldr + 15) / 16 * 16;
   const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(2 + 3 * 64);
@@ -541,13 +524,10 @@ int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
   const size_t diag_bytes = 4 * sizeof(double) * (size_t)np;
   const size_t sync_bytes = 64;
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + diag_bytes + sync_bytes,
-                       &ws));
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + diag_bytes + sync_bytes, &ws));
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   p += a32_bytes;
-  int* ipiv = reinterpret_cast<int*>(p);
-  p += piv_bytes;
   double* R = reinterpret_cast<double*>(p);
   p += r_bytes;
   float* D = reinterpret_cast<float*>(p);
@@ -561,25 +541,18 @@ int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
   double* dv = du + 2 * (size_t)np;
   p += diag_bytes;
   int* tsync = reinterpret_cast<int*>(p);
-  const bool fast_trsv = nrhs <= 4;
-
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
   LM_TRY(factor_runner([&](cudaStream_t s) {
     LM_TRY(rbt_diagonals(du, dv, np, s));
     LM_TRY(rbt_transform(A32, lda32, A, lda, n, np, du, dv, s));
-    LM_TRY(sgetrf_nopiv(c, np, A32, lda32, DinvL, DinvU, s));
-    if (fast_trsv) return LM_OK;
-    // identity swap list for the blocked substitutions
-    return identity_pivots(ipiv, np, s);
+    return sgetrf_nopiv(c, np, A32, lda32, DinvL, DinvU, s);
   }));
   return refine(c, n, np, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, true, R, ldr, D, nrm, iters_out, berr_out, st,
                 [&](float* Dd, cudaStream_t s) {
                   LM_TRY(rbt_rows(Dd, ldr, np, nrhs, du, true, s));
-                  if (fast_trsv) {
+                  {
                     Prof pt(c, kPhaseTrsm, 2.0 * np * np * nrhs, 4.0 * np * np, s);
                     LM_TRY(trsv_lu<float>(A32, lda32, np, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s));
-                  } else {
-                    LM_TRY(sgetrs(c, np, nrhs, A32, lda32, ipiv, Dd, ldr, s));
                   }
                   return rbt_rows(Dd, ldr, np, nrhs, dv, false, s);
                 });

@@ -9,9 +9,9 @@
 //     kernel (batch.cu) on its own stream; requests arriving meanwhile join
 //     the next micro-batch on whichever lane frees first;
 //   larger requests each take a worker (own context, stream and pre-grown
-//     workspace): mixed-precision LU with FP64 refinement (lm_dgesv_ir), FP64
-//     LU when refinement does not converge or the FP32 factor breaks down, and
-//     FP64 Cholesky for SPD requests.
+//     workspace): mixed-precision LU with FP64 refinement (lm_dgesv_ir) for
+//     general and SPD requests alike, then FP64 LU (general) or FP64 Cholesky
+//     (SPD) when refinement does not converge or the FP32 factor breaks down.
 // Admission by HBM footprint: every admitted request holds one block of a
 // device arena (its A, B, X, factor and pivots); a request is admitted only
 // when its block can be carved from the free space (first fit, coalescing on
@@ -357,7 +357,7 @@ int worker_solve(lm_server* s, Worker* w, Req* r) {
   LM_CUDA_TRY(cudaMemcpyAsync(dB, r->B, nr, cudaMemcpyHostToDevice, st));
   int info = 0, rc = LM_OK;
   bool fp64 = true;
-  if (r->kind == LM_BATCH_GENERAL && s->cfg.large_precision == LM_PREC_FP32_IR) {
+  if (s->cfg.large_precision == LM_PREC_FP32_IR) {
     int it = 0;
     double be = 0;
     rc = lm_dgesv_ir(w->ctx, r->n, r->nrhs, dA, r->n, dB, r->nrhs, dX, r->nrhs, 0.0, 30, &it, &be, &info);
@@ -546,7 +546,7 @@ int lm_server_default_config(lm_server_config* c) {
   if (!c) return LM_ERR_ARG;
   std::memset(c, 0, sizeof(*c));
   c->hbm_budget = 0;
-  c->large_workers = 4;
+  c->large_workers = 8;
   c->batch_lanes = 2;
   c->small_max_n = 256;
   c->small_precision = LM_PREC_FP64;

@@ -26,6 +26,8 @@
 // Thread (r, q) of a block owns row r and, of every tile, the float4/double2
 // groups at columns 16 v + 4 q (FP32) so that the four threads of a row read
 // 64 contiguous bytes per load instruction.
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -35,7 +37,8 @@ void count_launch(int n);
 
 namespace {
 
-constexpr int MAX_RHS = 4;
+constexpr int MAX_RHS = 4;    // one pass, both precisions
+constexpr int WIDE_RHS = 16;  // one pass of the FP32 wide variant
 
 template <typename T>
 struct TrsvCfg;
@@ -149,11 +152,12 @@ __device__ __forceinline__ void load_row_share(T* out, const T* src, int c0, int
 // One direction of the blocked substitution.  forward: L unit lower, blocks in
 // increasing order; backward: U upper, blocks in decreasing order.
 // sync[0] = progress counter, sync[1] = ticket dispenser (both zero at launch).
-template <typename T>
+template <typename T, int RHS>
 __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
                                                              int nrhs, int forward, const T* __restrict__ Dinv,
                                                              T* X, long long ldx, int* sync, int* status,
                                                              int vec_ok) {
+  constexpr int MAX_RHS = RHS;
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
   constexpr bool EXACT = TrsvCfg<T>::EXACT;
   static_assert(NT == 4 * BS, "four threads per row");
@@ -343,25 +347,41 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
   return LM_OK;
 }
 
-// X (n x nrhs, nrhs <= 4) <- U^-1 L^-1 X with the packed factor and (FP32)
-// its block inverses; FP64 ignores DinvL / DinvU.  `sync` holds 4 ints of
-// device scratch.
+// X (n x nrhs) <- U^-1 L^-1 X with the packed factor and (FP32) its block
+// inverses; FP64 ignores DinvL / DinvU and takes nrhs <= 4, FP32 takes any
+// nrhs (more than 4 in passes of 16 columns).  `sync` holds 4 ints of device
+// scratch.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
             int* sync, int* status, cudaStream_t st) {
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC;
-  if (nrhs > MAX_RHS) return LM_ERR_UNSUPPORTED;
   if (n <= 0 || nrhs <= 0) return LM_OK;
   if (!TrsvCfg<T>::EXACT && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
     return LM_ERR_ARG;
   const int nb = (n + BS - 1) / BS;
   const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
-  LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-  trsv_kernel<T><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok);
-  trsv_kernel<T><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok);
-  count_launch(2);
-  LM_CUDA_TRY(cudaGetLastError());
-  return LM_OK;
+  if (nrhs <= MAX_RHS) {
+    LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
+    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok);
+    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok);
+    count_launch(2);
+    LM_CUDA_TRY(cudaGetLastError());
+    return LM_OK;
+  }
+  // more right-hand sides: the FP32 wide variant, WIDE_RHS columns per pass
+  if constexpr (TrsvCfg<T>::EXACT) {
+    return LM_ERR_UNSUPPORTED;
+  } else {
+    for (int c0 = 0; c0 < nrhs; c0 += WIDE_RHS) {
+      const int nc = std::min(WIDE_RHS, nrhs - c0);
+      LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
+      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 1, DinvL, X + c0, ldx, sync, status, vec_ok);
+      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 0, DinvU, X + c0, ldx, sync + 2, status, vec_ok);
+      count_launch(2);
+      LM_CUDA_TRY(cudaGetLastError());
+    }
+    return LM_OK;
+  }
 }
 
 template size_t trsv_inv_elems<float>(int);

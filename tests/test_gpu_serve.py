@@ -1,8 +1,8 @@
 """Serving loop (continuous batching, HBM-budget admission) on the GPU.
 
 Requests mix small instances (micro-batched into the persistent batch kernel)
-and larger ones (mixed-precision LU + FP64 refinement, FP64 fallback, FP64
-Cholesky for SPD).  Checked: every result reaches the normwise backward error
+and larger ones (mixed-precision LU + FP64 refinement for general and SPD
+systems, FP64 LU or Cholesky as the fallback).  Checked: every result reaches the normwise backward error
 1e-15 n; each result is the same alone and in the mix (bitwise: the
 per-request computation does not depend on what else runs); admission never
 exceeds the arena; small requests overtake a large one in flight; host-side
