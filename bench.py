@@ -363,7 +363,8 @@ def run_serve(a, world, rank, local):
         "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"], "max": st["max_ms"]},
         "serving": {k2: st[k2] for k2 in ("completed", "rejected", "failed", "fp64_fallbacks", "queue_peak",
                                           "inflight_peak", "micro_batches", "small_solved", "arena_bytes",
-                                          "arena_peak_bytes", "fixed_bytes", "span_s", "tflops")},
+                                          "arena_peak_bytes", "fixed_bytes", "span_s", "tflops", "ir_solves",
+                                          "ir_gepp", "ir_iterations")},
         "gpu_launches": launches,
         "e2e": {"value": value, "unit": "FP64-accurate solves/s", "api": "lm_server_submit / lm_server_drain",
                 "note": "every request is host-to-host: A, B copied in and X copied out inside its latency"},

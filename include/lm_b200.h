@@ -290,6 +290,9 @@ typedef struct {
   size_t arena_bytes, arena_peak_bytes, fixed_bytes;
   double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> X in the host buffer */
   double span_s, solves_per_s, tflops;    /* first submission to last completion */
+  /* large requests solved by lm_dgesv_ir, how many of those needed its partial-
+   * pivoting fallback (LM_IR_GEPP), and their refinement steps in all */
+  long long ir_solves, ir_gepp, ir_iterations;
 } lm_server_stats_t;
 int lm_server_default_config(lm_server_config* cfg);
 typedef struct lm_server lm_server;

@@ -35,6 +35,9 @@ struct Ctx {
   cudaStream_t side = nullptr;  // capture stream when the caller's stream is the legacy default
   cudaStream_t aux = nullptr;   // look-ahead stream of the factorisations (ctx_aux)
   cudaEvent_t ev_la[2] = {};    // its fork / join events
+  void* pinned = nullptr;       // ctx_pinned
+  size_t pinned_bytes = 0;
+  size_t max_graphs = 16;
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   bool prof = false;
   std::vector<ProfRec> recs;
@@ -109,6 +112,26 @@ Prof::~Prof() {
 
 int* ctx_status(Ctx& c) { return c.d_status; }
 int ctx_num_sms(Ctx& c) { return c.num_sms; }
+
+int ctx_pinned(Ctx& c, size_t bytes, void** ptr) {
+  if (c.pinned_bytes < bytes) {
+    if (c.pinned) {
+      LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+      cudaFreeHost(c.pinned);
+      c.pinned = nullptr;
+      c.pinned_bytes = 0;
+    }
+    const size_t want = std::max(bytes, (size_t)4096);
+    if (cudaMallocHost(&c.pinned, want) != cudaSuccess) {
+      cudaGetLastError();
+      set_last_error("pinned host allocation failed");
+      return LM_ERR_NOMEM;
+    }
+    c.pinned_bytes = want;
+  }
+  *ptr = c.pinned;
+  return LM_OK;
+}
 
 int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join) {
   if (!c.aux) {
@@ -201,7 +224,7 @@ int run_graphed(Ctx& c, const std::string& key0, F&& body) {
   for (auto& g : c.gcache)
     if (g.key == key) e = &g;
   if (!e) {
-    if (c.gcache.size() >= 16) {
+    if (c.gcache.size() >= c.max_graphs) {
       if (c.gcache.front().exec) cudaGraphExecDestroy(c.gcache.front().exec);
       c.gcache.erase(c.gcache.begin());
     }
@@ -300,6 +323,12 @@ void ctx_set_graphs(lm_ctx* ctx, bool on) {
   std::lock_guard<std::mutex> lock(ctx->c.mu);
   ctx->c.graphs = on;
 }
+
+void ctx_set_graph_cache(lm_ctx* ctx, int max_graphs) {
+  if (!ctx || max_graphs < 1) return;
+  std::lock_guard<std::mutex> lock(ctx->c.mu);
+  ctx->c.max_graphs = (size_t)max_graphs;
+}
 }  // namespace lm
 
 namespace {
@@ -367,6 +396,7 @@ int lm_ctx_destroy(lm_ctx* ctx) {
       if (g.exec) cudaGraphExecDestroy(g.exec);
     if (ctx->c.side) cudaStreamDestroy(ctx->c.side);
     if (ctx->c.aux) cudaStreamDestroy(ctx->c.aux);
+    if (ctx->c.pinned) cudaFreeHost(ctx->c.pinned);
     for (auto e : ctx->c.ev_la)
       if (e) cudaEventDestroy(e);
     if (ctx->c.ev_in) cudaEventDestroy(ctx->c.ev_in);
@@ -565,21 +595,28 @@ int finish_info(Ctx& c, int* info) {
 // the reported info is that of the method whose result is returned.
 int ir_solve(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters, double* berr, const char* tag) {
-  const std::string t(tag);
+  // graph keys: the factor depends on A; a refinement step on every buffer
+  auto runner = [&](const char* method) {
+    return [&c, n, nrhs, A, lda, B, ldb, X, ldx, tag, method](const char* what,
+                                                              const std::function<int(cudaStream_t)>& body) {
+      const std::string k = std::string(method) + "_" + tag + "_" + what;
+      const std::string key =
+          std::strcmp(what, "factor") == 0
+              ? lm::gkey(k.c_str(), {n, (long long)A, lda})
+              : lm::gkey(k.c_str(), {n, nrhs, (long long)A, lda, (long long)B, ldb, (long long)X, ldx});
+      return lm::run_graphed(c, key, body);
+    };
+  };
   if (c.ir_method == LM_IR_RBT) {
-    const std::string key = lm::gkey(("rbt_ir_" + t).c_str(), {n, (long long)A, lda, nrhs <= 4 ? 1 : 0});
-    int r = lm::dgesv_rbt_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream,
-                             [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+    int r = lm::dgesv_rbt_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream, runner("rbt"));
     if (r != LM_ERR_NOT_CONVERGED) {
       c.ir_last = LM_IR_RBT;
       return r;
     }
     LM_TRY(lm::reset_info(c));
   }
-  const std::string key = lm::gkey(("sgetrf_ir_" + t).c_str(), {n, (long long)A, lda, nrhs <= 4 ? 1 : 0});
   c.ir_last = LM_IR_GEPP;
-  return lm::dgesv_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream,
-                      [&](const std::function<int(cudaStream_t)>& body) { return lm::run_graphed(c, key, body); });
+  return lm::dgesv_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream, runner("gepp"));
 }
 
 }  // namespace

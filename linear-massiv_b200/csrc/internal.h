@@ -25,6 +25,8 @@ int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr);
 // The context's look-ahead stream (highest priority, created on first use,
 // which must not be inside a stream capture) and its fork / join events.
 int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join);
+// Grow-only pinned host buffer owned by the context (not inside a capture).
+int ctx_pinned(Ctx& c, size_t bytes, void** ptr);
 
 // Per-phase CUDA-event tracing (enabled by lm_ctx_profile).  A Prof scope
 // brackets the kernels launched inside it with events on stream `st`.
@@ -163,9 +165,12 @@ int potrf_block(Ctx& c, T* A, long long lda, int w, int base, cudaStream_t st);
 int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st);
 int sgetrs(Ctx& c, int n, int nrhs, const float* LU, long long lda, const int* ipiv, float* X, long long ldx,
            cudaStream_t st);
+// Runs a fixed launch sequence tagged "factor" or "iter" (the caller maps the
+// tag and the solve's buffers to a CUDA-graph key, or runs it eagerly).
+using IrRunner = std::function<int(const char* tag, const std::function<int(cudaStream_t)>& body)>;
 int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
-             const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner);
+             const IrRunner& run);
 
 // Randomised variant (ir.cu, rbt.cu): depth-2 random butterflies on both
 // sides, FP32 LU without pivoting on the tensor cores, FP64 refinement.
@@ -173,7 +178,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 // to dgesv_ir).
 int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
                  long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
-                 const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner);
+                 const IrRunner& run);
 int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, cudaStream_t st);
 // Depth-2 recursive butterflies (rbt.cu); np is a multiple of 4.
 int rbt_diagonals(double* du, double* dv, int np, cudaStream_t st);
@@ -195,6 +200,8 @@ int dresidual(Ctx& c, int n, int nrhs, const double* A, long long lda, const dou
 // (api.cu); the serving loop's workers run each request on fresh arena
 // addresses, where capture would not pay.
 void ctx_set_graphs(lm_ctx* ctx, bool on);
+// Most captured graphs a context keeps (oldest evicted first; default 16).
+void ctx_set_graph_cache(lm_ctx* ctx, int max_graphs);
 
 // --- batched persistent factor + solve (batch.cu) ------------------------------
 struct BatchLimits {

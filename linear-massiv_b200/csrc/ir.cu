@@ -301,26 +301,33 @@ namespace {
 // early.
 int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
            long long ldx, double tol, int max_iter, bool stall_exit, double* R, long long ldr, float* D,
-           unsigned long long* nrm, int* iters_out, double* berr_out, cudaStream_t st,
+           unsigned long long* nrm, int* iters_out, double* berr_out, cudaStream_t st, const IrRunner& run,
            const std::function<int(float*, cudaStream_t)>& correct) {
   // x = 0, r = b
   LM_CUDA_TRY(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * nrhs, n, st));
   LM_TRY(copy2d<double>(R, ldr, B, ldb, n, nrhs, st));
-  std::vector<unsigned long long> h(1 + 3 * 64);
+  const size_t hwords = 1 + 3 * 64;
+  unsigned long long* h = nullptr;  // pinned: the copy below is part of the iteration's graph
+  LM_TRY(ctx_pinned(c, sizeof(unsigned long long) * hwords, reinterpret_cast<void**>(&h)));
   int it = 0;
   double worst = 0.0, prev = 1e300;
   for (it = 1; it <= max_iter; ++it) {
-    LM_TRY(convert_d2s(D, ldr, R, ldr, n, nrhs, st));
-    if (np > n) LM_CUDA_TRY(cudaMemsetAsync(D + (size_t)n * ldr, 0, sizeof(float) * (size_t)(np - n) * ldr, st));
-    LM_TRY(correct(D, st));
-    add_s2d_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, D, ldr, n, nrhs);
-    count_launch(1);
-    LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, st));
-    LM_CUDA_TRY(cudaMemsetAsync(nrm + 1 + 64, 0, sizeof(unsigned long long) * 128, st));
-    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(R, ldr, n, nrhs, nrm + 1 + 64);
-    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, n, nrhs, nrm + 1 + 128);
-    count_launch(2);
-    LM_CUDA_TRY(cudaMemcpyAsync(h.data(), nrm, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost, st));
+    // one correction step as a fixed launch sequence (captured and replayed
+    // by the runner), ending with the norms copied to the host
+    LM_TRY(run("iter", [&](cudaStream_t s) {
+      LM_TRY(convert_d2s(D, ldr, R, ldr, n, nrhs, s));
+      if (np > n) LM_CUDA_TRY(cudaMemsetAsync(D + (size_t)n * ldr, 0, sizeof(float) * (size_t)(np - n) * ldr, s));
+      LM_TRY(correct(D, s));
+      add_s2d_kernel<<<grid_of((long long)n * nrhs), 256, 0, s>>>(X, ldx, D, ldr, n, nrhs);
+      count_launch(1);
+      LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, s));
+      LM_CUDA_TRY(cudaMemsetAsync(nrm + 1 + 64, 0, sizeof(unsigned long long) * 128, s));
+      colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, s>>>(R, ldr, n, nrhs, nrm + 1 + 64);
+      colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, s>>>(X, ldx, n, nrhs, nrm + 1 + 128);
+      count_launch(2);
+      LM_CUDA_TRY(cudaMemcpyAsync(h, nrm, sizeof(unsigned long long) * hwords, cudaMemcpyDeviceToHost, s));
+      return LM_OK;
+    }));
     LM_CUDA_TRY(cudaStreamSynchronize(st));
     auto dbl = [](unsigned long long u) {
       double d;
@@ -368,7 +375,7 @@ int input_norms(int n, int nrhs, const double* A, long long lda, const double* B
 // LM_ERR_NOT_CONVERGED if some column misses tol after max_iter steps.
 int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
-             const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner) {
+             const IrRunner& run) {
   const long long lda32 = (n + 31) / 32 * 32;
   const long long ldr = (nrhs + 7) / 8 * 8;
   const size_t a32_bytes = sizeof(float) * (size_t)n * lda32;
@@ -398,12 +405,12 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
   // factor fl32(A)
-  LM_TRY(factor_runner([&](cudaStream_t s) {
+  LM_TRY(run("factor", [&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
     LM_TRY(sgetrf(c, n, A32, lda32, ipiv, s));
     return tri_inv_blocks<float>(A32, lda32, n, DinvL, DinvU, s);
   }));
-  return refine(c, n, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, false, R, ldr, D, nrm, iters_out, berr_out, st,
+  return refine(c, n, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, false, R, ldr, D, nrm, iters_out, berr_out, st, run,
                 [&](float* Dd, cudaStream_t s) {
                   {
                     Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
@@ -510,7 +517,7 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
 // stalls or runs out of steps; the caller then falls back to partial pivoting.
 int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
                  long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
-                 const std::function<int(const std::function<int(cudaStream_t)>&)>& factor_runner) {
+                 const IrRunner& run) {
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
   const int np = (n + 3) / 4 * 4;
   const long long lda32 = (np + 31) / 32 * 32;
@@ -542,12 +549,12 @@ int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
   p += diag_bytes;
   int* tsync = reinterpret_cast<int*>(p);
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
-  LM_TRY(factor_runner([&](cudaStream_t s) {
+  LM_TRY(run("factor", [&](cudaStream_t s) {
     LM_TRY(rbt_diagonals(du, dv, np, s));
     LM_TRY(rbt_transform(A32, lda32, A, lda, n, np, du, dv, s));
     return sgetrf_nopiv(c, np, A32, lda32, DinvL, DinvU, s);
   }));
-  return refine(c, n, np, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, true, R, ldr, D, nrm, iters_out, berr_out, st,
+  return refine(c, n, np, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, true, R, ldr, D, nrm, iters_out, berr_out, st, run,
                 [&](float* Dd, cudaStream_t s) {
                   LM_TRY(rbt_rows(Dd, ldr, np, nrhs, du, true, s));
                   {

@@ -105,6 +105,7 @@ struct Req {
   // arena block: [A n*n][B n*r][X n*r][F n*n (small only)][ipiv n ints]
   size_t off = 0, bytes = 0, oA = 0, oB = 0, oX = 0, oF = 0, oP = 0;
   int status = 0, iters = 0;
+  int ir_method = -1;  // method of a large mixed-precision solve (LM_IR_*), -1 if none
   bool fallback = false, done = false, cancelled = false;
 };
 
@@ -149,6 +150,10 @@ struct Worker {
   bool busy = false;
   std::condition_variable cv;
   double busy_s = 0;
+  // fixed operands of the mixed-precision solve (max_n x max_n, max_n x
+  // max_nrhs): a request of an order this worker has seen before replays the
+  // solve's captured CUDA graphs instead of launching every kernel again
+  double *Aw = nullptr, *Bw = nullptr, *Xw = nullptr;
 };
 
 }  // namespace
@@ -166,6 +171,7 @@ struct lm_server {
   std::vector<Worker*> workers;
   std::vector<double> lat_ms;
   long long next_id = 1, completed = 0, rejected = 0, cancelled = 0, fallbacks = 0, failed = 0;
+  long long ir_solves = 0, ir_gepp = 0, ir_iterations = 0;
   size_t queue_peak = 0;
   int inflight = 0, inflight_peak = 0;
   bool stopping = false;
@@ -191,6 +197,11 @@ void complete(lm_server* s, Req* r) {  // under s->mu
   s->lat_ms.push_back((r->t_done - r->t_submit) * 1e3);
   if (r->status < 0) ++s->failed;
   if (r->fallback) ++s->fallbacks;
+  if (r->ir_method >= 0) {
+    ++s->ir_solves;
+    if (r->ir_method == LM_IR_GEPP) ++s->ir_gepp;
+    if (r->iters > 0) s->ir_iterations += r->iters;
+  }
   s->flops_done += req_flops(*r);
 }
 
@@ -360,8 +371,12 @@ int worker_solve(lm_server* s, Worker* w, Req* r) {
   if (s->cfg.large_precision == LM_PREC_FP32_IR) {
     int it = 0;
     double be = 0;
-    rc = lm_dgesv_ir(w->ctx, r->n, r->nrhs, dA, r->n, dB, r->nrhs, dX, r->nrhs, 0.0, 30, &it, &be, &info);
+    LM_CUDA_TRY(cudaMemcpyAsync(w->Aw, dA, nn, cudaMemcpyDeviceToDevice, st));
+    LM_CUDA_TRY(cudaMemcpyAsync(w->Bw, dB, nr, cudaMemcpyDeviceToDevice, st));
+    rc = lm_dgesv_ir(w->ctx, r->n, r->nrhs, w->Aw, r->n, w->Bw, r->nrhs, w->Xw, r->nrhs, 0.0, 30, &it, &be, &info);
+    lm_ctx_ir_last_method(w->ctx, &r->ir_method);
     if (rc == LM_OK) {
+      LM_CUDA_TRY(cudaMemcpyAsync(dX, w->Xw, nr, cudaMemcpyDeviceToDevice, st));
       fp64 = false;
       r->iters = it;
     } else if (rc == LM_ERR_NOT_CONVERGED || rc > 0) {
@@ -441,6 +456,9 @@ void server_free(lm_server* s) {
   }
   for (Worker* w : s->workers) {
     if (w->ctx) lm_ctx_destroy(w->ctx);
+    cudaFree(w->Aw);
+    cudaFree(w->Bw);
+    cudaFree(w->Xw);
     delete w;
   }
   cudaFree(s->arena.base);
@@ -498,7 +516,11 @@ int server_init(lm_server* s) {
     w->s = s;
     s->workers.push_back(w);
     LM_TRY(lm_ctx_create(&w->ctx, s->device));
-    lm::ctx_set_graphs(w->ctx, false);  // arena addresses change per request
+    lm::ctx_set_graph_cache(w->ctx, 256);
+    const size_t nn = (size_t)s->cfg.max_n * s->cfg.max_n, nr = (size_t)s->cfg.max_n * s->cfg.max_nrhs;
+    LM_CUDA_TRY(cudaMalloc(&w->Aw, sizeof(double) * nn));
+    LM_CUDA_TRY(cudaMalloc(&w->Bw, sizeof(double) * nr));
+    LM_CUDA_TRY(cudaMalloc(&w->Xw, sizeof(double) * nr));
     LM_TRY(prewarm(s, w));
   }
   size_t free_after = 0;
@@ -702,6 +724,9 @@ int lm_server_stats(lm_server* s, lm_server_stats_t* o) {
   o->cancelled = s->cancelled;
   o->failed = s->failed;
   o->fp64_fallbacks = s->fallbacks;
+  o->ir_solves = s->ir_solves;
+  o->ir_gepp = s->ir_gepp;
+  o->ir_iterations = s->ir_iterations;
   o->queue_peak = (long long)s->queue_peak;
   o->inflight_peak = s->inflight_peak;
   o->arena_bytes = s->arena.size;
@@ -744,6 +769,7 @@ int lm_server_reset_stats(lm_server* s) {
   std::lock_guard<std::mutex> lk(s->mu);
   s->lat_ms.clear();
   s->completed = s->rejected = s->cancelled = s->failed = s->fallbacks = 0;
+  s->ir_solves = s->ir_gepp = s->ir_iterations = 0;
   s->queue_peak = 0;
   s->inflight_peak = s->inflight;
   s->t_first = s->t_last = 0;

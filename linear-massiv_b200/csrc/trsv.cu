@@ -163,8 +163,11 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
   static_assert(NT == 4 * BS, "four threads per row");
   static_assert(!EXACT || BS == 64, "the one-warp substitution holds two rows per lane");
   __shared__ int tk_sh, prog_sh;
-  __shared__ T xj[2][BS][MAX_RHS];
-  __shared__ T ys[BS][MAX_RHS];
+  // rows padded by one element: the four threads of a row read columns 4 q
+  // apart, which an unpadded power-of-two row length puts in one bank
+  constexpr int XS = MAX_RHS + 1;
+  __shared__ T xj[2][BS][XS];
+  __shared__ T ys[BS][XS];
   __shared__ TrsvDiag<T, EXACT> diag;
   const int nb = (n + BS - 1) / BS;
   if (threadIdx.x == 0) tk_sh = atomicAdd(sync + 1, 1);
@@ -224,7 +227,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
       __syncthreads();
       known = prog_sh;
     }
-    T(*xs)[MAX_RHS] = xj[d & 1];
+    T(*xs)[XS] = xj[d & 1];
     for (int i = threadIdx.x; i < BS * nrhs; i += NT) {
       const int rr = i / nrhs, h = i % nrhs;
       const int row = j * BS + rr;

@@ -595,7 +595,8 @@ class ServerStats(ctypes.Structure):
                 ("fixed_bytes", ctypes.c_size_t),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("mean_ms", ctypes.c_double),
                 ("max_ms", ctypes.c_double), ("span_s", ctypes.c_double), ("solves_per_s", ctypes.c_double),
-                ("tflops", ctypes.c_double)]
+                ("tflops", ctypes.c_double), ("ir_solves", ctypes.c_longlong), ("ir_gepp", ctypes.c_longlong),
+                ("ir_iterations", ctypes.c_longlong)]
 
 
 class Server:
