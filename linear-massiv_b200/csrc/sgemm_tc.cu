@@ -5,7 +5,8 @@
 //
 // One CTA per SM, persistent over 128 x 128 output tiles:
 //   warp 0      TMA producer: A / Bt k-slices (32 floats = one 128-byte
-//               swizzle row) into a 4-stage ring, and each tile's C block;
+//               swizzle row) into the stage ring, and an L2 prefetch of each
+//               tile's C block as the tile starts;
 //   warp 1      MMA issuer (one thread): 4 x tcgen05.mma (K = 8) per slice
 //               into a TMEM accumulator (two 128-column buffers, so the next
 //               tile's MMAs overlap this tile's epilogue); tcgen05.commit
@@ -93,6 +94,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* tmap, int x, int y) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
+                   reinterpret_cast<uint64_t>(tmap)),
+               "r"(x), "r"(y)
+               : "memory");
+}
 __device__ __forceinline__ void tma_store_2d(const CUtensorMap* tmap, const void* smem_src, int x, int y) {
   asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
                    reinterpret_cast<uint64_t>(tmap)),
@@ -172,6 +179,12 @@ __global__ void __launch_bounds__(T_THREADS, 1)
       int it = 0;
       for (int t = blockIdx.x; t < g.num_tiles && ok; t += gridDim.x) {
         const int tm = t % g.tiles_m, tn = t / g.tiles_m;
+        // this tile's C block towards L2 while its operands stream in, so
+        // that the epilogue's C load does not wait on DRAM
+        if (use_beta) {
+#pragma unroll
+          for (int q = 0; q < TBN / 32; ++q) tma_prefetch_l2_2d(&tmC, tn * TBN + q * 32, tm * TBM);
+        }
         for (int kb = 0; kb < KT && ok; ++kb, ++it) {
           const int s = it % TSTAGES;
           const uint32_t ph = (uint32_t)((it / TSTAGES) & 1) ^ 1u;
