@@ -635,12 +635,21 @@ def run_reference(a, world, rank):
 # launch divided by that launch's algorithmic bytes); the per-launch traffic
 # of this run is that ratio times its own average algorithmic bytes per launch.
 DRAM_PER_ALGO_BYTE = {
-    "dgemm": 1.11e9 / 1.090e9,   # profiles/dgemm_dmma_k128_n8192.md
+    "dgemm": 1.11e9 / 1.090e9,     # profiles/dgemm_dmma_k128_n8192.md
+    "sgemm": 481.2e6 / 528.0e6,    # profiles/sgemm_tf32_trailing_ir_n8192.md
 }
 
 
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (of measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+
+
 def traffic_per_launch(a, gp, steps):
-    key = "dgemm" if a.workload in ("lu", "chol", "gemm") else None
+    key = "dgemm" if a.workload in ("lu", "chol", "gemm") else "sgemm"
     if key is None or key not in DRAM_PER_ALGO_BYTE or not gp.get("launches"):
         return None
     return DRAM_PER_ALGO_BYTE[key] * gp["bytes"] / gp["launches"]
@@ -707,8 +716,12 @@ def run_ours(a, world, rank, local):
         accuracy = {"backward_error": num / den, "bound": 1e-15 * n}
         del R
     peak = None
+    tf32_peak = None
     if rank == 0 and not a.no_peak:
-        peak = measure_tf32_peak(torch) if a.workload == "ir" else measure_fp64_peak(torch)
+        if a.workload == "ir":
+            tf32_peak = measure_tf32_peak(torch)
+        else:
+            peak = measure_fp64_peak(torch)
 
     # Timed region: the captured CUDA graphs of the solve, no per-kernel events.
     launches0 = lmb200.launch_count()
@@ -811,14 +824,22 @@ def run_ours(a, world, rank, local):
     if rank != 0:
         return
     ps = max(a.profile_steps, 1)
-    gp = phases["gemm"] if phases else {"flops": 0.0, "ms": 0.0, "launches": 0}
-    achieved = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
+    gp = phases["gemm"] if phases else {"flops": 0.0, "ms": 0.0, "launches": 0, "bytes": 0.0}
     total_ms = sum(p["ms"] for p in phases.values()) if phases else 0.0
+    extra = {}
     if a.workload == "ir":
+        # the k = 128 trailing updates read and write C once per step: HBM-bound
         roof_kernel = "sgemm_tf32_kernel (tcgen05 kind::tf32, 3xTF32 split: 3 MMAs per logical product)"
-        peak_src = "cuBLAS TF32 GEMM (FP32 storage, allow_tf32) 8192^3 measured in this run"
+        bound, unit = "hbm", "GB/s"
+        achieved = gp["bytes"] / (gp["ms"] * 1e-3) / 1e9 if gp["ms"] > 0 else None
+        peak, peak_src = measured_hbm_gbs()
+        tf32 = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
+        extra = {"tf32_mma_tflops": tf32, "tf32_peak_tflops": tf32_peak,
+                 "tf32_peak_source": "cuBLAS TF32 GEMM (FP32 storage, allow_tf32) 8192^3 measured in this run"}
     else:
         roof_kernel = "dgemm_dmma_kernel (FP64 DMMA)"
+        bound, unit = "tensor", "TFLOP/s"
+        achieved = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
         peak_src = "cuBLAS DGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64)"
     line = {
         "metric": metric_name(a), "value": value, "unit": metric_name(a), "n_gpus": world, "steps": a.steps,
@@ -830,15 +851,15 @@ def run_ours(a, world, rank, local):
         "e2e": {"value": e2e_val, "unit": metric_name(a), "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": a.e2e_steps, "api": {"lu": "lm_lu_solve_host", "chol": "lm_chol_solve_host", "gemm": "lm_matmul_host",
                                              "ir": "lm_lu_solve_ir_host"}[a.workload]},
-        "roofline": {"bound": "tensor", "kernel": roof_kernel,
-                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "roofline": {"bound": bound, "kernel": roof_kernel,
+                     "achieved": achieved, "peak": peak, "unit": unit,
                      "frac": (achieved / peak) if (achieved and peak) else None,
                      "traffic": traffic_per_launch(a, gp, ps),
                      "peak_source": peak_src,
                      "launches_per_step": gp["launches"] / ps,
                      "timing": f"CUDA events around each launch of the kernel over {a.profile_steps} profiled "
                                f"step(s) run after the timed region ({prof_ms and round(prof_ms, 2)} ms per "
-                               f"profiled step, eager launches)"},
+                               f"profiled step, eager launches)", **extra},
         "phases_ms_per_step": ({k: v["ms"] / ps for k, v in phases.items()} if phases else None),
         "phase_share": ({k: (v["ms"] / total_ms if total_ms else None) for k, v in phases.items()} if phases else None),
         "tflops_whole_step": (2.0 * n * n * kk if a.workload == "gemm" else FLOPS[a.workload](n, nrhs)) * a.steps / t / 1e12,
