@@ -421,29 +421,39 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
                 });
 }
 
-// LU without pivoting of the FP32 matrix A (n x n, lda), right-looking with
-// 128-wide steps in which everything but the 128 x 128 diagonal block runs
-// on the tensor cores (3xTF32):
-//   diagonal block: LU and both inverses in one CTA (nopiv_diag);
-//   L21 = A21 inv(U11);  U12 = inv(L11) A12;  A22 -= L21 U12.
-// DinvL / DinvU receive the diagonal-block inverses in the layout of the
-// persistent substitutions.  A zero pivot is recorded in status[1].
+// LU without pivoting of the FP32 matrix A (n x n, lda), right-looking in
+// super-steps of two 128-column blocks a and b, so that the trailing update
+// is one k = 256 GEMM: it reads and writes A22 once per 256 columns, which
+// halves the HBM traffic that bounds it.  Everything but the 128 x 128
+// diagonal blocks runs on the tensor cores (3xTF32):
+//   a: diagonal block (nopiv_diag: LU and both inverses in one CTA);
+//      L_a = A[below a, a] inv(U_aa),  U_a = inv(L_aa) A[a, right of a];
+//      block b's column and row panels -= L_a U_a (k = 128);
+//   b: diagonal block, L_b and U_b likewise;
+//   A22 -= [L_a L_b] [U_a; U_b]  (k = 256).
+// Look-ahead: each diagonal block is factored on the priority stream, on the
+// SM that the concurrent GEMMs leave free (147 of 148 CTAs): block b beside
+// the rest of its panels' update, the next super-step's block a beside the
+// trailing update.  DinvL / DinvU receive the diagonal-block inverses in the
+// layout of the persistent substitutions.  A zero pivot is recorded in
+// status[1].
 int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, cudaStream_t st) {
-  void* ws = nullptr;
-  SScratch s;
-  s.ld = kNB;
+  constexpr int SW = 2 * kNB;  // super-step width
   const size_t blk = (size_t)kNB * kNB;
-  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * kNB + 8 * blk) + sizeof(int) * kSwapPlanInts, &ws));
-  s.Ahi = static_cast<float*>(ws);
-  s.Alo = s.Ahi + (size_t)n * kNB;
-  s.Bhi = s.Alo + (size_t)n * kNB;
-  s.Blo = s.Bhi + (size_t)n * kNB;
-  // two sets of diagonal-block operands: the look-ahead factors block k + 1
-  // while block k's are still being read
+  const long long ldk = SW;     // K-major operands of the k = 256 update
+  void* ws = nullptr;
+  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * SW + 2 * (size_t)n * kNB + 8 * blk), &ws));
+  float* Ahi = static_cast<float*>(ws);  // [L_a | L_b] split, n x 256 (row i <-> row k0 + wa + i)
+  float* Alo = Ahi + (size_t)n * SW;
+  float* Bhi = Alo + (size_t)n * SW;     // [U_a | U_b]^T split, n x 256 (row j <-> column k0 + wa + j)
+  float* Blo = Bhi + (size_t)n * SW;
+  float* Thi = Blo + (size_t)n * SW;     // operands of the inverse products, n x 128
+  float* Tlo = Thi + (size_t)n * kNB;
+  // two sets of diagonal-block operands (split inverses): the look-ahead
+  // factors the next block while this one's are still being read
   float* inv[2][4];
-  for (int b = 0; b < 2; ++b)
-    for (int q = 0; q < 4; ++q) inv[b][q] = s.Blo + (size_t)n * kNB + (size_t)(4 * b + q) * blk;
-  s.plan = nullptr;
+  for (int q2 = 0; q2 < 2; ++q2)
+    for (int q = 0; q < 4; ++q) inv[q2][q] = Tlo + (size_t)n * kNB + (size_t)(4 * q2 + q) * blk;
   cudaStream_t aux;
   cudaEvent_t ev_fork, ev_join;
   LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
@@ -455,55 +465,86 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
     return nopiv_diag(A + (long long)k0 * lda + k0, lda, w, k0, d[0], d[1], d[2], d[3], kNB,
                       DinvL + (size_t)(k0 / kNB) * blk, DinvU + (size_t)(k0 / kNB) * blk, ctx_status(c), ds);
   };
-  LM_TRY(diag(0, st));
-  // Step k: with the diagonal block factored, L21 = A21 inv(U11) and
-  // U12 = inv(L11) A12 (3xTF32), then A22 -= L21 U12 in three pieces: the next
-  // diagonal block first, whose factorisation then runs on the look-ahead
-  // stream (one CTA on the SM the other pieces leave free) while the rest of
-  // A22 is updated.
-  for (int k0 = 0; k0 < n; k0 += kNB) {
-    const int w = std::min(kNB, n - k0);
-    const int m = n - k0 - w;
-    if (m <= 0) break;
+  auto split_rows = [&](float* hi, float* lo, long long ldd, const float* src, int rows, int cols, cudaStream_t ss) {
+    split_kernel<<<grid_of((long long)rows * cols), 256, 0, ss>>>(hi, lo, ldd, src, lda, rows, cols);
+    count_launch(1);
+    LM_CUDA_TRY(cudaGetLastError());
+    return LM_OK;
+  };
+  auto split_cols = [&](float* hi, float* lo, long long ldd, const float* src, int rows, int cols, cudaStream_t ss) {
+    dim3 tb(32, 8), tg(cdiv(cols, 32), cdiv(rows, 32));
+    transpose_split_kernel<<<tg, tb, 0, ss>>>(hi, lo, ldd, src, lda, rows, cols);
+    count_launch(1);
+    LM_CUDA_TRY(cudaGetLastError());
+    return LM_OK;
+  };
+  // Block at k0 (w wide, diagonal block factored): L = A[k0+w:, k0:k0+w] inv(U)
+  // and U = inv(L) A[k0:k0+w, k0+w:] in place, m = n - k0 - w; then their
+  // splits into column `col` of the k = 256 operands, rows from `row0`.
+  auto block_solves = [&](int k0, int w, int m, float* ahi, float* alo, float* bhi, float* blo) {
     float** d = inv[(k0 / kNB) & 1];
     float* A11 = A + (long long)k0 * lda + k0;
     float* A21 = A11 + (long long)w * lda;
     float* A12 = A11 + w;
-    float* A22 = A21 + w;
     {
-      Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 4.0 * 2.0 * m * w, st);
-      split_kernel<<<grid_of((long long)m * w), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, w);
-      count_launch(1);
-      LM_CUDA_TRY(cudaGetLastError());
+      Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 8.0 * m * w, st);
+      LM_TRY(split_rows(Thi, Tlo, kNB, A21, m, w, st));
     }
-    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, s.Ahi, s.ld, d[2], kNB, 0.0f, A21, lda, st, s.Alo, d[3]));
+    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, Thi, kNB, d[2], kNB, 0.0f, A21, lda, st, Tlo, d[3]));
     {
-      Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 4.0 * 2.0 * m * w, st);
-      dim3 tb(32, 8), tg(cdiv(m, 32), cdiv(w, 32));
-      transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, A12, lda, w, m);
-      count_launch(1);
-      LM_CUDA_TRY(cudaGetLastError());
+      Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 8.0 * m * w, st);
+      LM_TRY(split_cols(Thi, Tlo, kNB, A12, w, m, st));
     }
-    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, s.Bhi, s.ld, 0.0f, A12, lda, st, d[1], s.Blo));
-    // split operands of the update: L21 -> Ahi/Alo, U12^T -> Bhi/Blo
-    {
-      dim3 tb(32, 8), tg(cdiv(m, 32), cdiv(w, 32));
-      transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, A12, lda, w, m);
-      split_kernel<<<grid_of((long long)m * w), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, w);
-      count_launch(2);
-      LM_CUDA_TRY(cudaGetLastError());
-    }
-    const int w2 = std::min(kNB, m);
-    LM_TRY(sgemm_tf32(c, w2, w2, w, -1.0f, s.Ahi, s.ld, s.Bhi, s.ld, 1.0f, A22, lda, st, s.Alo, s.Blo));
+    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, Thi, kNB, 0.0f, A12, lda, st, d[1], Tlo));
+    LM_TRY(split_rows(ahi, alo, ldk, A21, m, w, st));
+    return split_cols(bhi, blo, ldk, A12, w, m, st);
+  };
+  LM_TRY(diag(0, st));
+  for (int k0 = 0; k0 < n; k0 += SW) {
+    const int wa = std::min(kNB, n - k0);
+    const int ma = n - k0 - wa;  // rows below / columns right of block a
+    if (ma <= 0) break;
+    const int wb = std::min(kNB, ma);
+    const int mb = ma - wb;      // rows below / columns right of block b
+    // ---- block a ----
+    LM_TRY(block_solves(k0, wa, ma, Ahi, Alo, Bhi, Blo));
+    float* Abb = A + (long long)(k0 + wa) * lda + k0 + wa;
+    // b's diagonal block first, then its factorisation beside the rest of b's panels
+    LM_TRY(sgemm_tf32(c, wb, wb, wa, -1.0f, Ahi, ldk, Bhi, ldk, 1.0f, Abb, lda, st, Alo, Blo));
     LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
     LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
-    LM_TRY(diag(k0 + w, aux));
+    LM_TRY(diag(k0 + wa, aux));
     LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
-    if (m > w2) {
-      LM_TRY(sgemm_tf32(c, w2, m - w2, w, -1.0f, s.Ahi, s.ld, s.Bhi + (size_t)w2 * s.ld, s.ld, 1.0f, A22 + w2, lda, st,
-                        s.Alo, s.Blo + (size_t)w2 * s.ld, nsm - 1));
-      LM_TRY(sgemm_tf32(c, m - w2, m, w, -1.0f, s.Ahi + (size_t)w2 * s.ld, s.ld, s.Bhi, s.ld, 1.0f,
-                        A22 + (long long)w2 * lda, lda, st, s.Alo + (size_t)w2 * s.ld, s.Blo, nsm - 1));
+    if (mb > 0) {
+      // column panel of b below its diagonal block, row panel of b right of it
+      LM_TRY(sgemm_tf32(c, mb, wb, wa, -1.0f, Ahi + (size_t)wb * ldk, ldk, Bhi, ldk, 1.0f, Abb + (long long)wb * lda, lda,
+                        st, Alo + (size_t)wb * ldk, Blo, nsm - 1));
+      LM_TRY(sgemm_tf32(c, wb, mb, wa, -1.0f, Ahi, ldk, Bhi + (size_t)wb * ldk, ldk, 1.0f, Abb + wb, lda, st, Alo,
+                        Blo + (size_t)wb * ldk, nsm - 1));
+    }
+    LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+    if (mb <= 0) break;
+    // ---- block b ----  (its splits go to column 128 of the operands, rows from wb)
+    LM_TRY(block_solves(k0 + wa, wb, mb, Ahi + (size_t)wb * ldk + kNB, Alo + (size_t)wb * ldk + kNB,
+                        Bhi + (size_t)wb * ldk + kNB, Blo + (size_t)wb * ldk + kNB));
+    // ---- trailing update, k = wa + wb ----
+    const int kk = wa + wb;
+    const float* ah = Ahi + (size_t)wb * ldk;
+    const float* al = Alo + (size_t)wb * ldk;
+    const float* bh = Bhi + (size_t)wb * ldk;
+    const float* bl = Blo + (size_t)wb * ldk;
+    float* A22 = Abb + (long long)wb * lda + wb;
+    const int w2 = std::min(kNB, mb);
+    LM_TRY(sgemm_tf32(c, w2, w2, kk, -1.0f, ah, ldk, bh, ldk, 1.0f, A22, lda, st, al, bl));
+    LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
+    LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
+    LM_TRY(diag(k0 + kk, aux));
+    LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
+    if (mb > w2) {
+      LM_TRY(sgemm_tf32(c, w2, mb - w2, kk, -1.0f, ah, ldk, bh + (size_t)w2 * ldk, ldk, 1.0f, A22 + w2, lda, st, al,
+                        bl + (size_t)w2 * ldk, nsm - 1));
+      LM_TRY(sgemm_tf32(c, mb - w2, mb, kk, -1.0f, ah + (size_t)w2 * ldk, ldk, bh, ldk, 1.0f, A22 + (long long)w2 * lda,
+                        lda, st, al + (size_t)w2 * ldk, bl, nsm - 1));
     }
     LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
   }
