@@ -65,8 +65,10 @@ int trsm_unit_lower_gemm(Ctx& c, const double* L11, long long lda, int w, double
   return dgemm(c, d, st);
 }
 
+// gemm_ctas caps the grid of the panel's own GEMMs (0 = no cap), so that a
+// panel factored beside a trailing update fits on the SMs that update leaves.
 int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv,
-                    const TrsmScratch& s, cudaStream_t st) {
+                    const TrsmScratch& s, cudaStream_t st, int gemm_ctas = 0) {
   const int R = n - c0;
   const int wmax = panel_leaf_max_width_for(c, R);
   if (wmax <= 0) return LM_ERR_UNSUPPORTED;
@@ -79,7 +81,7 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int 
   int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
   if (w1 >= w) w1 = w - 4;
   const int w2 = w - w1;
-  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st));
+  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st, gemm_ctas));
   double* A11 = A + (long long)c0 * lda + c0;
   LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w1, A11 + w1, lda, w2, s, st));
   GemmDesc d;
@@ -88,11 +90,18 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int 
   d.A = A11 + (long long)w1 * lda; d.lda = lda;
   d.B = A11 + w1; d.ldb = lda;
   d.C = A11 + (long long)w1 * lda + w1; d.ldc = lda;
+  d.max_ctas = gemm_ctas;
   LM_TRY(dgemm(c, d, st));
-  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st);
+  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st, gemm_ctas);
 }
 
 }  // namespace
+
+// SMs left to a panel factored beside the trailing update (the widest panel
+// leaf is a cluster of 16 CTAs of one SM each), and the order from which that
+// look-ahead is used.
+constexpr int kLookaheadSms = 16;
+constexpr int kLookaheadMinN = 2048;
 
 int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) {
   TrsmScratch s;
@@ -102,24 +111,55 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
     s.Linv = static_cast<double*>(ws);
     s.plan = reinterpret_cast<int*>(s.Linv + (size_t)kNB * kNB);
   }
+  // Look-ahead: once the next panel's columns are updated, that panel is
+  // factored on the priority stream while the rest of the trailing update
+  // runs with a grid that leaves kLookaheadSms SMs free.  Its own GEMMs are
+  // capped to fit there.  Nothing waits across the two streams inside a
+  // kernel; at worst the panel starts when the update ends.
+  const int nsm = ctx_num_sms(c);
+  const bool la = n >= kLookaheadMinN && nsm > 2 * kLookaheadSms;
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  if (la) LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
+  const int panel_ctas = 2 * kLookaheadSms;
+  const int rest_ctas = 2 * (nsm - kLookaheadSms);
+  LM_TRY(getrf_panel_rec(c, A, lda, n, 0, std::min(kNB, n), 0, std::min(kNB, n), ipiv, s, st));
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
-    LM_TRY(getrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, s, st));
-    // this panel's interchanges on the columns left and right of it
+    // panel k is factored: its interchanges on the columns left and right of it
     {
       Prof p(c, kPhaseSwap, 0.0, 32.0 * w * (n - w), st);
       LM_TRY(laswp<double>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st, s.plan));
     }
-    if (k0 + w < n) {
-      double* A11 = A + (long long)k0 * lda + k0;
-      LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w, A11 + w, lda, n - k0 - w, s, st));
-      GemmDesc d;
-      d.m = n - k0 - w; d.n = n - k0 - w; d.k = w;
-      d.alpha = -1.0; d.beta = 1.0;
-      d.A = A11 + (long long)w * lda; d.lda = lda;
-      d.B = A11 + w; d.ldb = lda;
-      d.C = A11 + (long long)w * lda + w; d.ldc = lda;
-      LM_TRY(dgemm(c, d, st));
+    if (k0 + w >= n) break;
+    const int m = n - k0 - w;
+    const int wn = std::min(kNB, m);  // next panel
+    double* A11 = A + (long long)k0 * lda + k0;
+    LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w, A11 + w, lda, m, s, st));
+    GemmDesc d;  // A22 -= L21 U12, the next panel's columns first
+    d.m = m; d.n = wn; d.k = w;
+    d.alpha = -1.0; d.beta = 1.0;
+    d.A = A11 + (long long)w * lda; d.lda = lda;
+    d.B = A11 + w; d.ldb = lda;
+    d.C = A11 + (long long)w * lda + w; d.ldc = lda;
+    LM_TRY(dgemm(c, d, st));
+    GemmDesc r = d;  // the rest of the columns
+    r.n = m - wn;
+    r.B = A11 + w + wn;
+    r.C = A11 + (long long)w * lda + w + wn;
+    if (la) {
+      LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
+      LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
+      LM_TRY(getrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, aux, panel_ctas));
+      LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
+      if (r.n > 0) {
+        r.max_ctas = rest_ctas;
+        LM_TRY(dgemm(c, r, st));
+      }
+      LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+    } else {
+      if (r.n > 0) LM_TRY(dgemm(c, r, st));
+      LM_TRY(getrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, st));
     }
   }
   return LM_OK;
