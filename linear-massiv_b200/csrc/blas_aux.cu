@@ -117,63 +117,47 @@ __global__ void __launch_bounds__(kSwapThreads) laswp_kernel(T* A, long long lda
 // composes the swaps ipiv[k0..k1) into the list of (row, source row) pairs
 // that change (plan[0] = count, then rows, then sources, 2 * kSwapChunk
 // each), so that the column blocks need no serial prologue of their own.
-__global__ void __launch_bounds__(kSwapThreads) swap_plan_kernel(int nrows, const int* __restrict__ ipiv, int k0,
-                                                                 int k1, int* plan, int* status) {
-  __shared__ int rows[2 * kSwapChunk];
-  __shared__ int src[2 * kSwapChunk];
+// Every touched row (the swap positions k0..k1-1 and the distinct pivot rows
+// outside them) is a thread, which finds its source by walking the swap list
+// backwards: source(r) = tau_k0(tau_k0+1(... tau_k1-1(r))).
+__global__ void __launch_bounds__(2 * kSwapChunk) swap_plan_kernel(int nrows, const int* __restrict__ ipiv, int k0,
+                                                                   int k1, int* plan, int* status) {
   __shared__ int piv[kSwapChunk];
-  __shared__ int hkey[kHash];
-  __shared__ short hval[kHash];
-  __shared__ int m_sh, mm_sh;
+  __shared__ int mm_sh;
   const int tid = threadIdx.x;
   const int cnt = k1 - k0;
-  for (int i = tid; i < kHash; i += kSwapThreads) hkey[i] = -1;
-  for (int i = tid; i < cnt; i += kSwapThreads) {
-    rows[i] = k0 + i;
-    src[i] = k0 + i;
-    piv[i] = __ldg(ipiv + k0 + i);
+  if (tid < cnt) {
+    int p = __ldg(ipiv + k0 + tid);
+    if (p < 0 || p >= nrows) {  // a bad swap list: record it, treat as no swap
+      atomicCAS(status, 0, LM_DEVERR_BOUNDS);
+      p = k0 + tid;
+    }
+    piv[tid] = p;
   }
   if (tid == 0) mm_sh = 0;
   __syncthreads();
-  if (tid == 0) {
-    int m = cnt;
-    for (int q = 0; q < cnt; ++q) {
-      const int k = k0 + q;
-      const int p = piv[q];
-      if (p < 0 || p >= nrows) {
-        atomicCAS(status, 0, LM_DEVERR_BOUNDS);
-        continue;
-      }
-      if (p == k) continue;
-      int sp;
-      if (p >= k0 && p < k1) {
-        sp = p - k0;
-      } else {
-        unsigned h = ((unsigned)p * 2654435761u) & (kHash - 1);
-        while (hkey[h] != -1 && hkey[h] != p) h = (h + 1) & (kHash - 1);
-        if (hkey[h] == p) {
-          sp = hval[h];
-        } else {
-          hkey[h] = p;
-          hval[h] = (short)m;
-          rows[m] = p;
-          src[m] = p;
-          sp = m++;
-        }
-      }
-      const int t = src[q];
-      src[q] = src[sp];
-      src[sp] = t;
-    }
-    m_sh = m;
+  int r = -1;
+  if (tid < cnt) {
+    r = k0 + tid;
+  } else if (tid < 2 * cnt) {
+    const int q = tid - cnt;
+    const int p = piv[q];
+    bool first = p < k0 || p >= k1;  // swap positions are covered above
+    for (int e = 0; e < q && first; ++e) first = piv[e] != p;
+    if (first) r = p;
   }
-  __syncthreads();
-  for (int i = tid; i < m_sh; i += kSwapThreads)
-    if (src[i] != rows[i]) {
-      const int at = atomicAdd(&mm_sh, 1);
-      plan[1 + at] = rows[i];
-      plan[1 + 2 * kSwapChunk + at] = src[i];
+  if (r >= 0) {
+    int x = r;
+    for (int q = cnt - 1; q >= 0; --q) {
+      const int k = k0 + q, p = piv[q];
+      x = (x == k) ? p : ((x == p) ? k : x);
     }
+    if (x != r) {
+      const int at = atomicAdd(&mm_sh, 1);
+      plan[1 + at] = r;
+      plan[1 + 2 * kSwapChunk + at] = x;
+    }
+  }
   __syncthreads();
   if (tid == 0) plan[0] = mm_sh;
 }
@@ -411,7 +395,7 @@ int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int c
   for (int s0 = k0; s0 < k1; s0 += kSwapChunk) {
     const int s1 = std::min(k1, s0 + kSwapChunk);
     if (planned) {
-      swap_plan_kernel<<<1, kSwapThreads, 0, st>>>(nrows, ipiv, s0, s1, plan, status);
+      swap_plan_kernel<<<1, 2 * kSwapChunk, 0, st>>>(nrows, ipiv, s0, s1, plan, status);
       swap_apply_kernel<T><<<cdiv(cols, 32), kSwapThreads, smem, st>>>(A, lda, plan, ca0, ca1, cb0, cb1);
       count_launch(2);
     } else {

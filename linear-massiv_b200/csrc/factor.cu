@@ -45,14 +45,15 @@ struct TrsmScratch {
 // tensor cores, written in place: with m = w <= 128 there is one row of
 // output tiles, so each CTA reads exactly the columns of B that it later
 // overwrites, all of them before its epilogue, and no other CTA reads them.
+// With have_inv, s.Linv already holds inv(L11).
 int trsm_unit_lower_gemm(Ctx& c, const double* L11, long long lda, int w, double* B, long long ldb, int ncols,
-                         const TrsmScratch& s, cudaStream_t st) {
+                         const TrsmScratch& s, cudaStream_t st, bool have_inv = false) {
   if (w <= 0 || ncols <= 0) return LM_OK;
-  if (w <= 64 && ncols <= 128) {
+  if (w <= 64 && ncols <= 128 && !have_inv) {
     Prof p(c, kPhaseTrsm, (double)w * w * ncols, 8.0 * ((double)w * w / 2 + 2.0 * w * ncols), st);
     return trsm_lower_small<double>(L11, lda, w, true, B, ldb, ncols, st);
   }
-  {
+  if (!have_inv) {
     Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 8.0 * (double)w * w, st);
     LM_TRY(tri_inv_lower<double>(L11, lda, w, true, s.Linv, kNB, nullptr, st));
   }
@@ -135,7 +136,8 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
     const int m = n - k0 - w;
     const int wn = std::min(kNB, m);  // next panel
     double* A11 = A + (long long)k0 * lda + k0;
-    LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w, A11 + w, lda, m, s, st));
+    // with look-ahead, inv(L11) of this panel was formed beside the previous update
+    LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w, A11 + w, lda, m, s, st, la && k0 > 0));
     GemmDesc d;  // A22 -= L21 U12, the next panel's columns first
     d.m = m; d.n = wn; d.k = w;
     d.alpha = -1.0; d.beta = 1.0;
@@ -151,6 +153,12 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
       LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
       LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
       LM_TRY(getrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, aux, panel_ctas));
+      if (k0 + w + wn < n) {
+        // the next step's block solve needs inv(L11) of this panel; the
+        // current step's product with the old inverse has already run
+        Prof p(c, kPhaseTrsm, (double)wn * wn * wn / 3.0, 8.0 * (double)wn * wn, aux);
+        LM_TRY(tri_inv_lower<double>(A + (long long)(k0 + w) * lda + k0 + w, lda, wn, true, s.Linv, kNB, nullptr, aux));
+      }
       LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
       if (r.n > 0) {
         r.max_ctas = rest_ctas;
