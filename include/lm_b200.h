@@ -192,6 +192,12 @@ int lm_ctx_set_ir_method(lm_ctx* ctx, int method);
 /* Method that produced the last mixed-precision result on this context
  * (LM_IR_RBT, or LM_IR_GEPP after a fallback); -1 before the first solve. */
 int lm_ctx_ir_last_method(lm_ctx* ctx, int* method);
+/* Convergence record of the context's last mixed-precision solve: the worst
+ * normwise backward error after each refinement step, over both methods in
+ * the order they ran (randomised first, then partial pivoting after a
+ * fallback).  *steps receives the number of steps; up to max_steps values are
+ * written to berr. */
+int lm_ctx_ir_history(lm_ctx* ctx, double* berr, int max_steps, int* steps);
 
 /* ---- factorisation without allocation -----------------------------------------
  * No counterpart in the reference.  lm_dpotrf without any allocation: for

@@ -52,6 +52,7 @@ struct Ctx {
   std::mutex mu;
   int ir_method = LM_IR_RBT;  // lm_ctx_set_ir_method
   int ir_last = -1;           // method of the last mixed-precision result
+  std::vector<double> ir_hist;  // worst backward error after each refinement step (ctx_ir_history)
   // batch kernel panel width per precision and size bucket (lm_batch_tune)
   int batch_nb[2][BatchLimits::kBuckets] = {{16, 16, 16, 16}, {16, 16, 16, 16}};
 };
@@ -112,6 +113,8 @@ Prof::~Prof() {
 
 int* ctx_status(Ctx& c) { return c.d_status; }
 int ctx_num_sms(Ctx& c) { return c.num_sms; }
+
+std::vector<double>& ctx_ir_history(Ctx& c) { return c.ir_hist; }
 
 int ctx_pinned(Ctx& c, size_t bytes, void** ptr) {
   if (c.pinned_bytes < bytes) {
@@ -444,6 +447,16 @@ int lm_ctx_set_ir_method(lm_ctx* ctx, int method) {
   });
 }
 
+int lm_ctx_ir_history(lm_ctx* ctx, double* berr, int max_steps, int* steps) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (!steps || max_steps < 0 || (max_steps > 0 && !berr)) return LM_ERR_ARG;
+    const int k = std::min<int>(max_steps, (int)c.ir_hist.size());
+    for (int i = 0; i < k; ++i) berr[i] = c.ir_hist[i];
+    *steps = (int)c.ir_hist.size();
+    return LM_OK;
+  });
+}
+
 int lm_ctx_ir_last_method(lm_ctx* ctx, int* method) {
   return guarded(ctx, [&](Ctx& c) {
     if (!method) return LM_ERR_ARG;
@@ -607,6 +620,7 @@ int ir_solve(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
       return lm::run_graphed(c, key, body);
     };
   };
+  c.ir_hist.clear();
   if (c.ir_method == LM_IR_RBT) {
     int r = lm::dgesv_rbt_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream, runner("rbt"));
     if (r != LM_ERR_NOT_CONVERGED) {

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cstddef>
 #include <functional>
+#include <vector>
 
 #include "lm_b200.h"
 
@@ -25,6 +26,9 @@ int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr);
 // The context's look-ahead stream (highest priority, created on first use,
 // which must not be inside a stream capture) and its fork / join events.
 int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join);
+// Worst backward error after each refinement step of the context's last
+// mixed-precision solve (both methods, in order).
+std::vector<double>& ctx_ir_history(Ctx& c);
 // Grow-only pinned host buffer owned by the context (not inside a capture).
 int ctx_pinned(Ctx& c, size_t bytes, void** ptr);
 

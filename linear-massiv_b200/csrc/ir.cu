@@ -342,6 +342,7 @@ int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, cons
       const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
       worst = std::max(worst, (be != be) ? 1e300 : be);
     }
+    ctx_ir_history(c).push_back(worst);
     if (worst <= tol) break;
     if (stall_exit && it >= 2) {
       // give up when an iteration makes no progress, or when the observed

@@ -38,7 +38,7 @@ EXPORTS = [
     "lm_dgetrf", "lm_dgetrs", "lm_dgesv", "lm_dpotrf", "lm_dpotrs", "lm_dposv",
     "lm_lu_solve_host", "lm_chol_solve_host", "lm_matmul_host", "lm_gemm_host",
     "lm_lu_host", "lm_cholesky_host", "lm_det_host", "lm_ipiv_to_perm", "lm_dresidual",
-    "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_ctx_set_ir_method", "lm_ctx_ir_last_method", "lm_dpotrf_noalloc",
+    "lm_dgesv_ir", "lm_lu_solve_ir_host", "lm_ctx_set_ir_method", "lm_ctx_ir_last_method", "lm_ctx_ir_history", "lm_dpotrf_noalloc",
     "lm_batch_create", "lm_batch_destroy", "lm_batch_offsets", "lm_batch_solve", "lm_batch_results",
     "lm_batch_factors", "lm_batch_solve_host", "lm_batch_tune", "lm_batch_tune_get", "lm_batch_tune_set",
     "lm_server_default_config", "lm_server_create", "lm_server_submit", "lm_server_test", "lm_server_wait",
@@ -92,6 +92,7 @@ def _lib():
                 "lm_ctx_profile": ([vp, i], i),
                 "lm_ctx_set_ir_method": ([vp, i], i),
                 "lm_ctx_ir_last_method": ([vp, ip], i),
+                "lm_ctx_ir_history": ([vp, dp, i, ip], i),
                 "lm_ctx_profile_read": ([vp, ctypes.POINTER(ctypes.c_longlong), dp, dp, dp], i),
                 "lm_status_string": ([i], ctypes.c_char_p),
                 "lm_last_error": ([], ctypes.c_char_p),
@@ -202,6 +203,13 @@ class Context:
     def set_ir_method(self, method: int):
         """IR_RBT (randomised, no pivoting; default) or IR_GEPP for the mixed-precision solves."""
         _check(_lib().lm_ctx_set_ir_method(self.h, int(method)), "lm_ctx_set_ir_method")
+
+    def ir_history(self) -> list:
+        """Worst backward error after each refinement step of the last mixed-precision solve."""
+        buf = (ctypes.c_double * 256)()
+        k = ctypes.c_int(0)
+        _check(_lib().lm_ctx_ir_history(self.h, buf, 256, ctypes.byref(k)), "lm_ctx_ir_history")
+        return [buf[i] for i in range(min(k.value, 256))]
 
     def ir_last_method(self) -> int:
         m = ctypes.c_int(-1)
