@@ -180,9 +180,9 @@ int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const dou
  *     transforms, Ar = U^T A V (Baboulin, Dongarra, Herrmann, Tomov 2013), and
  *     Ar is factored in FP32 without pivoting, so that everything but the
  *     128 x 128 diagonal blocks runs on the tensor cores; corrections are
- *     V Ar^-1 U^T r.  If its refinement stalls (an iteration does not reduce the
- *     worst backward error, or its contraction rate cannot reach tol within
- *     max_iter) or runs out of steps, the solve is redone with
+ *     V Ar^-1 U^T r.  If its refinement stalls (two steps in a row do not
+ *     reduce the worst backward error, or its contraction rate cannot reach
+ *     tol within max_iter) or runs out of steps, the solve is redone with
  *     LM_IR_GEPP, and only that result is reported.
  *   LM_IR_GEPP: FP32 LU with partial pivoting, as described above.
  * The stopping test, tolerance and FP64 residual are the same for both. */

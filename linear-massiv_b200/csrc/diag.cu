@@ -27,6 +27,11 @@ namespace {
 constexpr int DB = 128;       // block order handled by one CTA
 constexpr int DLD = DB + 4;   // shared-memory leading dimension (rows 16-byte aligned)
 constexpr int TLD = 64 + 4;   // scratch leading dimension
+// 1-norm condition number of a no-pivot diagonal factor beyond which the
+// block solves that use its inverse take a correction step (measured: the
+// correction helps ill-conditioned blocks and slightly hurts well-conditioned
+// ones of graded matrices, so it is applied per block)
+constexpr double kRefineCond = 1e4;
 
 __device__ __forceinline__ void group_bar(int id, int nthreads) {
   if (id == 0)
@@ -293,11 +298,10 @@ __device__ __noinline__ void lu32_warp(float* blk, int o, int w, int base, int* 
 // 512 threads; L and U^T are inverted one after the other.
 __global__ void __launch_bounds__(512, 1)
     nopiv_diag_kernel(float* A11, long long lda, int w, int base, float* Lhi, float* Llo, float* UThi, float* UTlo,
-                      long long ldi, float* DinvL, float* DinvU, int* status) {
+                      long long ldi, float* DinvL, float* DinvU, float* LFhi, float* LFlo, float* UFThi,
+                      float* UFTlo, int* status) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  float* S = reinterpret_cast<float*>(dsm);   // L \ U, then inv(L)
-  float* S2 = S + DB * DLD;                    // U^T, then inv(U^T)
-  float* tmp = S2 + DB * DLD;                  // 64 x TLD
+  float* S = reinterpret_cast<float*>(dsm);   // L \ U
   const int t = threadIdx.x;
 #pragma unroll 8
   for (int e = t; e < DB * DB; e += 512) {
@@ -336,34 +340,98 @@ __global__ void __launch_bounds__(512, 1)
     const int i = e / w, j = e % w;
     A11[(long long)i * lda + j] = S[i * DLD + j];
   }
-  // S2 = U^T (lower, with U's diagonal); then S keeps only L (zero upper)
-  for (int e = t; e < DB * DB; e += 512) {
-    const int i = e / DB, j = e % DB;
-    S2[i * DLD + j] = (j <= i) ? S[j * DLD + i] : 0.f;
+  // split factors themselves (unit L, U^T) for the refinement of the block solves
+  for (int e = t; e < w * w; e += 512) {
+    const int i = e / w, j = e % w;
+    const float lf = (j < i) ? S[i * DLD + j] : (i == j ? 1.f : 0.f);
+    const float uf = (j <= i) ? S[j * DLD + i] : 0.f;
+    const float lh = tf32_hi_part(lf), uh = tf32_hi_part(uf);
+    LFhi[(long long)i * ldi + j] = lh;
+    LFlo[(long long)i * ldi + j] = lf - lh;
+    UFThi[(long long)i * ldi + j] = uh;
+    UFTlo[(long long)i * ldi + j] = uf - uh;
   }
-  __syncthreads();
-  for (int e = t; e < DB * DB; e += 512) {
-    const int i = e / DB, j = e % DB;
-    if (j > i) S[i * DLD + j] = 0.f;
-  }
-  __syncthreads();
-  inv_lower_smem<float>(S, tmp, true, false, t, 0);
-  inv_lower_smem<float>(S2, tmp, false, false, t, 0);
-  __syncthreads();
-  for (int e = t; e < DB * DB; e += 512) {
-    const int i = e / DB, j = e % DB;
-    const float li = (j <= i) ? S[i * DLD + j] : 0.f;    // inv(L)(i, j)
-    const float ut = (j <= i) ? S2[i * DLD + j] : 0.f;   // inv(U)^T(i, j) = inv(U)(j, i)
-    const float ui = (i <= j) ? S2[j * DLD + i] : 0.f;   // inv(U)(i, j)
-    DinvL[e] = li;
-    DinvU[e] = ui;
-    if (i < w && j < w) {
-      const float lh = tf32_hi_part(li), uh = tf32_hi_part(ut);
-      Lhi[(long long)i * ldi + j] = lh;
-      Llo[(long long)i * ldi + j] = li - lh;
-      UThi[(long long)i * ldi + j] = uh;
-      UTlo[(long long)i * ldi + j] = ut - uh;
+}
+
+// inv(L11) and inv(U11) of the FP32 factor just written to A11, computed in
+// FP64 (one after the other in the same shared memory) and rounded once:
+// without pivoting the diagonal blocks can be ill-conditioned, and an inverse
+// formed in FP32 would be too inaccurate for the correction steps of the
+// block solves and substitutions that use it.  Outputs as nopiv_diag.
+__global__ void __launch_bounds__(512, 1)
+    nopiv_inv_kernel(const float* __restrict__ A11, long long lda, int w, float* Lhi, float* Llo, float* UThi,
+                     float* UTlo, long long ldi, float* DinvL, float* DinvU, int* refine) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  double* S = reinterpret_cast<double*>(dsm);
+  double* tmp = S + DB * DLD;
+  __shared__ double colsum[DB];
+  __shared__ double norm_f;
+  const int t = threadIdx.x;
+  // 1-norm (largest column sum) of the lower triangle held in S
+  auto norm1 = [&]() {
+    if (t < DB) {
+      double sum = 0.0;
+      for (int i = t; i < DB; ++i) sum += fabs(S[i * DLD + t]);
+      colsum[t] = sum;
     }
+    __syncthreads();
+    if (t < 32) {
+      double m = 0.0;
+      for (int j = t; j < DB; j += 32) m = fmax(m, colsum[j]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+      if (t == 0) colsum[0] = m;
+    }
+    __syncthreads();
+    const double r = colsum[0];
+    __syncthreads();
+    return r;
+  };
+  for (int pass = 0; pass < 2; ++pass) {
+    // pass 0: unit-lower L; pass 1: U^T (lower, U's diagonal)
+#pragma unroll 8
+    for (int e = t; e < DB * DB; e += 512) {
+      const int i = e / DB, j = e % DB;
+      double v = 0.0;
+      if (i < w && j < w) {
+        if (pass == 0)
+          v = (j < i) ? (double)A11[(long long)i * lda + j] : (i == j ? 1.0 : 0.0);
+        else
+          v = (j <= i) ? (double)A11[(long long)j * lda + i] : 0.0;
+      } else if (i == j) {
+        v = 1.0;
+      }
+      S[i * DLD + j] = v;
+    }
+    __syncthreads();
+    const double nf = norm1();
+    if (t == 0) norm_f = nf;
+    inv_lower_smem<double>(S, tmp, pass == 0, false, t, 0);
+    __syncthreads();
+    const double ni = norm1();
+    // refine[0]: the products with inv(L) (U_a), refine[1]: with inv(U) (L_a)
+    if (t == 0) refine[pass] = (norm_f * ni > kRefineCond || !(norm_f * ni == norm_f * ni)) ? 1 : 0;
+    for (int e = t; e < DB * DB; e += 512) {
+      const int i = e / DB, j = e % DB;
+      if (pass == 0) {
+        const float li = (j <= i) ? (float)S[i * DLD + j] : 0.f;  // inv(L)(i, j)
+        DinvL[e] = li;
+        if (i < w && j < w) {
+          const float lh = tf32_hi_part(li);
+          Lhi[(long long)i * ldi + j] = lh;
+          Llo[(long long)i * ldi + j] = li - lh;
+        }
+      } else {
+        const float ut = (j <= i) ? (float)S[i * DLD + j] : 0.f;  // inv(U)^T(i, j)
+        DinvU[e] = (i <= j) ? (float)S[j * DLD + i] : 0.f;        // inv(U)(i, j)
+        if (i < w && j < w) {
+          const float uh = tf32_hi_part(ut);
+          UThi[(long long)i * ldi + j] = uh;
+          UTlo[(long long)i * ldi + j] = ut - uh;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -371,7 +439,7 @@ template <typename T>
 constexpr size_t inv_smem_bytes() {
   return sizeof(T) * ((size_t)DB * DLD + (size_t)64 * TLD);
 }
-constexpr size_t nopiv_smem_bytes() { return sizeof(float) * (2 * (size_t)DB * DLD + (size_t)64 * TLD); }
+constexpr size_t nopiv_smem_bytes() { return sizeof(float) * (size_t)DB * DLD; }
 
 }  // namespace
 
@@ -414,7 +482,8 @@ int trsm_lower_small(const T* L, long long ldl, int w, bool unit, T* B, long lon
 }
 
 int nopiv_diag(float* A11, long long lda, int w, int base, float* Lhi, float* Llo, float* UThi, float* UTlo,
-               long long ldi, float* DinvL, float* DinvU, int* status, cudaStream_t st) {
+               long long ldi, float* DinvL, float* DinvU, float* LFhi, float* LFlo, float* UFThi, float* UFTlo,
+               int* refine, int* status, cudaStream_t st) {
   if (w <= 0) return LM_OK;
   if (w > DB) return LM_ERR_ARG;
   static bool attr_set[kMaxDevices] = {};
@@ -423,11 +492,15 @@ int nopiv_diag(float* A11, long long lda, int w, int base, float* Lhi, float* Ll
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(nopiv_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)nopiv_smem_bytes()));
+    LM_CUDA_TRY(cudaFuncSetAttribute(nopiv_inv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)inv_smem_bytes<double>()));
     attr_set[dev] = true;
   }
   nopiv_diag_kernel<<<1, 512, nopiv_smem_bytes(), st>>>(A11, lda, w, base, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
-                                                         status);
-  count_launch(1);
+                                                         LFhi, LFlo, UFThi, UFTlo, status);
+  nopiv_inv_kernel<<<1, 512, inv_smem_bytes<double>(), st>>>(A11, lda, w, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
+                                                             refine);
+  count_launch(2);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;
 }

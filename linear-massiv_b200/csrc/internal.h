@@ -123,11 +123,16 @@ int trsm_lower_small(const T* L, long long ldl, int w, bool unit, T* B, long lon
 
 // LU without pivoting of the w x w (w <= 128) FP32 block A11 in place, with
 // split(inv(L11)) into Lhi/Llo and split(inv(U11)^T) into UThi/UTlo (w x w,
-// ld ldi), and inv(L11) / inv(U11) as 128 x 128 identity-padded blocks into
-// DinvL / DinvU; the first zero or NaN pivot is recorded as base + k + 1 in
-// status[1] (diag.cu).
+// ld ldi), inv(L11) / inv(U11) as 128 x 128 identity-padded blocks into
+// DinvL / DinvU, and split(L11) (unit diagonal) / split(U11^T) into
+// LFhi/LFlo / UFThi/UFTlo (w x w, ld ldi); the first zero or NaN pivot is
+// recorded as base + k + 1 in status[1] (diag.cu).  The inverses are formed
+// in FP64; refine[0] / refine[1] are set to 1 when L11 / U11 is
+// ill-conditioned enough for the products with its inverse to need a
+// correction step.
 int nopiv_diag(float* A11, long long lda, int w, int base, float* Lhi, float* Llo, float* UThi, float* UTlo,
-               long long ldi, float* DinvL, float* DinvU, int* status, cudaStream_t st);
+               long long ldi, float* DinvL, float* DinvU, float* LFhi, float* LFlo, float* UFThi, float* UFTlo,
+               int* refine, int* status, cudaStream_t st);
 
 // 2D copy (rows x cols) between strided buffers on the device.
 template <typename T>

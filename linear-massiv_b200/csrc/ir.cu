@@ -25,10 +25,11 @@ namespace lm {
 
 void count_launch(int n);
 // C = alpha A Bt^T + beta C on tcgen05 (sgemm_tc.cu); max_ctas caps the
-// persistent grid (0 = one CTA per SM).
+// persistent grid (0 = one CTA per SM); with gate set the launch does
+// nothing when *gate == 0 (a device-side switch inside captured sequences).
 int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
                long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
-               const float* Btlo, int max_ctas = 0);
+               const float* Btlo, int max_ctas = 0, const int* gate = nullptr);
 
 
 namespace {
@@ -49,13 +50,23 @@ __device__ __forceinline__ float tf32_hi(float a) { return __uint_as_float(__flo
 // Split for 3xTF32: hi = a with the 13 low mantissa bits cleared (exactly
 // representable in TF32), lo = a - hi (exact in FP32).
 // dst_hi/dst_lo (cols x rows) = split(src (rows x cols))^T.
+// With `gate` given and *gate == 0 nothing is written (a correction step
+// switched off on the device, inside a captured sequence, whose consumers are
+// gated by the same flag).  With `cpy` given, src is also copied unchanged to
+// cpy (rows x cols, ldc).
 __global__ void transpose_split_kernel(float* dhi, float* dlo, long long ldd, const float* src, long long lds,
-                                       int rows, int cols) {
+                                       int rows, int cols, const int* gate = nullptr, float* cpy = nullptr,
+                                       long long ldc = 0) {
+  if (gate != nullptr && *gate == 0) return;
   __shared__ float tile[32][33];
   const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int r = by + j, c = bx + threadIdx.x;
-    if (r < rows && c < cols) tile[j][threadIdx.x] = src[(long long)r * lds + c];
+    if (r < rows && c < cols) {
+      const float a = src[(long long)r * lds + c];
+      tile[j][threadIdx.x] = a;
+      if (cpy != nullptr) cpy[(long long)r * ldc + c] = a;
+    }
   }
   __syncthreads();
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
@@ -70,13 +81,16 @@ __global__ void transpose_split_kernel(float* dhi, float* dlo, long long ldd, co
 }
 
 // dst_hi/dst_lo (rows x cols, ldd) = split(src (rows x cols, lds)).
+// `gate` and `cpy` as for transpose_split_kernel.
 __global__ void split_kernel(float* dhi, float* dlo, long long ldd, const float* src, long long lds, int rows,
-                             int cols) {
+                             int cols, const int* gate = nullptr, float* cpy = nullptr, long long ldc = 0) {
+  if (gate != nullptr && *gate == 0) return;
   const long long total = (long long)rows * cols;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     const int r = (int)(i / cols), c = (int)(i % cols);
     const float a = src[(long long)r * lds + c];
+    if (cpy != nullptr) cpy[(long long)r * ldc + c] = a;
     const float h = tf32_hi(a);
     dhi[(long long)r * ldd + c] = h;
     dlo[(long long)r * ldd + c] = a - h;
@@ -295,10 +309,10 @@ namespace {
 // FP64), D (np x ldr FP32, np >= n) and nrm (2 + 3 * 64 words, nrm[0] and
 // nrm[1..] already hold ||A||_inf and ||B_c||_inf) are device scratch.
 // `correct(D, s)` turns D = fl32(r) (rows n..np-1 zero) into the correction.
-// With stall_exit the loop gives up as soon as an iteration fails to reduce
-// the worst backward error, or the observed contraction rate could not reach
-// tol within max_iter, so that a poor factor hands over to the next method
-// early.
+// With stall_exit the loop gives up after two steps in a row that fail to
+// reduce the worst backward error, or when the observed contraction rate
+// could not reach tol within max_iter, so that a poor factor hands over to
+// the next method early.
 int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
            long long ldx, double tol, int max_iter, bool stall_exit, double* R, long long ldr, float* D,
            unsigned long long* nrm, int* iters_out, double* berr_out, cudaStream_t st, const IrRunner& run,
@@ -311,6 +325,7 @@ int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, cons
   LM_TRY(ctx_pinned(c, sizeof(unsigned long long) * hwords, reinterpret_cast<void**>(&h)));
   int it = 0;
   double worst = 0.0, prev = 1e300;
+  int flat = 0;  // consecutive steps without progress
   for (it = 1; it <= max_iter; ++it) {
     // one correction step as a fixed launch sequence (captured and replayed
     // by the runner), ending with the norms copied to the host
@@ -345,11 +360,12 @@ int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, cons
     ctx_ir_history(c).push_back(worst);
     if (worst <= tol) break;
     if (stall_exit && it >= 2) {
-      // give up when an iteration makes no progress, or when the observed
-      // contraction cannot reach tol within max_iter
+      // give up after two steps in a row without progress, or when the
+      // observed contraction cannot reach tol within max_iter
       const double rate = worst / prev;
-      if (!(rate < 1.0)) break;
-      if (rate > 0.5 && it + std::log(tol / worst) / std::log(rate) > max_iter) break;
+      flat = rate < 1.0 ? 0 : flat + 1;
+      if (flat >= 2 || !(worst == worst)) break;
+      if (rate < 1.0 && rate > 0.5 && it + std::log(tol / worst) / std::log(rate) > max_iter) break;
     }
     prev = worst;
   }
@@ -428,7 +444,13 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 // halves the HBM traffic that bounds it.  Everything but the 128 x 128
 // diagonal blocks runs on the tensor cores (3xTF32):
 //   a: diagonal block (nopiv_diag: LU and both inverses in one CTA);
-//      L_a = A[below a, a] inv(U_aa),  U_a = inv(L_aa) A[a, right of a];
+//      L_a = A[below a, a] inv(U_aa),  U_a = inv(L_aa) A[a, right of a],
+//      each with one correction step (X += (B - X U) inv(U)) when the
+//      diagonal factor's 1-norm condition number exceeds kRefineCond: without
+//      pivoting a few diagonal blocks are ill-conditioned, and a plain product
+//      with their explicit inverse loses accuracy by that condition (the
+//      diagonal kernel sets the per-block flags; a switched-off correction
+//      adds zero);
 //      block b's column and row panels -= L_a U_a (k = 128);
 //   b: diagonal block, L_b and U_b likewise;
 //   A22 -= [L_a L_b] [U_a; U_b]  (k = 256).
@@ -443,18 +465,28 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
   const size_t blk = (size_t)kNB * kNB;
   const long long ldk = SW;     // K-major operands of the k = 256 update
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * SW + 2 * (size_t)n * kNB + 8 * blk), &ws));
+  const long long ldr = (n + 3) / 4 * 4;  // rows of the transposed residual
+  const int nblk = (n + kNB - 1) / kNB;
+  LM_TRY(ctx_workspace(c, 1,
+                       sizeof(float) * (4 * (size_t)n * SW + 5 * (size_t)n * kNB + 16 * blk + 2 * (size_t)kNB * ldr) +
+                           sizeof(int) * (2 * (size_t)nblk + 4),
+                       &ws));
   float* Ahi = static_cast<float*>(ws);  // [L_a | L_b] split, n x 256 (row i <-> row k0 + wa + i)
   float* Alo = Ahi + (size_t)n * SW;
   float* Bhi = Alo + (size_t)n * SW;     // [U_a | U_b]^T split, n x 256 (row j <-> column k0 + wa + j)
   float* Blo = Bhi + (size_t)n * SW;
   float* Thi = Blo + (size_t)n * SW;     // operands of the inverse products, n x 128
   float* Tlo = Thi + (size_t)n * kNB;
-  // two sets of diagonal-block operands (split inverses): the look-ahead
-  // factors the next block while this one's are still being read
-  float* inv[2][4];
+  float* Xhi = Tlo + (size_t)n * kNB;    // split first products, n x 128
+  float* Xlo = Xhi + (size_t)n * kNB;
+  float* Rb = Xlo + (size_t)n * kNB;     // residual of L_a (n x 128)
+  // two sets of diagonal-block operands (split inverses, then split factors):
+  // the look-ahead factors the next block while this one's are still read
+  float* inv[2][8];
   for (int q2 = 0; q2 < 2; ++q2)
-    for (int q = 0; q < 4; ++q) inv[q2][q] = Tlo + (size_t)n * kNB + (size_t)(4 * q2 + q) * blk;
+    for (int q = 0; q < 8; ++q) inv[q2][q] = Rb + (size_t)n * kNB + (size_t)(8 * q2 + q) * blk;
+  float* Rt = inv[1][7] + blk;           // residual of U_a (128 x ldr)
+  int* rflag = reinterpret_cast<int*>(Rt + 2 * (size_t)kNB * ldr);  // [2 * block]: refine U_a, L_a
   cudaStream_t aux;
   cudaEvent_t ev_fork, ev_join;
   LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
@@ -464,17 +496,21 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
     float** d = inv[(k0 / kNB) & 1];
     Prof p(c, kPhasePanel, 2.0 / 3.0 * w * w * w, 8.0 * w * w, ds);
     return nopiv_diag(A + (long long)k0 * lda + k0, lda, w, k0, d[0], d[1], d[2], d[3], kNB,
-                      DinvL + (size_t)(k0 / kNB) * blk, DinvU + (size_t)(k0 / kNB) * blk, ctx_status(c), ds);
+                      DinvL + (size_t)(k0 / kNB) * blk, DinvU + (size_t)(k0 / kNB) * blk, d[4], d[5], d[6], d[7],
+                      rflag + 2 * (k0 / kNB), ctx_status(c), ds);
   };
-  auto split_rows = [&](float* hi, float* lo, long long ldd, const float* src, int rows, int cols, cudaStream_t ss) {
-    split_kernel<<<grid_of((long long)rows * cols), 256, 0, ss>>>(hi, lo, ldd, src, lda, rows, cols);
+  auto split_rows = [&](float* hi, float* lo, long long ldd, const float* src, int rows, int cols, cudaStream_t ss,
+                        long long lds = 0, const int* gate = nullptr, float* cpy = nullptr, long long ldc = 0) {
+    split_kernel<<<grid_of((long long)rows * cols), 256, 0, ss>>>(hi, lo, ldd, src, lds ? lds : lda, rows, cols,
+                                                                  gate, cpy, ldc);
     count_launch(1);
     LM_CUDA_TRY(cudaGetLastError());
     return LM_OK;
   };
-  auto split_cols = [&](float* hi, float* lo, long long ldd, const float* src, int rows, int cols, cudaStream_t ss) {
+  auto split_cols = [&](float* hi, float* lo, long long ldd, const float* src, int rows, int cols, cudaStream_t ss,
+                        long long lds = 0, const int* gate = nullptr, float* cpy = nullptr, long long ldc = 0) {
     dim3 tb(32, 8), tg(cdiv(cols, 32), cdiv(rows, 32));
-    transpose_split_kernel<<<tg, tb, 0, ss>>>(hi, lo, ldd, src, lda, rows, cols);
+    transpose_split_kernel<<<tg, tb, 0, ss>>>(hi, lo, ldd, src, lds ? lds : lda, rows, cols, gate, cpy, ldc);
     count_launch(1);
     LM_CUDA_TRY(cudaGetLastError());
     return LM_OK;
@@ -487,16 +523,31 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
     float* A11 = A + (long long)k0 * lda + k0;
     float* A21 = A11 + (long long)w * lda;
     float* A12 = A11 + w;
+    // L = B inv(U): X0 = B inv(U), R = B - X0 U, X = X0 + R inv(U); the
+    // correction (all launches after the first product) runs only when the
+    // diagonal kernel flagged U11 as ill-conditioned (gl), and likewise for
+    // U with L11 (gu)
+    const int* gu = rflag + 2 * (k0 / kNB);
+    const int* gl = gu + 1;
     {
       Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 8.0 * m * w, st);
-      LM_TRY(split_rows(Thi, Tlo, kNB, A21, m, w, st));
+      LM_TRY(split_rows(Thi, Tlo, kNB, A21, m, w, st, 0, nullptr, Rb, kNB));
     }
     LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, Thi, kNB, d[2], kNB, 0.0f, A21, lda, st, Tlo, d[3]));
+    LM_TRY(split_rows(Xhi, Xlo, kNB, A21, m, w, st, 0, gl));
+    LM_TRY(sgemm_tf32(c, m, w, w, -1.0f, Xhi, kNB, d[6], kNB, 1.0f, Rb, kNB, st, Xlo, d[7], 0, gl));
+    LM_TRY(split_rows(Thi, Tlo, kNB, Rb, m, w, st, kNB, gl));
+    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, Thi, kNB, d[2], kNB, 1.0f, A21, lda, st, Tlo, d[3], 0, gl));
+    // U = inv(L) B likewise, with B^T as the K-major operand
     {
       Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 8.0 * m * w, st);
-      LM_TRY(split_cols(Thi, Tlo, kNB, A12, w, m, st));
+      LM_TRY(split_cols(Thi, Tlo, kNB, A12, w, m, st, 0, nullptr, Rt, ldr));
     }
     LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, Thi, kNB, 0.0f, A12, lda, st, d[1], Tlo));
+    LM_TRY(split_cols(Xhi, Xlo, kNB, A12, w, m, st, 0, gu));
+    LM_TRY(sgemm_tf32(c, w, m, w, -1.0f, d[4], kNB, Xhi, kNB, 1.0f, Rt, ldr, st, d[5], Xlo, 0, gu));
+    LM_TRY(split_cols(Thi, Tlo, kNB, Rt, w, m, st, ldr, gu));
+    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, Thi, kNB, 1.0f, A12, lda, st, d[1], Tlo, 0, gu));
     LM_TRY(split_rows(ahi, alo, ldk, A21, m, w, st));
     return split_cols(bhi, blo, ldk, A12, w, m, st);
   };

@@ -45,6 +45,7 @@ struct SgemmArgs {
   float alpha, beta;
   int tiles_m, tiles_n, num_tiles;
   int* status;
+  const int* gate;  // when set and *gate == 0 the launch does nothing
 };
 
 // ---- tcgen05 / bulk-copy wrappers -------------------------------------------
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(T_THREADS, 1)
   uint64_t* c_full = acc_empty + 2;       // [1]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(c_full + 1);
 
+  if (g.gate != nullptr && *g.gate == 0) return;  // uniform over the grid, before any barrier or TMEM
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int KT = (g.k + TBK - 1) / TBK;
   const bool use_beta = g.beta != 0.0f;
@@ -295,7 +297,7 @@ void count_launch(int n);
 
 int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
                long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
-               const float* Btlo, int max_ctas) {
+               const float* Btlo, int max_ctas, const int* gate) {
   if (m <= 0 || n <= 0) return LM_OK;
   if (k <= 0) return LM_ERR_ARG;
   const bool split = Alo != nullptr && Btlo != nullptr;
@@ -333,6 +335,7 @@ int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long 
   g.tiles_n = cdiv(n, TBN);
   g.num_tiles = g.tiles_m * g.tiles_n;
   g.status = ctx_status(ctx);
+  g.gate = gate;
   const int grid = std::min(g.num_tiles, max_ctas > 0 ? std::min(max_ctas, ctx_num_sms(ctx)) : ctx_num_sms(ctx));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);

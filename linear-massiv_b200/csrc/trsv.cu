@@ -299,25 +299,67 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
         }
     }
   } else {
-    // x_b = inv(T_bb) y
+    // x_b = inv(T_bb) y, then one correction x_b += inv(T_bb) (y - T_bb x_b):
+    // the diagonal blocks of a factor without pivoting can be ill-conditioned,
+    // and a product with the explicit inverse alone loses accuracy by their
+    // condition number
+    auto inv_times_ys = [&](T (&out)[MAX_RHS]) {
 #pragma unroll
-    for (int h = 0; h < MAX_RHS; ++h) acc[h] = T(0);
+      for (int h = 0; h < MAX_RHS; ++h) out[h] = T(0);
+#pragma unroll
+      for (int e = 0; e < CP; ++e) {
+        const int cc = col_of(e);
+#pragma unroll
+        for (int h = 0; h < MAX_RHS; ++h)
+          if (h < nrhs) out[h] = fma(dv[e], ys[cc][h], out[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h) {
+        out[h] += __shfl_xor_sync(0xffffffffu, out[h], 1);
+        out[h] += __shfl_xor_sync(0xffffffffu, out[h], 2);
+      }
+    };
+    inv_times_ys(acc);
+    // this thread's share of row r of T_bb (unit diagonal forward, identity padding)
+    T tb[CP];
+    load_row_share<T>(tb, LU + (long long)(r0 + (row_ok ? r : 0)) * lda, r0, q, n, row_ok, vec_ok != 0);
+#pragma unroll
+    for (int e = 0; e < CP; ++e) {
+      const int cc = col_of(e);
+      const bool keep = row_ok && cc < rows && (forward ? cc < r : cc >= r);
+      tb[e] = keep ? tb[e] : ((cc == r && (forward || !row_ok || cc >= rows)) ? T(1) : T(0));
+    }
+    T(*xb)[XS] = xj[0];
+    if (q == 0)
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h) xb[r][h] = acc[h];
+    __syncthreads();
+    T rr[MAX_RHS];
+#pragma unroll
+    for (int h = 0; h < MAX_RHS; ++h) rr[h] = T(0);
 #pragma unroll
     for (int e = 0; e < CP; ++e) {
       const int cc = col_of(e);
 #pragma unroll
       for (int h = 0; h < MAX_RHS; ++h)
-        if (h < nrhs) acc[h] = fma(dv[e], ys[cc][h], acc[h]);
+        if (h < nrhs) rr[h] = fma(tb[e], xb[cc][h], rr[h]);
     }
 #pragma unroll
     for (int h = 0; h < MAX_RHS; ++h) {
-      acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 1);
-      acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 2);
+      rr[h] += __shfl_xor_sync(0xffffffffu, rr[h], 1);
+      rr[h] += __shfl_xor_sync(0xffffffffu, rr[h], 2);
     }
+    __syncthreads();  // every thread has read ys for the first product
+    if (q == 0)
+#pragma unroll
+      for (int h = 0; h < MAX_RHS; ++h) ys[r][h] = row_ok ? ys[r][h] - rr[h] : T(0);
+    __syncthreads();
+    T dx[MAX_RHS];
+    inv_times_ys(dx);
     if (q == 0 && row_ok)
 #pragma unroll
       for (int h = 0; h < MAX_RHS; ++h)
-        if (h < nrhs) X[(long long)(r0 + r) * ldx + h] = acc[h];
+        if (h < nrhs) X[(long long)(r0 + r) * ldx + h] = acc[h] + dx[h];
   }
   __syncthreads();
   if (threadIdx.x == 0) {
