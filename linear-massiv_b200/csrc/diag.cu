@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(512, 1)
 }
 
 // inv(L11) and inv(U11) of the FP32 factor just written to A11, computed in
-// FP64 (one after the other in the same shared memory) and rounded once:
+// FP64 (one CTA per triangle, so the two run side by side) and rounded once:
 // without pivoting the diagonal blocks can be ill-conditioned, and an inverse
 // formed in FP32 would be too inaccurate for the correction steps of the
 // block solves and substitutions that use it.  Outputs as nopiv_diag.
@@ -387,8 +387,9 @@ __global__ void __launch_bounds__(512, 1)
     __syncthreads();
     return r;
   };
-  for (int pass = 0; pass < 2; ++pass) {
-    // pass 0: unit-lower L; pass 1: U^T (lower, U's diagonal)
+  {
+    // CTA 0: unit-lower L; CTA 1: U^T (lower, U's diagonal)
+    const int pass = blockIdx.x;
 #pragma unroll 8
     for (int e = t; e < DB * DB; e += 512) {
       const int i = e / DB, j = e % DB;
@@ -498,7 +499,7 @@ int nopiv_diag(float* A11, long long lda, int w, int base, float* Lhi, float* Ll
   }
   nopiv_diag_kernel<<<1, 512, nopiv_smem_bytes(), st>>>(A11, lda, w, base, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
                                                          LFhi, LFlo, UFThi, UFTlo, status);
-  nopiv_inv_kernel<<<1, 512, inv_smem_bytes<double>(), st>>>(A11, lda, w, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
+  nopiv_inv_kernel<<<2, 512, inv_smem_bytes<double>(), st>>>(A11, lda, w, Lhi, Llo, UThi, UTlo, ldi, DinvL, DinvU,
                                                              refine);
   count_launch(2);
   LM_CUDA_TRY(cudaGetLastError());

@@ -61,10 +61,11 @@ template <typename T>
 int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaStream_t st);
 // X (n x nrhs) <- U^-1 L^-1 X, two persistent launches per pass (FP64:
 // nrhs <= 4; FP32: any nrhs, in passes of 16 beyond 4); `sync` is 4 ints of
-// device scratch.
+// device scratch.  FP32: corr (two flags per 128-row block: L, U), when
+// given, limits the diagonal-block correction step to flagged blocks.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-            int* sync, int* status, cudaStream_t st);
+            int* sync, int* status, cudaStream_t st, const int* corr = nullptr);
 
 // --- FP64 GEMM (dgemm.cu) ----------------------------------------------------
 // C = alpha * op(A) * op(B) + beta * C, row-major.
@@ -188,7 +189,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
                  long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
                  const IrRunner& run);
-int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, cudaStream_t st);
+int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, int* rflag, cudaStream_t st);
 // Depth-2 recursive butterflies (rbt.cu); np is a multiple of 4.
 int rbt_diagonals(double* du, double* dv, int np, cudaStream_t st);
 int rbt_transform(float* Ar, long long ldr, const double* A, long long lda, int n, int np, const double* du,

@@ -443,7 +443,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 // is one k = 256 GEMM: it reads and writes A22 once per 256 columns, which
 // halves the HBM traffic that bounds it.  Everything but the 128 x 128
 // diagonal blocks runs on the tensor cores (3xTF32):
-//   a: diagonal block (nopiv_diag: LU and both inverses in one CTA);
+//   a: diagonal block (nopiv_diag: LU in one CTA, then the FP64 inverses);
 //      L_a = A[below a, a] inv(U_aa),  U_a = inv(L_aa) A[a, right of a],
 //      each with one correction step (X += (B - X U) inv(U)) when the
 //      diagonal factor's 1-norm condition number exceeds kRefineCond: without
@@ -455,21 +455,21 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 //   b: diagonal block, L_b and U_b likewise;
 //   A22 -= [L_a L_b] [U_a; U_b]  (k = 256).
 // Look-ahead: each diagonal block is factored on the priority stream, on the
-// SM that the concurrent GEMMs leave free (147 of 148 CTAs): block b beside
+// two SMs that the concurrent GEMMs leave free (146 of 148 CTAs; the LU takes
+// one, the two triangle inversions one each): block b beside
 // the rest of its panels' update, the next super-step's block a beside the
 // trailing update.  DinvL / DinvU receive the diagonal-block inverses in the
-// layout of the persistent substitutions.  A zero pivot is recorded in
-// status[1].
-int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, cudaStream_t st) {
+// layout of the persistent substitutions, rflag (2 ints per 128-column block:
+// L, U) the ill-conditioning flags that the substitutions' correction step
+// follows too.  A zero pivot is recorded in status[1].
+int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, int* rflag, cudaStream_t st) {
   constexpr int SW = 2 * kNB;  // super-step width
   const size_t blk = (size_t)kNB * kNB;
   const long long ldk = SW;     // K-major operands of the k = 256 update
   void* ws = nullptr;
   const long long ldr = (n + 3) / 4 * 4;  // rows of the transposed residual
-  const int nblk = (n + kNB - 1) / kNB;
   LM_TRY(ctx_workspace(c, 1,
-                       sizeof(float) * (4 * (size_t)n * SW + 5 * (size_t)n * kNB + 16 * blk + 2 * (size_t)kNB * ldr) +
-                           sizeof(int) * (2 * (size_t)nblk + 4),
+                       sizeof(float) * (4 * (size_t)n * SW + 5 * (size_t)n * kNB + 16 * blk + 2 * (size_t)kNB * ldr),
                        &ws));
   float* Ahi = static_cast<float*>(ws);  // [L_a | L_b] split, n x 256 (row i <-> row k0 + wa + i)
   float* Alo = Ahi + (size_t)n * SW;
@@ -486,7 +486,6 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
   for (int q2 = 0; q2 < 2; ++q2)
     for (int q = 0; q < 8; ++q) inv[q2][q] = Rb + (size_t)n * kNB + (size_t)(8 * q2 + q) * blk;
   float* Rt = inv[1][7] + blk;           // residual of U_a (128 x ldr)
-  int* rflag = reinterpret_cast<int*>(Rt + 2 * (size_t)kNB * ldr);  // [2 * block]: refine U_a, L_a
   cudaStream_t aux;
   cudaEvent_t ev_fork, ev_join;
   LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
@@ -570,9 +569,9 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
     if (mb > 0) {
       // column panel of b below its diagonal block, row panel of b right of it
       LM_TRY(sgemm_tf32(c, mb, wb, wa, -1.0f, Ahi + (size_t)wb * ldk, ldk, Bhi, ldk, 1.0f, Abb + (long long)wb * lda, lda,
-                        st, Alo + (size_t)wb * ldk, Blo, nsm - 1));
+                        st, Alo + (size_t)wb * ldk, Blo, nsm - 2));
       LM_TRY(sgemm_tf32(c, wb, mb, wa, -1.0f, Ahi, ldk, Bhi + (size_t)wb * ldk, ldk, 1.0f, Abb + wb, lda, st, Alo,
-                        Blo + (size_t)wb * ldk, nsm - 1));
+                        Blo + (size_t)wb * ldk, nsm - 2));
     }
     LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
     if (mb <= 0) break;
@@ -594,9 +593,9 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
     LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
     if (mb > w2) {
       LM_TRY(sgemm_tf32(c, w2, mb - w2, kk, -1.0f, ah, ldk, bh + (size_t)w2 * ldk, ldk, 1.0f, A22 + w2, lda, st, al,
-                        bl + (size_t)w2 * ldk, nsm - 1));
+                        bl + (size_t)w2 * ldk, nsm - 2));
       LM_TRY(sgemm_tf32(c, mb - w2, mb, kk, -1.0f, ah + (size_t)w2 * ldk, ldk, bh, ldk, 1.0f, A22 + (long long)w2 * lda,
-                        lda, st, al + (size_t)w2 * ldk, bl, nsm - 1));
+                        lda, st, al + (size_t)w2 * ldk, bl, nsm - 2));
     }
     LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
   }
@@ -623,8 +622,10 @@ int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
   const size_t inv_bytes = 2 * sizeof(float) * inv_elems;
   const size_t diag_bytes = 4 * sizeof(double) * (size_t)np;
   const size_t sync_bytes = 64;
+  const size_t flag_bytes = sizeof(int) * 2 * (size_t)((np + 127) / 128);
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 0, a32_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + diag_bytes + sync_bytes, &ws));
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + diag_bytes + sync_bytes + flag_bytes,
+                       &ws));
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   p += a32_bytes;
@@ -641,18 +642,21 @@ int dgesv_rbt_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
   double* dv = du + 2 * (size_t)np;
   p += diag_bytes;
   int* tsync = reinterpret_cast<int*>(p);
+  p += sync_bytes;
+  int* rflag = reinterpret_cast<int*>(p);
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
   LM_TRY(run("factor", [&](cudaStream_t s) {
     LM_TRY(rbt_diagonals(du, dv, np, s));
     LM_TRY(rbt_transform(A32, lda32, A, lda, n, np, du, dv, s));
-    return sgetrf_nopiv(c, np, A32, lda32, DinvL, DinvU, s);
+    return sgetrf_nopiv(c, np, A32, lda32, DinvL, DinvU, rflag, s);
   }));
   return refine(c, n, np, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, true, R, ldr, D, nrm, iters_out, berr_out, st, run,
                 [&](float* Dd, cudaStream_t s) {
                   LM_TRY(rbt_rows(Dd, ldr, np, nrhs, du, true, s));
                   {
                     Prof pt(c, kPhaseTrsm, 2.0 * np * np * nrhs, 4.0 * np * np, s);
-                    LM_TRY(trsv_lu<float>(A32, lda32, np, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s));
+                    LM_TRY(trsv_lu<float>(A32, lda32, np, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s,
+                                          rflag));
                   }
                   return rbt_rows(Dd, ldr, np, nrhs, dv, false, s);
                 });

@@ -152,11 +152,13 @@ __device__ __forceinline__ void load_row_share(T* out, const T* src, int c0, int
 // One direction of the blocked substitution.  forward: L unit lower, blocks in
 // increasing order; backward: U upper, blocks in decreasing order.
 // sync[0] = progress counter, sync[1] = ticket dispenser (both zero at launch).
+// corr (FP32 only): per-block flags at stride 2; when given, the correction
+// step on the diagonal block runs only for blocks whose flag is set.
 template <typename T, int RHS>
 __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
                                                              int nrhs, int forward, const T* __restrict__ Dinv,
                                                              T* X, long long ldx, int* sync, int* status,
-                                                             int vec_ok) {
+                                                             int vec_ok, const int* corr) {
   constexpr int MAX_RHS = RHS;
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
   constexpr bool EXACT = TrsvCfg<T>::EXACT;
@@ -320,6 +322,18 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
       }
     };
     inv_times_ys(acc);
+    if (corr != nullptr && corr[2 * b] == 0) {  // uniform over the CTA
+      if (q == 0 && row_ok)
+#pragma unroll
+        for (int h = 0; h < MAX_RHS; ++h)
+          if (h < nrhs) X[(long long)(r0 + r) * ldx + h] = acc[h];
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();
+        st_release(sync, t + 1);
+      }
+      return;
+    }
     // this thread's share of row r of T_bb (unit diagonal forward, identity padding)
     T tb[CP];
     load_row_share<T>(tb, LU + (long long)(r0 + (row_ok ? r : 0)) * lda, r0, q, n, row_ok, vec_ok != 0);
@@ -395,10 +409,11 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
 // X (n x nrhs) <- U^-1 L^-1 X with the packed factor and (FP32) its block
 // inverses; FP64 ignores DinvL / DinvU and takes nrhs <= 4, FP32 takes any
 // nrhs (more than 4 in passes of 16 columns).  `sync` holds 4 ints of device
-// scratch.
+// scratch.  FP32: corr, when given, holds two flags per diagonal block (L, U);
+// only flagged blocks take the correction step, all blocks do without it.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-            int* sync, int* status, cudaStream_t st) {
+            int* sync, int* status, cudaStream_t st, const int* corr) {
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC;
   if (n <= 0 || nrhs <= 0) return LM_OK;
   if (!TrsvCfg<T>::EXACT && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
@@ -407,8 +422,9 @@ int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T
   const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
   if (nrhs <= MAX_RHS) {
     LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok);
-    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok);
+    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok, corr);
+    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok,
+                                               corr ? corr + 1 : nullptr);
     count_launch(2);
     LM_CUDA_TRY(cudaGetLastError());
     return LM_OK;
@@ -420,8 +436,10 @@ int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T
     for (int c0 = 0; c0 < nrhs; c0 += WIDE_RHS) {
       const int nc = std::min(WIDE_RHS, nrhs - c0);
       LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 1, DinvL, X + c0, ldx, sync, status, vec_ok);
-      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 0, DinvU, X + c0, ldx, sync + 2, status, vec_ok);
+      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 1, DinvL, X + c0, ldx, sync, status, vec_ok,
+                                                  corr);
+      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 0, DinvU, X + c0, ldx, sync + 2, status, vec_ok,
+                                                  corr ? corr + 1 : nullptr);
       count_launch(2);
       LM_CUDA_TRY(cudaGetLastError());
     }
@@ -434,8 +452,8 @@ template size_t trsv_inv_elems<double>(int);
 template int tri_inv_blocks<float>(const float*, long long, int, float*, float*, cudaStream_t);
 template int tri_inv_blocks<double>(const double*, long long, int, double*, double*, cudaStream_t);
 template int trsv_lu<float>(const float*, long long, int, int, const float*, const float*, float*, long long, int*,
-                            int*, cudaStream_t);
+                            int*, cudaStream_t, const int*);
 template int trsv_lu<double>(const double*, long long, int, int, const double*, const double*, double*, long long,
-                             int*, int*, cudaStream_t);
+                             int*, int*, cudaStream_t, const int*);
 
 }  // namespace lm
