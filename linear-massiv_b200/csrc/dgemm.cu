@@ -13,6 +13,10 @@
 //   warps 0..NC-1 : consumers, each a 64 x 32 warp tile of m16n8k4 DMMAs,
 //                   then a fused epilogue C = alpha*acc + beta*C (in place),
 //                   optionally restricted to the lower triangle (SYRK tiles).
+// Short-k updates with beta != 0 (the factorisations' trailing updates) stage
+// each C tile in shared memory: the producer TMA-loads it while the tile's
+// main loop runs, so the epilogue reads C on chip instead of waiting on
+// L2/HBM (at k = 128 those waits were about a third of the time).
 // No cluster multicast is used anywhere.
 #include "common.cuh"
 #include "internal.h"
@@ -55,16 +59,20 @@ __device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* tmap, int 
 // MINB CTAs share an SM: with two, one CTA's epilogue (C read-modify-write)
 // overlaps the other's DMMA main loop, which matters for the short-k
 // trailing updates of the factorisations.
-template <int BM, int BN, int MINB>
+template <int BM, int BN, int MINB, bool CSM = false>
 struct GemmCfg {
   static constexpr int NC = (BM / 64) * (BN / 32);  // consumer warps
   static constexpr int THREADS = (NC + 1) * 32;
   static constexpr int A_BYTES = BM * kBK * 8;
   static constexpr int B_BYTES = BN * kBK * 8;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
-  static constexpr int BUDGET = (200 * 1024) / MINB;
+  // C staged in smem as BN / 16 boxes of BM x 16 doubles (128-byte swizzle)
+  static constexpr int C_BYTES = CSM ? BM * BN * 8 : 0;
+  static constexpr int BUDGET = CSM ? 227 * 1024 - C_BYTES - 2048 : (200 * 1024) / MINB;
   static constexpr int STAGES = BUDGET / STAGE_BYTES > 8 ? 8 : BUDGET / STAGE_BYTES;
-  static constexpr int SMEM = STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;  // + alignment slack
+  static constexpr int SMEM = STAGES * STAGE_BYTES + C_BYTES + 2 * STAGES * 8 + 16 + 1024;  // + alignment slack
+  static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+  static_assert(STAGES >= 2, "operand ring depth");
 };
 
 __device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& tm, int& tn) {
@@ -87,19 +95,25 @@ __device__ __forceinline__ void tile_coords(const GemmArgs& g, int t, int& tm, i
   }
 }
 
-template <int BM, int BN, bool AT, bool BT, int MINB>
-__global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
+// CSM: C staged in shared memory (tmC then maps 16-double x BM boxes with the
+// 128-byte swizzle); requires beta != 0.
+template <int BM, int BN, bool AT, bool BT, int MINB, bool CSM>
+__global__ void __launch_bounds__(GemmCfg<BM, BN, MINB, CSM>::THREADS, MINB)
     dgemm_dmma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ CUtensorMap tmC, GemmArgs g) {
-  using Cfg = GemmCfg<BM, BN, MINB>;
+  using Cfg = GemmCfg<BM, BN, MINB, CSM>;
   constexpr int STAGES = Cfg::STAGES;
+  constexpr int C_BOX = BM * 16 * 8;  // bytes of one staged C box
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   unsigned char* sA = smem;
   unsigned char* sB = smem + STAGES * Cfg::A_BYTES;
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * Cfg::STAGE_BYTES);
+  unsigned char* sC = smem + STAGES * Cfg::STAGE_BYTES;  // 1024-aligned: stage sizes are multiples of 2 KB
+  uint64_t* full = reinterpret_cast<uint64_t*>(sC + Cfg::C_BYTES);
   uint64_t* empty = full + STAGES;
+  uint64_t* cfull = empty + STAGES;  // C tile landed
+  uint64_t* cempty = cfull + 1;      // every consumer warp has read it
 
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
@@ -110,6 +124,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], Cfg::NC);
     }
+    mbar_init(cfull, 1);
+    mbar_init(cempty, Cfg::NC);
     fence_barrier_init();
   }
   __syncthreads();
@@ -119,11 +135,12 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
     if (lane == 0) {
       tma_prefetch_desc(&tmA);
       tma_prefetch_desc(&tmB);
-      int it = 0;
-      for (int t = blockIdx.x; t < g.num_tiles; t += gridDim.x) {
+      if (CSM) tma_prefetch_desc(&tmC);
+      int it = 0, cj = 0;
+      for (int t = blockIdx.x; t < g.num_tiles; t += gridDim.x, ++cj) {
         int tm, tn;
         tile_coords(g, t, tm, tn);
-        if (g.prefetch_c) tma_prefetch_l2_2d(&tmC, tn * BN, tm * BM);
+        if (!CSM && g.prefetch_c) tma_prefetch_l2_2d(&tmC, tn * BN, tm * BM);
         for (int kb = 0; kb < KT; ++kb, ++it) {
           const int s = it % STAGES;
           const uint32_t ph = (uint32_t)((it / STAGES) & 1) ^ 1u;
@@ -143,6 +160,15 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
             for (int j = 0; j < BN / 16; ++j)
               tma_load_2d(sB + s * Cfg::B_BYTES + j * 2048, &tmB, tn * BN + j * 16, kb * kBK, &full[s]);
           }
+          if (CSM && kb == min(STAGES, KT) - 1) {
+            // this tile's C, once the previous tile's epilogue has read the
+            // buffer; issued after the first ring slots so that the main
+            // loop never waits on it
+            if (!mbar_wait(cempty, (uint32_t)(cj & 1) ^ 1u, g.status)) return;
+            mbar_arrive_expect_tx(cfull, Cfg::C_BYTES);
+#pragma unroll
+            for (int j = 0; j < BN / 16; ++j) tma_load_2d(sC + j * C_BOX, &tmC, tn * BN + j * 16, tm * BM, cfull);
+          }
         }
       }
     }
@@ -157,8 +183,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
   const uint32_t sA32 = smem_u32(sA);
   const uint32_t sB32 = smem_u32(sB);
 
-  int it = 0;
-  for (int t = blockIdx.x; t < g.num_tiles; t += gridDim.x) {
+  int it = 0, cj = 0;
+  for (int t = blockIdx.x; t < g.num_tiles; t += gridDim.x, ++cj) {
     int tm, tn;
     tile_coords(g, t, tm, tn);
     double acc[4][4][4];
@@ -211,49 +237,84 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB>::THREADS, MINB)
     // Per 16-row slice: issue all of its C loads first, then the FMAs and stores.
     const bool vec_ok = ((g.ldc & 1) == 0) && ((reinterpret_cast<uintptr_t>(g.C) & 15) == 0);
     const bool use_beta = g.beta != 0.0;
+    if constexpr (CSM) {
+      if (!mbar_wait(cfull, (uint32_t)(cj & 1), g.status)) return;
+      const uint32_t sC32 = smem_u32(sC);
 #pragma unroll
-    for (int mi = 0; mi < 4; ++mi) {
-      double old[2][4][2];
+      for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int row = tm * BM + wm * 64 + mi * 16 + gq + h * 8;
-        const double* crow = g.C + (long long)row * g.ldc;
+        for (int h = 0; h < 2; ++h) {
+          const int rl = wm * 64 + mi * 16 + gq + h * 8;  // row within the tile
+          const int row = tm * BM + rl;
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
-          const int col = tn * BN + wn * 32 + ni * 8 + 2 * tq;
-          old[h][ni][0] = 0.0;
-          old[h][ni][1] = 0.0;
-          if (use_beta && row < g.m) {
+          for (int ni = 0; ni < 4; ++ni) {
+            const int cl = wn * 32 + ni * 8 + 2 * tq;  // column within the tile (even)
+            double2 o;
+            asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];"
+                         : "=d"(o.x), "=d"(o.y)
+                         : "r"(sC32 + (cl >> 4) * C_BOX + swz128(rl, cl & 15)));
+            if (row >= g.m) continue;
+            const int col = tn * BN + cl;
             const bool in0 = col < g.n && (!g.lower_only || col <= row);
             const bool in1 = col + 1 < g.n && (!g.lower_only || col + 1 <= row);
+            const double r0 = fma(g.alpha, acc[mi][ni][2 * h], g.beta * o.x);
+            const double r1 = fma(g.alpha, acc[mi][ni][2 * h + 1], g.beta * o.y);
+            double* crow = g.C + (long long)row * g.ldc;
             if (in0 && in1 && vec_ok) {
-              const double2 o = *reinterpret_cast<const double2*>(crow + col);
-              old[h][ni][0] = o.x;
-              old[h][ni][1] = o.y;
+              *reinterpret_cast<double2*>(crow + col) = make_double2(r0, r1);
             } else {
-              if (in0) old[h][ni][0] = crow[col];
-              if (in1) old[h][ni][1] = crow[col + 1];
+              if (in0) crow[col] = r0;
+              if (in1) crow[col + 1] = r1;
             }
           }
         }
-      }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(cempty);
+    } else {
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int row = tm * BM + wm * 64 + mi * 16 + gq + h * 8;
-        if (row >= g.m) continue;
-        double* crow = g.C + (long long)row * g.ldc;
+      for (int mi = 0; mi < 4; ++mi) {
+        double old[2][4][2];
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
-          const int col = tn * BN + wn * 32 + ni * 8 + 2 * tq;
-          const bool in0 = col < g.n && (!g.lower_only || col <= row);
-          const bool in1 = col + 1 < g.n && (!g.lower_only || col + 1 <= row);
-          const double r0 = fma(g.alpha, acc[mi][ni][2 * h], use_beta ? g.beta * old[h][ni][0] : 0.0);
-          const double r1 = fma(g.alpha, acc[mi][ni][2 * h + 1], use_beta ? g.beta * old[h][ni][1] : 0.0);
-          if (in0 && in1 && vec_ok) {
-            *reinterpret_cast<double2*>(crow + col) = make_double2(r0, r1);
-          } else {
-            if (in0) crow[col] = r0;
-            if (in1) crow[col + 1] = r1;
+        for (int h = 0; h < 2; ++h) {
+          const int row = tm * BM + wm * 64 + mi * 16 + gq + h * 8;
+          const double* crow = g.C + (long long)row * g.ldc;
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) {
+            const int col = tn * BN + wn * 32 + ni * 8 + 2 * tq;
+            old[h][ni][0] = 0.0;
+            old[h][ni][1] = 0.0;
+            if (use_beta && row < g.m) {
+              const bool in0 = col < g.n && (!g.lower_only || col <= row);
+              const bool in1 = col + 1 < g.n && (!g.lower_only || col + 1 <= row);
+              if (in0 && in1 && vec_ok) {
+                const double2 o = *reinterpret_cast<const double2*>(crow + col);
+                old[h][ni][0] = o.x;
+                old[h][ni][1] = o.y;
+              } else {
+                if (in0) old[h][ni][0] = crow[col];
+                if (in1) old[h][ni][1] = crow[col + 1];
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int row = tm * BM + wm * 64 + mi * 16 + gq + h * 8;
+          if (row >= g.m) continue;
+          double* crow = g.C + (long long)row * g.ldc;
+#pragma unroll
+          for (int ni = 0; ni < 4; ++ni) {
+            const int col = tn * BN + wn * 32 + ni * 8 + 2 * tq;
+            const bool in0 = col < g.n && (!g.lower_only || col <= row);
+            const bool in1 = col + 1 < g.n && (!g.lower_only || col + 1 <= row);
+            const double r0 = fma(g.alpha, acc[mi][ni][2 * h], use_beta ? g.beta * old[h][ni][0] : 0.0);
+            const double r1 = fma(g.alpha, acc[mi][ni][2 * h + 1], use_beta ? g.beta * old[h][ni][1] : 0.0);
+            if (in0 && in1 && vec_ok) {
+              *reinterpret_cast<double2*>(crow + col) = make_double2(r0, r1);
+            } else {
+              if (in0) crow[col] = r0;
+              if (in1) crow[col + 1] = r1;
+            }
           }
         }
       }
@@ -272,11 +333,11 @@ __global__ void scale_kernel(double* C, long long ldc, int m, int n, double beta
   }
 }
 
-template <int BM, int BN, bool AT, bool BT, int MINB>
+template <int BM, int BN, bool AT, bool BT, int MINB, bool CSM = false>
 int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
-  using Cfg = GemmCfg<BM, BN, MINB>;
+  using Cfg = GemmCfg<BM, BN, MINB, CSM>;
   static bool attr_set[kMaxDevices] = {};  // per instantiation and device, set under the API lock
-  auto kern = dgemm_dmma_kernel<BM, BN, AT, BT, MINB>;
+  auto kern = dgemm_dmma_kernel<BM, BN, AT, BT, MINB, CSM>;
   const int dev = ctx_device(ctx);
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
@@ -297,7 +358,11 @@ int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
                         CU_TENSOR_MAP_SWIZZLE_128B));
   CUtensorMap tmC;
   const bool c_ok = d.beta != 0.0 && !(reinterpret_cast<uintptr_t>(d.C) & 15) && !(d.ldc & 1);
-  if (c_ok)
+  if (CSM && !c_ok) return LM_ERR_ARG;
+  if (CSM)
+    LM_TRY(make_tmap_2d(&tmC, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.C, d.n, d.m, d.ldc, 16, BM,
+                        CU_TENSOR_MAP_SWIZZLE_128B));
+  else if (c_ok)
     LM_TRY(make_tmap_2d(&tmC, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 8, d.C, d.n, d.m, d.ldc, BN, BM,
                         CU_TENSOR_MAP_SWIZZLE_NONE));
   else
@@ -312,7 +377,8 @@ int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
   g.tiles_n = cdiv(d.n, BN);
   g.num_tiles = d.lower_only ? g.tiles_m * (g.tiles_m + 1) / 2 : g.tiles_m * g.tiles_n;
   g.status = ctx_status(ctx);
-  int grid = std::min(g.num_tiles, d.max_ctas > 0 ? d.max_ctas : MINB * ctx_num_sms(ctx));
+  const int sms = d.max_sms > 0 ? std::min(d.max_sms, ctx_num_sms(ctx)) : ctx_num_sms(ctx);
+  int grid = std::min(g.num_tiles, MINB * sms);
   kern<<<grid, Cfg::THREADS, Cfg::SMEM, st>>>(tmA, tmB, tmC, g);
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());
@@ -339,13 +405,21 @@ int dgemm(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
       (d.lda & 1) || (d.ldb & 1))
     return LM_ERR_UNSUPPORTED;
   if (d.a_trans && d.b_trans) return LM_ERR_UNSUPPORTED;
-  // Short k (the factorisations' trailing updates): 128 x 64 tiles, two CTAs
-  // per SM.  Long k: 128 x 128 tiles, one CTA per SM, deeper pipeline.
+  // Short k with beta != 0 (the factorisations' trailing updates): 128 x 128
+  // tiles with C staged in shared memory.  Other short-k or narrow products:
+  // 128 x 64 tiles, two CTAs per SM.  Long k: 128 x 128 tiles, one CTA per
+  // SM, deeper pipeline.
   const double flops = d.lower_only ? (double)d.m * (d.m + 1) * d.k : 2.0 * d.m * d.n * d.k;
   const double bytes = 8.0 * ((double)d.m * d.k + (double)d.k * d.n +
                               (d.beta != 0.0 ? 2.0 : 1.0) * (d.lower_only ? 0.5 : 1.0) * d.m * d.n);
   Prof prof(ctx, kPhaseGemm, flops, bytes, st);
   const bool narrow = (d.n <= 64 || d.k <= 256) && !d.lower_only;
+  const bool c_tma = d.beta != 0.0 && !(reinterpret_cast<uintptr_t>(d.C) & 15) && !(d.ldc & 1);
+  if (d.k <= 256 && d.n > 64 && c_tma) {
+    if (d.a_trans) return launch_dmma<128, 128, true, false, 1, true>(ctx, d, st);
+    if (d.b_trans) return launch_dmma<128, 128, false, true, 1, true>(ctx, d, st);
+    return launch_dmma<128, 128, false, false, 1, true>(ctx, d, st);
+  }
   if (d.a_trans)
     return narrow ? launch_dmma<128, 64, true, false, 2>(ctx, d, st)
                   : launch_dmma<128, 128, true, false, 1>(ctx, d, st);

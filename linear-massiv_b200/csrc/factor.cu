@@ -66,10 +66,10 @@ int trsm_unit_lower_gemm(Ctx& c, const double* L11, long long lda, int w, double
   return dgemm(c, d, st);
 }
 
-// gemm_ctas caps the grid of the panel's own GEMMs (0 = no cap), so that a
+// gemm_sms caps the SMs of the panel's own GEMMs (0 = no cap), so that a
 // panel factored beside a trailing update fits on the SMs that update leaves.
 int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv,
-                    const TrsmScratch& s, cudaStream_t st, int gemm_ctas = 0) {
+                    const TrsmScratch& s, cudaStream_t st, int gemm_sms = 0) {
   const int R = n - c0;
   const int wmax = panel_leaf_max_width_for(c, R);
   if (wmax <= 0) return LM_ERR_UNSUPPORTED;
@@ -82,7 +82,7 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int 
   int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
   if (w1 >= w) w1 = w - 4;
   const int w2 = w - w1;
-  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st, gemm_ctas));
+  LM_TRY(getrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st, gemm_sms));
   double* A11 = A + (long long)c0 * lda + c0;
   LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w1, A11 + w1, lda, w2, s, st));
   GemmDesc d;
@@ -91,9 +91,9 @@ int getrf_panel_rec(Ctx& c, double* A, long long lda, int n, int c0, int w, int 
   d.A = A11 + (long long)w1 * lda; d.lda = lda;
   d.B = A11 + w1; d.ldb = lda;
   d.C = A11 + (long long)w1 * lda + w1; d.ldc = lda;
-  d.max_ctas = gemm_ctas;
+  d.max_sms = gemm_sms;
   LM_TRY(dgemm(c, d, st));
-  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st, gemm_ctas);
+  return getrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st, gemm_sms);
 }
 
 }  // namespace
@@ -122,8 +122,8 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   if (la) LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
-  const int panel_ctas = 2 * kLookaheadSms;
-  const int rest_ctas = 2 * (nsm - kLookaheadSms);
+  const int panel_sms = kLookaheadSms;
+  const int rest_sms = nsm - kLookaheadSms;
   LM_TRY(getrf_panel_rec(c, A, lda, n, 0, std::min(kNB, n), 0, std::min(kNB, n), ipiv, s, st));
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
@@ -152,7 +152,7 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
     if (la) {
       LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
       LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
-      LM_TRY(getrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, aux, panel_ctas));
+      LM_TRY(getrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, aux, panel_sms));
       if (k0 + w + wn < n) {
         // the next step's block solve needs inv(L11) of this panel; the
         // current step's product with the old inverse has already run
@@ -161,7 +161,7 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
       }
       LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
       if (r.n > 0) {
-        r.max_ctas = rest_ctas;
+        r.max_sms = rest_sms;
         LM_TRY(dgemm(c, r, st));
       }
       LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));

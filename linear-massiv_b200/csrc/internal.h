@@ -72,7 +72,7 @@ int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T
 //   a_trans = false: A is m x k (lda)  | true: A^T is stored, k x m (lda)
 //   b_trans = false: B is k x n (ldb)  | true: B^T is stored, n x k (ldb)
 // lower_only: only C(i,j) with j <= i is read or written (requires m == n).
-// max_ctas: cap on the persistent grid (0 = one CTA per SM).
+// max_sms: SMs the persistent grid may occupy (0 = all of them).
 struct GemmDesc {
   int m = 0, n = 0, k = 0;
   double alpha = 1.0, beta = 0.0;
@@ -83,7 +83,7 @@ struct GemmDesc {
   double* C = nullptr;
   long long ldc = 0;
   bool a_trans = false, b_trans = false, lower_only = false;
-  int max_ctas = 0;
+  int max_sms = 0;
 };
 int dgemm(Ctx& c, const GemmDesc& d, cudaStream_t st);
 

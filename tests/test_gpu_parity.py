@@ -57,6 +57,17 @@ def test_gemm_alpha_beta(ctx, alpha, beta):
     assert np.all(np.abs(C - ref) <= abs(alpha) * gemm_bound(A, B, k) + 4 * EPS * np.abs(beta * C0))
 
 
+@pytest.mark.parametrize("m,k,n", [(2100, 200, 2050), (1500, 128, 3000), (700, 16, 900)])
+def test_gemm_short_k_update_many_tiles(ctx, m, k, n):
+    # the trailing-update shape (k <= 256, beta != 0) with several output
+    # tiles per persistent CTA and ragged edges
+    g = philox(m + 3 * k + 5 * n)
+    A, B, C0 = g.uniform(-1, 1, (m, k)), g.uniform(-1, 1, (k, n)), g.uniform(-1, 1, (m, n))
+    C = host(lmb200.gemm(-1.0, dev(A), dev(B), 1.0, dev(C0), ctx))
+    ref = C0 - A @ B
+    assert np.all(np.abs(C - ref) <= gemm_bound(A, B, k) + 4 * EPS * np.abs(C0))
+
+
 def test_gemm_known_answers(ctx, golden_known):
     c = golden_known["test_gemmLarger"]
     got = host(lmb200.gemm(c["alpha"], dev(np.array(c["A"], float)), dev(np.array(c["B"], float)), c["beta"],
