@@ -62,7 +62,20 @@ __device__ __forceinline__ void tma_prefetch_l2_2d(const CUtensorMap* tmap, int 
 template <int BM, int BN, int MINB, bool CSM = false>
 struct GemmCfg {
   static constexpr int NC = (BM / 64) * (BN / 32);  // consumer warps
-  static constexpr int THREADS = (NC + 1) * 32;
+  // Short-k update (CSM): the producer is a whole warpgroup so that
+  // setmaxnreg can move its registers to the consumers (a lone producer warp
+  // puts three warps on one SM sub-partition, which caps every thread at 168
+  // registers and spills the 64 x 32 FP64 accumulator tile in the main loop;
+  // at k = 128 that cost 17%, while the long-k kernel measured the same
+  // either way)
+  static constexpr bool SPLIT_REGS = CSM && NC == 8 && MINB == 1;
+  static constexpr int PRODUCER_WARPS = SPLIT_REGS ? 4 : 1;
+  static constexpr int THREADS = (NC + PRODUCER_WARPS) * 32;
+  static constexpr int LAUNCH_REGS = 168;  // 65536 / 384, rounded down to 8
+  static constexpr int CONSUMER_REGS = 232, PRODUCER_REGS = 40;
+  static_assert(!SPLIT_REGS || NC * 32 * CONSUMER_REGS + PRODUCER_WARPS * 32 * PRODUCER_REGS <=
+                                     THREADS * LAUNCH_REGS,
+                "register split must fit in what the CTA is launched with");
   static constexpr int A_BYTES = BM * kBK * 8;
   static constexpr int B_BYTES = BN * kBK * 8;
   static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
@@ -130,9 +143,11 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB, CSM>::THREADS, MINB)
   }
   __syncthreads();
 
-  if (warp == Cfg::NC) {
+  if (warp >= Cfg::NC) {
     // ---------------- producer ----------------
-    if (lane == 0) {
+    if constexpr (Cfg::SPLIT_REGS)
+      asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(Cfg::PRODUCER_REGS) : "memory");
+    if (warp == Cfg::NC && lane == 0) {
       tma_prefetch_desc(&tmA);
       tma_prefetch_desc(&tmB);
       if (CSM) tma_prefetch_desc(&tmC);
@@ -176,6 +191,8 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB, CSM>::THREADS, MINB)
   }
 
   // ---------------- consumers ----------------
+  if constexpr (Cfg::SPLIT_REGS)
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(Cfg::CONSUMER_REGS) : "memory");
   const int wm = warp / (BN / 32);
   const int wn = warp % (BN / 32);
   const int gq = lane >> 2;  // groupID
@@ -341,6 +358,13 @@ int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
   const int dev = ctx_device(ctx);
   if (!attr_set[dev]) {
     LM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
+    if (Cfg::SPLIT_REGS) {
+      // the setmaxnreg split assumes the CTA is launched with LAUNCH_REGS per
+      // thread; with fewer the consumers' increase could never be granted
+      cudaFuncAttributes fa;
+      LM_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
+      if (fa.numRegs < Cfg::LAUNCH_REGS) return LM_ERR_UNSUPPORTED;
+    }
     attr_set[dev] = true;
   }
   CUtensorMap tmA, tmB;
