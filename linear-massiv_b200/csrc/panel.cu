@@ -12,6 +12,11 @@
 //   memory, picks the pivot (largest |a|, lowest row on ties — the reference's
 //   strict '>' scan), swaps and eliminates its own rows, fusing the next
 //   column's local argmax into the elimination pass.
+//   Each thread keeps its rows in registers in a rotating layout (slot 0 is
+//   always the current column; finished columns move to the end), so that
+//   every column step runs the same compact code: a loop body specialised per
+//   column index does not fit the instruction cache and made each step
+//   fetch-bound.
 //   NaN rule of the reference scan: if |a_jj| is NaN it stays the pivot; NaNs
 //   below it never win.
 //
@@ -71,9 +76,16 @@ struct LeafSmem {
   static constexpr size_t tsrc_off = trow_off + 2 * W * sizeof(int);        // int[2W] their sources
   static constexpr size_t tm_off = tsrc_off + 2 * W * sizeof(int);          // int touched count
   static constexpr size_t stage_off = (tm_off + sizeof(int) + 15) / 16 * 16;
-  // Swap staging for the other panel columns: 2W rows x up to 128 columns, split over the cluster.
+  // One region, used twice: first the CTA's slab (rpc rows x W, row stride
+  // W + 1) for coalesced loads and write-back, then the swap staging for the
+  // other panel columns (2W rows x up to 128 columns, split over the cluster).
+  static constexpr int SLD = W + 1;
   static size_t stage_elems(int C) { return (size_t)(2 * W * 128 + C - 1) / C; }
-  static size_t bytes(int /*rpc*/, int C) { return stage_off + stage_elems(C) * sizeof(T); }
+  static size_t region_elems(int rpc, int C) {
+    const size_t slab = (size_t)rpc * SLD;
+    return slab > stage_elems(C) ? slab : stage_elems(C);
+  }
+  static size_t bytes(int rpc, int C) { return stage_off + region_elems(rpc, C) * sizeof(T); }
 };
 
 template <typename T>
@@ -137,13 +149,22 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     fence_barrier_init();
   }
   // This thread's rows of the slab, in registers: row r = tid + u * threads.
+  // The slab through shared memory: each warp instruction reads 32 / W whole
+  // rows (coalesced), then every thread takes its rows from there.
+  constexpr int SLD = L::SLD;
+  constexpr int RPI = 32 / W;  // rows per warp instruction
+  T* slab = stage;
+  for (int r = warp * RPI + lane / W; r < rcnt; r += (kLeafThreads / 32) * RPI) {
+    const int c = lane % W;
+    slab[r * SLD + c] = c < w ? A[(long long)(c0 + rbeg + r) * lda + c0 + c] : T(0);
+  }
+  __syncthreads();
   T x[RPT][W];
 #pragma unroll
   for (int u = 0; u < RPT; ++u) {
     const int r = tid + u * kLeafThreads;
-    const T* src = A + (long long)(c0 + rbeg + r) * lda + c0;
 #pragma unroll
-    for (int c = 0; c < W; ++c) x[u][c] = (r < rcnt && c < w) ? src[c] : T(0);
+    for (int c = 0; c < W; ++c) x[u][c] = r < rcnt ? slab[r * SLD + c] : T(0);
   }
   cluster_sync_all();  // every CTA's barriers exist before anyone pushes into them
 
@@ -159,9 +180,10 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   }
 
   bool timed_out = false;
-#pragma unroll
-  for (int j = 0; j < W; ++j) {
-    if (j >= w) break;
+  // Column j's step.  Register layout of a row at step j: slot c < W - j holds
+  // column j + c, slot W - j + i holds the finished column i.
+#pragma unroll 1
+  for (int j = 0; j < w; ++j) {
     const int par = j & 1;
     const int owner_j = j / rpc;
     if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)((C + 1) * M::BYTES));
@@ -217,7 +239,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
               if (u == uj) {
 #pragma unroll
                 for (int c = 0; c < W; ++c) outj[4 + c] = x[u][c];
-                const T d = x[u][j];
+                const T d = x[u][0];
                 outj[0] = (d != d) ? T(1) : T(0);
                 outj[1] = T(0);
                 outj[2] = T(0);
@@ -255,7 +277,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
       prow = rc + qw * M::N + 4;
     }
     const T* rowj = rj + 4;
-    const T piv = prow[j];
+    const T piv = prow[0];
     if (tid == 0) hist[j] = p;
     if (q == 0 && tid == 0) {
       ipiv[c0 + j] = c0 + p;
@@ -278,52 +300,81 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
           for (int c = 0; c < W; ++c) x[u][c] = rowj[c];
         }
         if (gr > j) {
-          const T mult = x[u][j] / piv;
-          x[u][j] = mult;
+          const T mult = x[u][0] / piv;
+          x[u][0] = mult;
 #pragma unroll
-          for (int c = j + 1; c < W; ++c) x[u][c] = fma(-mult, prow[c], x[u][c]);
+          for (int c = 1; c < W; ++c)
+            if (c < W - j) x[u][c] = fma(-mult, prow[c], x[u][c]);
           if (j + 1 < w) {
-            const T a1 = absval(x[u][j + 1]);
+            const T a1 = absval(x[u][1]);
             if (better(a1, gr, bv, bi)) { bv = a1; bi = gr; }
           }
         }
       }
+      // column j's final value moves to the end
+      const T t0 = x[u][0];
+#pragma unroll
+      for (int c = 0; c + 1 < W; ++c) x[u][c] = x[u][c + 1];
+      x[u][W - 1] = t0;
     }
     // The buffers of this parity are rewritten two columns later; the
     // barrier at the top of the next column orders these reads before this
     // CTA pushes again, and no CTA can run two columns ahead of another.
   }
+  // a leaf narrower than W stops w steps into the rotation: finish it
+#pragma unroll 1
+  for (int k = w; k < W; ++k)
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+      const T t0 = x[u][0];
+#pragma unroll
+      for (int c = 0; c + 1 < W; ++c) x[u][c] = x[u][c + 1];
+      x[u][W - 1] = t0;
+    }
   // Nobody may leave while others can still write into it.
   cluster_sync_all();
+  // write-back through the slab, coalesced like the load
 #pragma unroll
   for (int u = 0; u < RPT; ++u) {
     const int r = tid + u * kLeafThreads;
-    if (r < rcnt) {
-      T* dst = A + (long long)(c0 + rbeg + r) * lda + c0;
+    if (r < rcnt)
 #pragma unroll
-      for (int c = 0; c < W; ++c)
-        if (c < w) dst[c] = x[u][c];
-    }
+      for (int c = 0; c < W; ++c) slab[r * SLD + c] = x[u][c];
   }
+  __syncthreads();
+  for (int r = warp * RPI + lane / W; r < rcnt; r += (kLeafThreads / 32) * RPI) {
+    const int c = lane % W;
+    if (c < w) A[(long long)(c0 + rbeg + r) * lda + c0 + c] = slab[r * SLD + c];
+  }
+  __syncthreads();  // the region is the swap staging from here on
   // This leaf's interchanges on the other columns of the enclosing panel
   // [pc0, pc0 + pw): compose them (rows relative to c0), gather every touched
   // row's source over the cluster, barrier, scatter.
   const int ocols = pw - w;
   if (ocols > 0) {
-    if (tid == 0) {
-      int m = w;
-      for (int ii = 0; ii < w; ++ii) { trow[ii] = ii; tsrc[ii] = ii; }
-      for (int ii = 0; ii < w; ++ii) {
-        const int pr = hist[ii];
-        if (pr == ii) continue;
-        int sp = -1;
-        if (pr < w) sp = pr;
-        for (int e = w; e < m && sp < 0; ++e)
-          if (trow[e] == pr) sp = e;
-        if (sp < 0) { trow[m] = pr; tsrc[m] = pr; sp = m++; }
-        const int t = tsrc[ii]; tsrc[ii] = tsrc[sp]; tsrc[sp] = t;
+    // Touched rows: 0 .. w-1, then each pivot row >= w in order of first
+    // use; the source of row r is tau_0(tau_1(... tau_{w-1}(r))), walking
+    // the interchanges backwards.  One warp (w <= 32).
+    if (warp == 0) {
+      const int pr = lane < w ? hist[lane] : -1;
+      bool fresh = lane < w && pr >= w;
+      for (int jj = 0; jj < lane && jj < w; ++jj)
+        if (hist[jj] == pr) fresh = false;
+      const unsigned bal = __ballot_sync(0xffffffffu, fresh);
+      if (lane < w) trow[lane] = lane;
+      if (fresh) trow[w + __popc(bal & ((1u << lane) - 1u))] = pr;
+      const int m = w + __popc(bal);
+      __syncwarp();
+      for (int e = lane; e < m; e += 32) {
+        int r = trow[e];
+        for (int jj = w - 1; jj >= 0; --jj) {
+          const int h = hist[jj];
+          if (r == jj) r = h;
+          else if (r == h) r = jj;
+        }
+        tsrc[e] = r;
       }
-      *tm = m;
+      if (lane == 0) *tm = m;
     }
     __syncthreads();
     const int m = *tm;
