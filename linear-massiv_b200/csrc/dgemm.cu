@@ -360,7 +360,8 @@ int launch_dmma(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
     LM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::SMEM));
     if (Cfg::SPLIT_REGS) {
       // the setmaxnreg split assumes the CTA is launched with LAUNCH_REGS per
-      // thread; with fewer the consumers' increase could never be granted
+      // thread; with fewer the consumers' increase could never be granted,
+      // so the caller falls back to another kernel
       cudaFuncAttributes fa;
       LM_CUDA_TRY(cudaFuncGetAttributes(&fa, kern));
       if (fa.numRegs < Cfg::LAUNCH_REGS) return LM_ERR_UNSUPPORTED;
@@ -440,9 +441,16 @@ int dgemm(Ctx& ctx, const GemmDesc& d, cudaStream_t st) {
   const bool narrow = (d.n <= 64 || d.k <= 256) && !d.lower_only;
   const bool c_tma = d.beta != 0.0 && !(reinterpret_cast<uintptr_t>(d.C) & 15) && !(d.ldc & 1);
   if (d.k <= 256 && d.n > 64 && c_tma) {
-    if (d.a_trans) return launch_dmma<128, 128, true, false, 1, true>(ctx, d, st);
-    if (d.b_trans) return launch_dmma<128, 128, false, true, 1, true>(ctx, d, st);
-    return launch_dmma<128, 128, false, false, 1, true>(ctx, d, st);
+    int rc;
+    if (d.a_trans)
+      rc = launch_dmma<128, 128, true, false, 1, true>(ctx, d, st);
+    else if (d.b_trans)
+      rc = launch_dmma<128, 128, false, true, 1, true>(ctx, d, st);
+    else
+      rc = launch_dmma<128, 128, false, false, 1, true>(ctx, d, st);
+    // LM_ERR_UNSUPPORTED before any launch: compiled with fewer registers
+    // than the register split needs; the kernels below take the update
+    if (rc != LM_ERR_UNSUPPORTED) return rc;
   }
   if (d.a_trans)
     return narrow ? launch_dmma<128, 64, true, false, 2>(ctx, d, st)
