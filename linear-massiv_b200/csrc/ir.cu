@@ -445,7 +445,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 // diagonal blocks runs on the tensor cores (3xTF32):
 //   a: diagonal block (nopiv_diag: LU in one CTA, then the FP64 inverses);
 //      L_a = A[below a, a] inv(U_aa),  U_a = inv(L_aa) A[a, right of a],
-//      each with one correction step (X += (B - X U) inv(U)) when the
+//      each with one correction step (X += (B - X U) inv(U)), for n > 4096, when the
 //      diagonal factor's 1-norm condition number exceeds kRefineCond: without
 //      pivoting a few diagonal blocks are ill-conditioned, and a plain product
 //      with their explicit inverse loses accuracy by that condition (the
@@ -462,6 +462,8 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
 // layout of the persistent substitutions, rflag (2 ints per 128-column block:
 // L, U) the ill-conditioning flags that the substitutions' correction step
 // follows too.  A zero pivot is recorded in status[1].
+constexpr int kBlockCorrMinN = 4096;
+
 int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* DinvU, int* rflag, cudaStream_t st) {
   constexpr int SW = 2 * kNB;  // super-step width
   const size_t blk = (size_t)kNB * kNB;
@@ -517,6 +519,10 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
   // Block at k0 (w wide, diagonal block factored): L = A[k0+w:, k0:k0+w] inv(U)
   // and U = inv(L) A[k0:k0+w, k0+w:] in place, m = n - k0 - w; then their
   // splits into column `col` of the k = 256 operands, rows from `row0`.
+  // Below this order the first-step errors of the uncorrected factor stay
+  // small (5e-5 at n = 4096 for kappa = 1e2), and the correction chain's five
+  // launches per block part, switched off or not, cost more than they save.
+  const bool block_corr = n > kBlockCorrMinN;
   auto block_solves = [&](int k0, int w, int m, float* ahi, float* alo, float* bhi, float* blo) {
     float** d = inv[(k0 / kNB) & 1];
     float* A11 = A + (long long)k0 * lda + k0;
@@ -530,23 +536,27 @@ int sgetrf_nopiv(Ctx& c, int n, float* A, long long lda, float* DinvL, float* Di
     const int* gl = gu + 1;
     {
       Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 8.0 * m * w, st);
-      LM_TRY(split_rows(Thi, Tlo, kNB, A21, m, w, st, 0, nullptr, Rb, kNB));
+      LM_TRY(split_rows(Thi, Tlo, kNB, A21, m, w, st, 0, nullptr, block_corr ? Rb : nullptr, kNB));
     }
     LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, Thi, kNB, d[2], kNB, 0.0f, A21, lda, st, Tlo, d[3]));
-    LM_TRY(split_rows(Xhi, Xlo, kNB, A21, m, w, st, 0, gl));
-    LM_TRY(sgemm_tf32(c, m, w, w, -1.0f, Xhi, kNB, d[6], kNB, 1.0f, Rb, kNB, st, Xlo, d[7], 0, gl));
-    LM_TRY(split_rows(Thi, Tlo, kNB, Rb, m, w, st, kNB, gl));
-    LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, Thi, kNB, d[2], kNB, 1.0f, A21, lda, st, Tlo, d[3], 0, gl));
+    if (block_corr) {
+      LM_TRY(split_rows(Xhi, Xlo, kNB, A21, m, w, st, 0, gl));
+      LM_TRY(sgemm_tf32(c, m, w, w, -1.0f, Xhi, kNB, d[6], kNB, 1.0f, Rb, kNB, st, Xlo, d[7], 0, gl));
+      LM_TRY(split_rows(Thi, Tlo, kNB, Rb, m, w, st, kNB, gl));
+      LM_TRY(sgemm_tf32(c, m, w, w, 1.0f, Thi, kNB, d[2], kNB, 1.0f, A21, lda, st, Tlo, d[3], 0, gl));
+    }
     // U = inv(L) B likewise, with B^T as the K-major operand
     {
       Prof p(c, kPhaseTrsm, 2.0 * m * w * w, 8.0 * m * w, st);
-      LM_TRY(split_cols(Thi, Tlo, kNB, A12, w, m, st, 0, nullptr, Rt, ldr));
+      LM_TRY(split_cols(Thi, Tlo, kNB, A12, w, m, st, 0, nullptr, block_corr ? Rt : nullptr, ldr));
     }
     LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, Thi, kNB, 0.0f, A12, lda, st, d[1], Tlo));
-    LM_TRY(split_cols(Xhi, Xlo, kNB, A12, w, m, st, 0, gu));
-    LM_TRY(sgemm_tf32(c, w, m, w, -1.0f, d[4], kNB, Xhi, kNB, 1.0f, Rt, ldr, st, d[5], Xlo, 0, gu));
-    LM_TRY(split_cols(Thi, Tlo, kNB, Rt, w, m, st, ldr, gu));
-    LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, Thi, kNB, 1.0f, A12, lda, st, d[1], Tlo, 0, gu));
+    if (block_corr) {
+      LM_TRY(split_cols(Xhi, Xlo, kNB, A12, w, m, st, 0, gu));
+      LM_TRY(sgemm_tf32(c, w, m, w, -1.0f, d[4], kNB, Xhi, kNB, 1.0f, Rt, ldr, st, d[5], Xlo, 0, gu));
+      LM_TRY(split_cols(Thi, Tlo, kNB, Rt, w, m, st, ldr, gu));
+      LM_TRY(sgemm_tf32(c, w, m, w, 1.0f, d[0], kNB, Thi, kNB, 1.0f, A12, lda, st, d[1], Tlo, 0, gu));
+    }
     LM_TRY(split_rows(ahi, alo, ldk, A21, m, w, st));
     return split_cols(bhi, blo, ldk, A12, w, m, st);
   };

@@ -153,7 +153,8 @@ __device__ __forceinline__ void load_row_share(T* out, const T* src, int c0, int
 // increasing order; backward: U upper, blocks in decreasing order.
 // sync[0] = progress counter, sync[1] = ticket dispenser (both zero at launch).
 // corr (FP32 only): per-block flags at stride 2; when given, the correction
-// step on the diagonal block runs only for blocks whose flag is set.
+// step on the diagonal block runs only for blocks whose flag is set.  The
+// 16-column variant never takes the correction step.
 template <typename T, int RHS>
 __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
                                                              int nrhs, int forward, const T* __restrict__ Dinv,
@@ -322,7 +323,9 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
       }
     };
     inv_times_ys(acc);
-    if (corr != nullptr && corr[2 * b] == 0) {  // uniform over the CTA
+    // The 16-column variant keeps the plain product: the correction's
+    // operands do not fit its registers (it spilled in the dependency loop).
+    if (RHS > 4 || (corr != nullptr && corr[2 * b] == 0)) {  // uniform over the CTA
       if (q == 0 && row_ok)
 #pragma unroll
         for (int h = 0; h < MAX_RHS; ++h)
@@ -411,6 +414,7 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
 // nrhs (more than 4 in passes of 16 columns).  `sync` holds 4 ints of device
 // scratch.  FP32: corr, when given, holds two flags per diagonal block (L, U);
 // only flagged blocks take the correction step, all blocks do without it.
+// Passes of the 16-column variant (nrhs > 4) multiply by the inverse only.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
             int* sync, int* status, cudaStream_t st, const int* corr) {
