@@ -47,6 +47,38 @@ __device__ __forceinline__ T absval(T x) {
   return (a != a) ? T(-1) : a;  // NaN never wins the scan
 }
 
+// Scan values (absval's: -1 or >= 0) as integers in the order of better():
+// 0 for -1, 1 for zero (either sign), the IEEE bits + 1 above, which grow
+// with the value.  A warp then reduces (key, row) with three redux.sync
+// instead of five shuffle rounds of (value, row) pairs.
+template <typename T>
+__device__ __forceinline__ unsigned long long scan_key(T v) {
+  if (!(v >= T(0))) return 0ull;
+  if (v == T(0)) return 1ull;
+  if constexpr (sizeof(T) == 8)
+    return (unsigned long long)__double_as_longlong((double)v) + 1ull;
+  else
+    return (unsigned long long)__float_as_uint((float)v) + 1ull;
+}
+template <typename T>
+__device__ __forceinline__ T key_value(unsigned long long k) {
+  if (k == 0ull) return T(-1);
+  if constexpr (sizeof(T) == 8)
+    return (T)__longlong_as_double((long long)(k - 1ull));
+  else
+    return (T)__uint_as_float((unsigned)(k - 1ull));
+}
+// Every lane receives the warp's best (key, row) under better(): the largest
+// key, then the lowest row (rows are >= 0, or INT_MAX for none).
+__device__ __forceinline__ void warp_best(unsigned long long& key, int& row) {
+  const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
+  const unsigned hi = __reduce_max_sync(0xffffffffu, khi);
+  const unsigned lo = __reduce_max_sync(0xffffffffu, khi == hi ? klo : 0u);
+  const unsigned long long best = ((unsigned long long)hi << 32) | lo;
+  row = (int)__reduce_min_sync(0xffffffffu, key == best ? (unsigned)row : 0xffffffffu);
+  key = best;
+}
+
 // Per-column messages pushed into every CTA of the cluster (T elements):
 //   candidate message (one per source CTA): [0] |a| of its best candidate or
 //     -1, [1] that row relative to c0 (or -1), [2..3] unused, [4, 4 + W) the row;
@@ -187,23 +219,21 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     const int par = j & 1;
     const int owner_j = j / rpc;
     if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)((C + 1) * M::BYTES));
-    // ---- CTA argmax: warp shuffles, one barrier, every warp reduces ----
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T ov = __shfl_xor_sync(0xffffffffu, bv, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (better(ov, oi, bv, bi)) { bv = ov; bi = oi; }
+    // ---- CTA argmax: warp reduction, one barrier, every warp reduces ----
+    {
+      unsigned long long k = scan_key(bv);
+      warp_best(k, bi);
+      bv = key_value<T>(k);
     }
     if (lane == 0) { wval[warp] = bv; widx[warp] = bi; }
     __syncthreads();
     {
       T v = lane < kLeafThreads / 32 ? wval[lane] : T(-1);
       int i = lane < kLeafThreads / 32 ? widx[lane] : INT_MAX;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-        if (better(ov, oi, v, i)) { v = ov; i = oi; }
+      {
+        unsigned long long k = scan_key(v);
+        warp_best(k, i);
+        v = key_value<T>(k);
       }
       // the warp owning the CTA's best row stages and pushes it (warp 0 if none)
       const int rl = (i != INT_MAX) ? i - rbeg : -1;
@@ -256,16 +286,15 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
 
     const T* rc = cand + (size_t)par * 16 * M::N;
     const T* rj = rowjb + (size_t)par * M::N;
-    T v = lane < C ? rc[lane * M::N + 0] : T(-1);
     int i = lane < C ? (int)rc[lane * M::N + 1] : INT_MAX;
     if (i < 0) i = INT_MAX;
-    int qw = lane;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T ov = __shfl_xor_sync(0xffffffffu, v, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, i, o);
-      const int oq = __shfl_xor_sync(0xffffffffu, qw, o);
-      if (better(ov, oi, v, i)) { v = ov; i = oi; qw = oq; }
+    int qw;
+    {
+      const unsigned long long mine = scan_key(lane < C ? rc[lane * M::N + 0] : T(-1));
+      const int my_row = i;
+      unsigned long long k = mine;
+      warp_best(k, i);
+      qw = __ffs(__ballot_sync(0xffffffffu, mine == k && my_row == i)) - 1;  // the winning CTA
     }
     int p;
     const T* prow;
