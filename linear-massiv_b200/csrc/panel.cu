@@ -16,7 +16,10 @@
 //   always the current column; finished columns move to the end), so that
 //   every column step runs the same compact code: a loop body specialised per
 //   column index does not fit the instruction cache and made each step
-//   fetch-bound.
+//   fetch-bound.  Rows never move between threads: each carries its logical
+//   row index, an interchange swaps two labels, and the write-back puts every
+//   row at its final position.  So only the candidates travel per column; the
+//   NaN rule for a_jj rides on the candidate of the CTA holding row j.
 //   NaN rule of the reference scan: if |a_jj| is NaN it stays the pivot; NaNs
 //   below it never win.
 //
@@ -60,13 +63,25 @@ __device__ __forceinline__ unsigned long long scan_key(T v) {
   else
     return (unsigned long long)__float_as_uint((float)v) + 1ull;
 }
+// Row j with a NaN a_jj stays the pivot (the reference scan starts at row j
+// and NaN never compares greater): its key beats every other.
+constexpr unsigned long long kForcedKey = ~0ull;
+// A key in the message's T-sized slot, bit for bit (float keys fit 32 bits).
 template <typename T>
-__device__ __forceinline__ T key_value(unsigned long long k) {
-  if (k == 0ull) return T(-1);
+__device__ __forceinline__ T key_to_msg(unsigned long long k) {
   if constexpr (sizeof(T) == 8)
-    return (T)__longlong_as_double((long long)(k - 1ull));
+    return (T)__longlong_as_double((long long)k);
   else
-    return (T)__uint_as_float((unsigned)(k - 1ull));
+    return (T)__uint_as_float(k == kForcedKey ? 0xffffffffu : (unsigned)k);
+}
+template <typename T>
+__device__ __forceinline__ unsigned long long msg_to_key(T m) {
+  if constexpr (sizeof(T) == 8) {
+    return (unsigned long long)__double_as_longlong((double)m);
+  } else {
+    const unsigned b = __float_as_uint((float)m);
+    return b == 0xffffffffu ? kForcedKey : (unsigned long long)b;
+  }
 }
 // Every lane receives the warp's best (key, row) under better(): the largest
 // key, then the lowest row (rows are >= 0, or INT_MAX for none).
@@ -79,11 +94,11 @@ __device__ __forceinline__ void warp_best(unsigned long long& key, int& row) {
   key = best;
 }
 
-// Per-column messages pushed into every CTA of the cluster (T elements):
-//   candidate message (one per source CTA): [0] |a| of its best candidate or
-//     -1, [1] that row relative to c0 (or -1), [2..3] unused, [4, 4 + W) the row;
-//   row-j message (from the CTA owning row j): [0] 1 if a_jj is NaN,
-//     [1..3] unused, [4, 4 + W) row j.
+// Per-column message pushed into every CTA of the cluster (T elements), one
+// per source CTA: [0] the scan key of its best candidate (bit pattern, see
+// scan_key; kForcedKey when that row is row j with a NaN a_jj), [1] that
+// row's logical index relative to c0 (or -1), [2..3] unused, [4, 4 + W) the
+// row in the rotated register layout.
 template <typename T, int W>
 struct LeafMsg {
   static constexpr int N = 4 + W;
@@ -97,24 +112,24 @@ template <typename T, int W>
 struct LeafSmem {
   using M = LeafMsg<T, W>;
   static constexpr size_t cand_off = 0;                                    // T[2][16][N]
-  static constexpr size_t rowj_off = cand_off + 2 * 16 * (size_t)M::BYTES;  // T[2][N]
-  static constexpr size_t outc_off = rowj_off + 2 * (size_t)M::BYTES;       // T[N] outgoing candidate
-  static constexpr size_t outj_off = outc_off + (size_t)M::BYTES;           // T[N] outgoing row j
-  static constexpr size_t bar_off = outj_off + (size_t)M::BYTES;            // uint64_t[2]
-  static constexpr size_t wval_off = bar_off + 16;                          // T[16]
-  static constexpr size_t widx_off = wval_off + 16 * sizeof(T);             // int[16]
+  static constexpr size_t outc_off = cand_off + 2 * 16 * (size_t)M::BYTES;  // T[N] outgoing candidate
+  static constexpr size_t bar_off = outc_off + (size_t)M::BYTES;            // uint64_t[2]
+  static constexpr size_t wkey_off = bar_off + 16;                          // uint64_t[16] warp best keys
+  static constexpr size_t widx_off = wkey_off + 16 * sizeof(unsigned long long);  // int[16] their rows
   static constexpr size_t hist_off = widx_off + 16 * sizeof(int);           // int[W] pivot rows
   static constexpr size_t trow_off = hist_off + W * sizeof(int);            // int[2W] touched rows
   static constexpr size_t tsrc_off = trow_off + 2 * W * sizeof(int);        // int[2W] their sources
   static constexpr size_t tm_off = tsrc_off + 2 * W * sizeof(int);          // int touched count
   static constexpr size_t stage_off = (tm_off + sizeof(int) + 15) / 16 * 16;
   // One region, used twice: first the CTA's slab (rpc rows x W, row stride
-  // W + 1) for coalesced loads and write-back, then the swap staging for the
-  // other panel columns (2W rows x up to 128 columns, split over the cluster).
+  // W + 1) for coalesced loads and write-back, followed by the rows' final
+  // logical indices (rpc ints), then the swap staging for the other panel
+  // columns (2W rows x up to 128 columns, split over the cluster).
   static constexpr int SLD = W + 1;
   static size_t stage_elems(int C) { return (size_t)(2 * W * 128 + C - 1) / C; }
+  __host__ __device__ static size_t slab_elems(int rpc) { return (size_t)rpc * SLD; }
   static size_t region_elems(int rpc, int C) {
-    const size_t slab = (size_t)rpc * SLD;
+    const size_t slab = slab_elems(rpc) + ((size_t)rpc * sizeof(int) + sizeof(T) - 1) / sizeof(T);
     return slab > stage_elems(C) ? slab : stage_elems(C);
   }
   static size_t bytes(int rpc, int C) { return stage_off + region_elems(rpc, C) * sizeof(T); }
@@ -153,11 +168,9 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   using M = LeafMsg<T, W>;
   extern __shared__ __align__(16) unsigned char sm[];
   T* cand = reinterpret_cast<T*>(sm + L::cand_off);
-  T* rowjb = reinterpret_cast<T*>(sm + L::rowj_off);
   T* outc = reinterpret_cast<T*>(sm + L::outc_off);
-  T* outj = reinterpret_cast<T*>(sm + L::outj_off);
   uint64_t* rbar = reinterpret_cast<uint64_t*>(sm + L::bar_off);
-  T* wval = reinterpret_cast<T*>(sm + L::wval_off);
+  unsigned long long* wkey = reinterpret_cast<unsigned long long*>(sm + L::wkey_off);
   int* widx = reinterpret_cast<int*>(sm + L::widx_off);
   int* hist = reinterpret_cast<int*>(sm + L::hist_off);
   int* trow = reinterpret_cast<int*>(sm + L::trow_off);
@@ -200,14 +213,19 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
   }
   cluster_sync_all();  // every CTA's barriers exist before anyone pushes into them
 
-  T bv = T(-1);
+  // logical row (relative to c0) of each of this thread's rows
+  int lr[RPT];
+#pragma unroll
+  for (int u = 0; u < RPT; ++u) lr[u] = rbeg + tid + u * kLeafThreads;
+  // this thread's best candidate for the next column: (key, logical row)
+  unsigned long long bk = 0ull;
   int bi = INT_MAX;
 #pragma unroll
   for (int u = 0; u < RPT; ++u) {
     const int r = tid + u * kLeafThreads;
     if (r < rcnt) {
-      const T v = absval(x[u][0]);
-      if (better(v, rbeg + r, bv, bi)) { bv = v; bi = rbeg + r; }
+      const unsigned long long k = scan_key(absval(x[u][0]));
+      if (k > bk || (k == bk && lr[u] < bi)) { bk = k; bi = lr[u]; }
     }
   }
 
@@ -217,95 +235,64 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
 #pragma unroll 1
   for (int j = 0; j < w; ++j) {
     const int par = j & 1;
-    const int owner_j = j / rpc;
-    if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)((C + 1) * M::BYTES));
-    // ---- CTA argmax: warp reduction, one barrier, every warp reduces ----
-    {
-      unsigned long long k = scan_key(bv);
-      warp_best(k, bi);
-      bv = key_value<T>(k);
+    if (tid == 0) mbar_arrive_expect_tx(&rbar[par], (uint32_t)(C * M::BYTES));
+    // row j with a NaN a_jj is this CTA's candidate whatever else it holds
+#pragma unroll
+    for (int u = 0; u < RPT; ++u) {
+      const int r = tid + u * kLeafThreads;
+      if (r < rcnt && lr[u] == j && x[u][0] != x[u][0]) { bk = kForcedKey; bi = j; }
     }
-    if (lane == 0) { wval[warp] = bv; widx[warp] = bi; }
+    // ---- CTA argmax: warp reduction, one barrier, every warp reduces ----
+    warp_best(bk, bi);
+    if (lane == 0) { wkey[warp] = bk; widx[warp] = bi; }
     __syncthreads();
     {
-      T v = lane < kLeafThreads / 32 ? wval[lane] : T(-1);
-      int i = lane < kLeafThreads / 32 ? widx[lane] : INT_MAX;
-      {
-        unsigned long long k = scan_key(v);
-        warp_best(k, i);
-        v = key_value<T>(k);
-      }
-      // the warp owning the CTA's best row stages and pushes it (warp 0 if none)
-      const int rl = (i != INT_MAX) ? i - rbeg : -1;
-      const int wo = rl >= 0 ? (rl % kLeafThreads) >> 5 : 0;
+      const unsigned long long k0 = lane < kLeafThreads / 32 ? wkey[lane] : 0ull;
+      const int i0 = lane < kLeafThreads / 32 ? widx[lane] : INT_MAX;
+      unsigned long long k = k0;
+      int i = i0;
+      warp_best(k, i);
+      // the warp holding the CTA's best row stages and pushes it (warp 0 if none)
+      const int wo = i == INT_MAX ? 0 : __ffs(__ballot_sync(0xffffffffu, k0 == k && i0 == i)) - 1;
       if (warp == wo) {
-        if (rl >= 0 && tid == rl % kLeafThreads) {
-          const int uo = rl / kLeafThreads;
+        if (i != INT_MAX) {
 #pragma unroll
           for (int u = 0; u < RPT; ++u)
-            if (u == uo) {
+            if (tid + u * kLeafThreads < rcnt && lr[u] == i) {
 #pragma unroll
               for (int c = 0; c < W; ++c) outc[4 + c] = x[u][c];
             }
+        } else if (lane < W) {
+          outc[4 + lane] = T(0);
         }
-        if (rl < 0 && lane < W) outc[4 + lane] = T(0);
         if (lane == 0) {
-          outc[0] = rl >= 0 ? v : T(-1);
-          outc[1] = rl >= 0 ? T(i) : T(-1);
+          outc[0] = key_to_msg<T>(k);
+          outc[1] = i != INT_MAX ? T(i) : T(-1);
           outc[2] = T(0);
           outc[3] = T(0);
         }
         __syncwarp();
         push_all<T, W>(outc, cand + ((size_t)par * 16 + q) * M::N, &rbar[par], C, lane);
       }
-      // the warp owning row j pushes it
-      if (q == owner_j) {
-        const int rj = j - rbeg;
-        if (warp == ((rj % kLeafThreads) >> 5)) {
-          if (tid == rj % kLeafThreads) {
-            const int uj = rj / kLeafThreads;
-#pragma unroll
-            for (int u = 0; u < RPT; ++u)
-              if (u == uj) {
-#pragma unroll
-                for (int c = 0; c < W; ++c) outj[4 + c] = x[u][c];
-                const T d = x[u][0];
-                outj[0] = (d != d) ? T(1) : T(0);
-                outj[1] = T(0);
-                outj[2] = T(0);
-                outj[3] = T(0);
-              }
-          }
-          __syncwarp();
-          push_all<T, W>(outj, rowjb + (size_t)par * M::N, &rbar[par], C, lane);
-        }
-      }
     }
-    // ---- wait for the C candidates and row j ----
+    // ---- wait for the C candidates ----
     if (!timed_out && !mbar_wait_spin(&rbar[par], (uint32_t)((j >> 1) & 1), status)) timed_out = true;
 
     const T* rc = cand + (size_t)par * 16 * M::N;
-    const T* rj = rowjb + (size_t)par * M::N;
     int i = lane < C ? (int)rc[lane * M::N + 1] : INT_MAX;
     if (i < 0) i = INT_MAX;
     int qw;
     {
-      const unsigned long long mine = scan_key(lane < C ? rc[lane * M::N + 0] : T(-1));
+      const unsigned long long mine = lane < C ? msg_to_key(rc[lane * M::N + 0]) : 0ull;
       const int my_row = i;
       unsigned long long k = mine;
       warp_best(k, i);
       qw = __ffs(__ballot_sync(0xffffffffu, mine == k && my_row == i)) - 1;  // the winning CTA
     }
-    int p;
-    const T* prow;
-    if (rj[0] != T(0) || i == INT_MAX || qw >= C) {
-      p = j;
-      prow = rj + 4;
-    } else {
-      p = i;
-      prow = rc + qw * M::N + 4;
-    }
-    const T* rowj = rj + 4;
+    // (row j itself is always a candidate, so some CTA wins; the fallback
+    // only keeps the indexing in bounds)
+    const int p = (i == INT_MAX || qw >= C) ? j : i;
+    const T* prow = rc + ((i == INT_MAX || qw >= C) ? 0 : qw) * M::N + 4;
     const T piv = prow[0];
     if (tid == 0) hist[j] = p;
     if (q == 0 && tid == 0) {
@@ -313,30 +300,26 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
       if (piv == T(0)) atomicCAS(status + 1, 0, c0 + j + 1);
     }
 
-    // ---- swap, eliminate own rows in registers, scan column j+1 ----
-    bv = T(-1);
+    // ---- interchange labels, eliminate own rows in registers, scan column j+1 ----
+    bk = 0ull;
     bi = INT_MAX;
 #pragma unroll
     for (int u = 0; u < RPT; ++u) {
       const int r = tid + u * kLeafThreads;
       if (r < rcnt) {
-        const int gr = rbeg + r;
-        if (gr == j) {
-#pragma unroll
-          for (int c = 0; c < W; ++c) x[u][c] = prow[c];
-        } else if (gr == p) {
-#pragma unroll
-          for (int c = 0; c < W; ++c) x[u][c] = rowj[c];
-        }
-        if (gr > j) {
+        if (lr[u] == p)
+          lr[u] = j;
+        else if (lr[u] == j)
+          lr[u] = p;
+        if (lr[u] > j) {
           const T mult = x[u][0] / piv;
           x[u][0] = mult;
 #pragma unroll
           for (int c = 1; c < W; ++c)
             if (c < W - j) x[u][c] = fma(-mult, prow[c], x[u][c]);
           if (j + 1 < w) {
-            const T a1 = absval(x[u][1]);
-            if (better(a1, gr, bv, bi)) { bv = a1; bi = gr; }
+            const unsigned long long k1 = scan_key(absval(x[u][1]));
+            if (k1 > bk || (k1 == bk && lr[u] < bi)) { bk = k1; bi = lr[u]; }
           }
         }
       }
@@ -362,18 +345,22 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
     }
   // Nobody may leave while others can still write into it.
   cluster_sync_all();
-  // write-back through the slab, coalesced like the load
+  // write-back through the slab, coalesced like the load, each row to its
+  // logical position
+  int* lrow = reinterpret_cast<int*>(slab + L::slab_elems(rpc));
 #pragma unroll
   for (int u = 0; u < RPT; ++u) {
     const int r = tid + u * kLeafThreads;
-    if (r < rcnt)
+    if (r < rcnt) {
 #pragma unroll
       for (int c = 0; c < W; ++c) slab[r * SLD + c] = x[u][c];
+      lrow[r] = lr[u];
+    }
   }
   __syncthreads();
   for (int r = warp * RPI + lane / W; r < rcnt; r += (kLeafThreads / 32) * RPI) {
     const int c = lane % W;
-    if (c < w) A[(long long)(c0 + rbeg + r) * lda + c0 + c] = slab[r * SLD + c];
+    if (c < w) A[(long long)(c0 + lrow[r]) * lda + c0 + c] = slab[r * SLD + c];
   }
   __syncthreads();  // the region is the swap staging from here on
   // This leaf's interchanges on the other columns of the enclosing panel
