@@ -40,19 +40,15 @@ constexpr int kLeafThreads = 512;
 constexpr int kLeafRowsTimesW = 16384;  // rows per CTA * leaf width (128 KB of FP64)
 
 template <typename T>
-__device__ __forceinline__ bool better(T v1, int i1, T v2, int i2) {
-  return v1 > v2 || (v1 == v2 && i1 < i2);
-}
-
-template <typename T>
 __device__ __forceinline__ T absval(T x) {
   T a = x < T(0) ? -x : x;
   return (a != a) ? T(-1) : a;  // NaN never wins the scan
 }
 
-// Scan values (absval's: -1 or >= 0) as integers in the order of better():
-// 0 for -1, 1 for zero (either sign), the IEEE bits + 1 above, which grow
-// with the value.  A warp then reduces (key, row) with three redux.sync
+// The pivot order of the reference's scan (strict '>' from row j down): the
+// larger |a| wins, the lower row on ties, NaN never wins.  Scan values
+// (absval's: -1 or >= 0) become integers in that order: 0 for -1, 1 for zero
+// (either sign), the IEEE bits + 1 above, which grow with the value.  A warp then reduces (key, row) with three redux.sync
 // instead of five shuffle rounds of (value, row) pairs.
 template <typename T>
 __device__ __forceinline__ unsigned long long scan_key(T v) {
@@ -83,8 +79,8 @@ __device__ __forceinline__ unsigned long long msg_to_key(T m) {
     return b == 0xffffffffu ? kForcedKey : (unsigned long long)b;
   }
 }
-// Every lane receives the warp's best (key, row) under better(): the largest
-// key, then the lowest row (rows are >= 0, or INT_MAX for none).
+// Every lane receives the warp's best (key, row) in the pivot order: the
+// largest key, then the lowest row (rows are >= 0, or INT_MAX for none).
 __device__ __forceinline__ void warp_best(unsigned long long& key, int& row) {
   const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
   const unsigned hi = __reduce_max_sync(0xffffffffu, khi);
