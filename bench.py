@@ -72,7 +72,8 @@ def parse():
     p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
     p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
     p.add_argument("--kappa", type=float, default=1e6, help="ir: condition number of A (0 = uniform A)")
-    p.add_argument("--reflectors", type=int, default=4, help="ir: Householder reflectors per side")
+    p.add_argument("--reflectors", type=int, default=0,
+                   help="ir: Householder reflectors per side (0 = dense Haar-random orthogonal U, V)")
     p.add_argument("--n", type=int, default=16384)
     p.add_argument("--nrhs", type=int, default=1)
     p.add_argument("--seed", type=int, default=0)
@@ -96,8 +97,13 @@ def workload_name(a):
                 f"in [1,16], half SPD (B B^T + n I, Cholesky) half general (uniform[-1,1], LU), "
                 f"{'FP64' if a.precision == 'fp64' else 'FP32 factor + FP64 refinement'}")
     if a.workload == "ir":
-        spec = (f"A = U diag(sigma) V^T, kappa={a.kappa:g}, {a.reflectors} Householder reflectors per side"
-                if a.kappa > 0 else "A uniform[-1,1]")
+        if a.kappa <= 0:
+            spec = "A uniform[-1,1]"
+        elif a.reflectors <= 0:
+            spec = (f"A = U diag(sigma) V^T, kappa={a.kappa:g}, U and V dense random orthogonal "
+                    f"(Q of seeded Gaussian, n Householder reflectors each)")
+        else:
+            spec = f"A = U diag(sigma) V^T, kappa={a.kappa:g}, {a.reflectors} Householder reflectors per side"
         return f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU + 3xTF32 tcgen05, FP64 refinement"
     if a.workload == "lu":
         return f"luSolve FP64 n={a.n} nrhs={a.nrhs}, A uniform[-1,1]"
@@ -482,9 +488,33 @@ def max_over_ranks(x: float, world: int) -> float:
 
 # ---- inputs ---------------------------------------------------------------------------
 
+def dense_randsvd_matrix(n, kappa, seed, torch):
+    """A = U diag(sigma) V^T on the GPU (input preparation, not timed) with U, V
+    dense Haar-random orthogonal: the Q factors of seeded Gaussian matrices, each
+    a product of n Householder reflectors (the reference's randsvd construction,
+    test/Test/Types.hs:196-213); sigma_i = kappa^(-i/(n-1))."""
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(int(seed))
+    s = kappa ** (-torch.arange(n, dtype=torch.float64, device="cuda") / max(n - 1, 1))
+    A = None
+    for side in range(2):
+        G = torch.randn((n, n), dtype=torch.float64, device="cuda", generator=gen)
+        Q, R = torch.linalg.qr(G)
+        Q *= torch.sign(torch.diagonal(R)).unsqueeze(0)  # Haar measure
+        del G, R
+        if side == 0:
+            A = Q * s.unsqueeze(0)   # U diag(sigma)
+        else:
+            A = A @ Q.T              # ... V^T
+        del Q
+    torch.cuda.empty_cache()
+    return A.cpu()
+
+
 def sigma_spectrum_matrix(n, kappa, reflectors, g, torch, np):
     """A = U diag(sigma) V^T on the GPU (input preparation, not timed): sigma_i =
-    kappa^(-i/(n-1)), U and V products of seeded Householder reflectors."""
+    kappa^(-i/(n-1)), U and V products of `reflectors` seeded Householder
+    reflectors (a nearly diagonal matrix for few reflectors)."""
     s = torch.from_numpy(kappa ** (-np.arange(n) / max(n - 1, 1))).cuda()
     A = torch.diag(s)
     for side in ("left", "right"):
@@ -501,7 +531,9 @@ def sigma_spectrum_matrix(n, kappa, reflectors, g, torch, np):
 def make_inputs(a, rank, torch, np):
     g = np.random.Generator(np.random.Philox(a.seed + 7919 * rank))
     n = a.n
-    if a.workload == "ir" and a.kappa > 0:
+    if a.workload == "ir" and a.kappa > 0 and a.reflectors <= 0:
+        A = dense_randsvd_matrix(n, a.kappa, a.seed + 7919 * rank, torch)
+    elif a.workload == "ir" and a.kappa > 0:
         A = sigma_spectrum_matrix(n, a.kappa, a.reflectors, g, torch, np)
     else:
         A = torch.from_numpy(g.uniform(-1.0, 1.0, (n, n)))
@@ -707,6 +739,7 @@ def run_ours(a, world, rank, local):
     torch.cuda.synchronize()
     ctx.check()
     ir_method = ctx.ir_last_method() if a.workload == "ir" else None
+    ir_hist = ctx.ir_history() if a.workload == "ir" else None
     # accuracy of the last warm-up result (FP64 backward error, checked on the GPU)
     accuracy = {}
     if a.workload != "gemm":
@@ -865,7 +898,8 @@ def run_ours(a, world, rank, local):
         "tflops_whole_step": (2.0 * n * n * kk if a.workload == "gemm" else FLOPS[a.workload](n, nrhs)) * a.steps / t / 1e12,
         "host_enqueue_ms_per_step": host_enqueue_ms,
         "accuracy": accuracy,
-        "ir": ({**ir_stats, **(fp64_ref or {}), "method": {0: "rbt", 1: "gepp"}.get(ir_method, ir_method)}
+        "ir": ({**ir_stats, **(fp64_ref or {}), "method": {0: "rbt", 1: "gepp"}.get(ir_method, ir_method),
+                "berr_history": ir_hist}
                if a.workload == "ir" else None),
         "clocks": clk,
     }

@@ -148,6 +148,39 @@ void gemm_bibj(const double* A, const double* B, double* C, int biStart, int biE
 }
 
 // ---------------------------------------------------------------------------
+// Host threads for the oracle's large cases.  Only row ranges of the trailing
+// updates are split, at multiples of rawGemmBIBJSlice's 64-row tile, so every
+// element is computed by exactly the same instruction sequence as in the
+// single-threaded reference (the tile and 4-row grouping of a row depend only
+// on its offset from the start of its 64-row tile).  0 = all hardware threads.
+// ---------------------------------------------------------------------------
+int g_threads = 0;
+
+int oracle_threads() {
+  if (g_threads > 0) return g_threads;
+  const unsigned h = std::thread::hardware_concurrency();
+  return h > 0 ? (int)h : 1;
+}
+
+// fn(r0, r1) over [0, rows) in chunks whose starts are multiples of 64.
+template <class F>
+void par_rows(int rows, F fn) {
+  const int tiles = (rows + 63) / 64;
+  const int nt = std::min(oracle_threads(), tiles);
+  if (nt <= 1 || (long long)rows * 1 < 256) {
+    if (rows > 0) fn(0, rows);
+    return;
+  }
+  std::vector<std::thread> th;
+  const int per = (tiles + nt - 1) / nt;
+  for (int t = 0; t < nt; ++t) {
+    const int r0 = t * per * 64, r1 = std::min(rows, (t + 1) * per * 64);
+    if (r0 < r1) th.emplace_back([=] { fn(r0, r1); });
+  }
+  for (auto& x : th) x.join();
+}
+
+// ---------------------------------------------------------------------------
 // Packed-B GEMM: rawGemmBISlicePackedBK (K.hs:412-805).  B is packed into
 // kc x 8 panels per 64-row k slice (packB, K.hs:573-590); the 4x8 / 1x8
 // micro-kernels read the panels, columns past the last full 8-panel use the
@@ -350,20 +383,27 @@ void panel_lu_factor(double* A, int n, int nb, std::vector<int>& pk, std::vector
       const int mT = n - panelEnd, nT = n - panelEnd;
       // rawCopySubmatrixToDense (LU.hs:411-440): L21 and U12 as dense buffers
       bufL.resize((size_t)mT * actualNb);
-      for (int i = 0; i < mT; ++i)
-        for (int j = 0; j < actualNb; ++j)
-          bufL[(size_t)i * actualNb + j] = A[(size_t)(panelEnd + i) * n + k0 + j];
       bufU.resize((size_t)actualNb * nT);
       for (int i = 0; i < actualNb; ++i)
         for (int j = 0; j < nT; ++j) bufU[(size_t)i * nT + j] = A[(size_t)(k0 + i) * n + panelEnd + j];
-      bufC.assign((size_t)mT * nT, 0.0);  // rawZeroDoubles
-      gemm_kernel(bufL.data(), bufU.data(), bufC.data(), mT, actualNb, nT);
-      // rawSubtractFromStrided (LU.hs:444-476): a + (-c) == a - c
-      for (int i = 0; i < mT; ++i) {
-        double* arow = A + (size_t)(panelEnd + i) * n + panelEnd;
-        const double* crow = &bufC[(size_t)i * nT];
-        for (int j = 0; j < nT; ++j) arow[j] = arow[j] - crow[j];
-      }
+      bufC.resize((size_t)mT * nT);
+      // k = actualNb <= 32 < 96: rawGemmKernel takes the unpacked path
+      // (rawGemmBIBJSlice over all rows), split here by 64-row tiles
+      double* Lp = bufL.data();
+      double* Up = bufU.data();
+      double* Cp = bufC.data();
+      par_rows(mT, [=](int r0, int r1) {
+        for (int i = r0; i < r1; ++i)
+          for (int j = 0; j < actualNb; ++j) Lp[(size_t)i * actualNb + j] = A[(size_t)(panelEnd + i) * n + k0 + j];
+        std::memset(Cp + (size_t)r0 * nT, 0, (size_t)(r1 - r0) * nT * sizeof(double));  // rawZeroDoubles
+        gemm_bibj(Lp, Up, Cp, r0, r1, 0, nT, mT, actualNb, nT);
+        // rawSubtractFromStrided (LU.hs:444-476): a + (-c) == a - c
+        for (int i = r0; i < r1; ++i) {
+          double* arow = A + (size_t)(panelEnd + i) * n + panelEnd;
+          const double* crow = Cp + (size_t)i * nT;
+          for (int j = 0; j < nT; ++j) arow[j] = arow[j] - crow[j];
+        }
+      });
     }
     k0 = panelEnd;
   }
@@ -479,16 +519,23 @@ void panel_chol_factor(double* G, int n, int nb) {
     const int nBelow = n - j;
     if (j > 0) {
       bufA.resize((size_t)nBelow * j);  // rawCopyCholSubmatrix (Chol.hs:325-358)
-      for (int i = 0; i < nBelow; ++i)
-        std::memcpy(&bufA[(size_t)i * j], G + (size_t)(j + i) * n, (size_t)j * sizeof(double));
       bufBT.resize((size_t)j * jb);  // rawCopyCholTranspose (Chol.hs:363-384)
       for (int i = 0; i < jb; ++i)
         for (int c = 0; c < j; ++c) bufBT[(size_t)c * jb + i] = G[(size_t)(j + i) * n + c];
-      bufC.assign((size_t)nBelow * jb, 0.0);
-      gemm_kernel(bufA.data(), bufBT.data(), bufC.data(), nBelow, j, jb);
-      for (int i = 0; i < nBelow; ++i)  // rawCholSubtractPanel (Chol.hs:388-416)
-        for (int c = 0; c < jb; ++c)
-          G[(size_t)(j + i) * n + j + c] = G[(size_t)(j + i) * n + j + c] - bufC[(size_t)i * jb + c];
+      bufC.resize((size_t)nBelow * jb);
+      // n = jb <= 32 < 96: the unpacked path, split by 64-row tiles
+      double* Ap = bufA.data();
+      double* Bp = bufBT.data();
+      double* Cp = bufC.data();
+      const int jj = j;
+      par_rows(nBelow, [=](int r0, int r1) {
+        for (int i = r0; i < r1; ++i) std::memcpy(Ap + (size_t)i * jj, G + (size_t)(jj + i) * n, (size_t)jj * sizeof(double));
+        std::memset(Cp + (size_t)r0 * jb, 0, (size_t)(r1 - r0) * jb * sizeof(double));
+        gemm_bibj(Ap, Bp, Cp, r0, r1, 0, jb, nBelow, jj, jb);
+        for (int i = r0; i < r1; ++i)  // rawCholSubtractPanel (Chol.hs:388-416)
+          for (int c = 0; c < jb; ++c)
+            G[(size_t)(jj + i) * n + jj + c] = G[(size_t)(jj + i) * n + jj + c] - Cp[(size_t)i * jb + c];
+      });
     }
     for (int c = j; c < j + jb; ++c) chol_column_from(G, n, c, j);
     j += jb;
@@ -756,6 +803,71 @@ void orc_matvec_generic(const double* A, const double* x, double* y, int m, int 
     for (int j = 0; j < n; ++j) acc = acc + A[(size_t)i * n + j] * x[j];
     y[i] = acc;
   }
+}
+
+// Threads used by the row-parallel trailing updates (0 = all hardware threads).
+void orc_set_threads(int t) { g_threads = t; }
+
+// luNoPivot (LU.hs:196-214): outer-product LU without pivoting, in place,
+// GVL4 Algorithm 3.2.1.  For each k: multipliers a_ik / a_kk for the rows
+// below, then a_ij - a_ik * a_kj (separately rounded) for j > k, i > k, with
+// j the outer loop; the order inside one k does not change any value.
+void orc_lu_nopivot(double* A, int n) {
+  for (int k = 0; k <= n - 2; ++k) {
+    const double akk = A[(size_t)k * n + k];
+    for (int i = k + 1; i < n; ++i) A[(size_t)i * n + k] = A[(size_t)i * n + k] / akk;
+    for (int j = k + 1; j < n; ++j) {
+      const double akj = A[(size_t)k * n + j];
+      for (int i = k + 1; i < n; ++i) A[(size_t)i * n + j] = A[(size_t)i * n + j] - A[(size_t)i * n + k] * akj;
+    }
+  }
+}
+
+// choleskyGaxpy (Chol.hs:173-204), GVL4 Algorithm 4.2.2: G starts as the
+// lower triangle of A (zeros above); column j gets g_ij - g_ik * g_jk for
+// k = 0 .. j-1 in order, then every g_ij (i >= j) is divided by sqrt(g_jj).
+void orc_cholesky_gaxpy(const double* A, double* G, int n) {
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) G[(size_t)i * n + j] = (i >= j) ? A[(size_t)i * n + j] : 0.0;
+  for (int j = 0; j < n; ++j) {
+    for (int k = 0; k < j; ++k) {
+      const double gjk = G[(size_t)j * n + k];
+      for (int i = j; i < n; ++i) G[(size_t)i * n + j] = G[(size_t)i * n + j] - G[(size_t)i * n + k] * gjk;
+    }
+    const double sjj = std::sqrt(G[(size_t)j * n + j]);
+    for (int i = j; i < n; ++i) G[(size_t)i * n + j] = G[(size_t)i * n + j] / sjj;
+  }
+}
+
+// tridiagSolve (Solve/Banded.hs:292-342), GVL4 Algorithm 4.3.6: LDL^T of the
+// SPD tridiagonal (diag, supdiag[0..n-2]) folded with the substitutions.
+void orc_tridiag_solve(const double* diag, const double* supdiag, const double* b, double* x, int n) {
+  if (n <= 0) return;
+  std::vector<double> alpha(diag, diag + n), beta(n, 0.0);
+  for (int i = 0; i < n - 1; ++i) beta[i] = supdiag[i];
+  for (int i = 0; i < n; ++i) x[i] = b[i];
+  for (int k = 1; k < n; ++k) {  // t = beta(k-1), beta(k-1) = t / alpha(k-1), alpha(k) -= t * beta(k-1)
+    const double t = beta[k - 1];
+    const double bk1 = t / alpha[k - 1];
+    beta[k - 1] = bk1;
+    alpha[k] = alpha[k] - t * bk1;
+  }
+  for (int k = 1; k < n; ++k) x[k] = x[k] - beta[k - 1] * x[k - 1];
+  x[n - 1] = x[n - 1] / alpha[n - 1];
+  for (int k = n - 2; k >= 0; --k) x[k] = x[k] / alpha[k] - beta[k] * x[k + 1];
+}
+
+// normInf (Norms.hs:135-141): the largest row sum of |a_ij|, each row summed
+// as a left fold from 0 in column order.  vnormInf (Norms.hs:94-96) of x is
+// normInf of x as an n x 1 matrix.
+double orc_norm_inf(const double* A, int m, int n) {
+  double best = 0.0;
+  for (int i = 0; i < m; ++i) {
+    double acc = 0.0;
+    for (int j = 0; j < n; ++j) acc = acc + std::fabs(A[(size_t)i * n + j]);
+    best = (i == 0) ? acc : std::max(best, acc);
+  }
+  return best;
 }
 
 // Throughput helper for the CPU baseline: `count` independent luSolveP solves

@@ -53,12 +53,17 @@ def lib():
             "orc_matvec_generic": [_dp, _dp, _dp, i, i],
             "orc_lu_solve_p_many": [_dp, _dp, _dp, i, i, i],
             "orc_chol_solve_p_many": [_dp, _dp, _dp, i, i, i],
+            "orc_set_threads": [i],
+            "orc_lu_nopivot": [_dp, i],
+            "orc_cholesky_gaxpy": [_dp, _dp, i],
+            "orc_tridiag_solve": [_dp, _dp, _dp, _dp, i],
+            "orc_norm_inf": [_dp, i, i],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = ctypes.c_int if name in ("orc_lu_factor_p", "orc_lu_solve_p") else (
-                ctypes.c_double if name == "orc_det" else None)
+                ctypes.c_double if name in ("orc_det", "orc_norm_inf") else None)
         _LIB = L
     return _LIB
 
@@ -208,7 +213,44 @@ def chol_solve_generic(A, b):
     return x
 
 
-# --- BLAS-2 -----------------------------------------------------------------
+def set_threads(threads: int) -> None:
+    """Host threads of the row-parallel trailing updates (0 = all; bitwise the same result)."""
+    lib().orc_set_threads(int(threads))
+
+
+def lu_nopivot(A) -> np.ndarray:
+    """luNoPivot: packed unit-L / U without row interchanges."""
+    LU = _c(A).copy()
+    lib().orc_lu_nopivot(_d(LU), LU.shape[0])
+    return LU
+
+
+def cholesky_gaxpy(A) -> np.ndarray:
+    """choleskyGaxpy: G (lower, zeros above) by the gaxpy column loop."""
+    A = _c(A)
+    G = np.empty_like(A)
+    lib().orc_cholesky_gaxpy(_d(A), _d(G), A.shape[0])
+    return G
+
+
+def tridiag_solve(diag, supdiag, b) -> np.ndarray:
+    """tridiagSolve: SPD tridiagonal solve from the diagonal and superdiagonal
+    (length n, entries 0..n-2 used)."""
+    diag, supdiag, b = _c(diag), _c(supdiag), _c(b)
+    x = np.empty_like(b)
+    lib().orc_tridiag_solve(_d(diag), _d(supdiag), _d(b), _d(x), b.shape[0])
+    return x
+
+
+# --- BLAS-2 and norms ---------------------------------------------------------
+
+def norm_inf(A) -> float:
+    """normInf: largest row sum of |a_ij| (each row a left fold in column order)."""
+    A = _c(A)
+    if A.ndim == 1:
+        A = A.reshape(-1, 1)
+    return lib().orc_norm_inf(_d(A), A.shape[0], A.shape[1])
+
 
 def matvec_p(A, x):
     A, x = _c(A), _c(x)
