@@ -7,12 +7,12 @@ Workloads (--workload):
         work buffer (luSolveP's thaw), LU with partial pivoting, solve.
   chol  choleskySolve with A = B B^T + n I, B uniform[-1,1].
   gemm  C = A B, m = n = k.
-  ir    (default) mixed precision: random butterflies + FP32 LU without
-        pivoting with tcgen05 3xTF32 updates (partial pivoting if refinement
-        stalls), refined in FP64 to the normwise backward error 1e-15 n;
-        A = U diag(sigma) V^T with U, V products of seeded Householder
-        reflectors and sigma geometric from 1 to 1/kappa (--kappa; 0 =
-        uniform[-1,1] A).  The plain FP64 LU solve of the same system is timed
+  ir    (default) mixed precision: FP32 LU with partial pivoting and
+        tcgen05 3xTF32 updates, refined in FP64 to the normwise backward error
+        1e-15 n; A = U diag(sigma) V^T with U, V dense random orthogonal (Q
+        factors of seeded Gaussian matrices; --reflectors k > 0 uses k seeded
+        Householder reflectors per side instead) and sigma geometric from 1 to
+        1/kappa (--kappa; 0 = uniform[-1,1] A).  The plain FP64 LU solve of the same system is timed
         beside it (the metric's comparison).
 The timed region replays the solve's captured CUDA graphs; per-kernel CUDA
 events (the roofline's kernel time and the phase breakdown) come from
@@ -104,7 +104,8 @@ def workload_name(a):
                     f"(Q of seeded Gaussian, n Householder reflectors each)")
         else:
             spec = f"A = U diag(sigma) V^T, kappa={a.kappa:g}, {a.reflectors} Householder reflectors per side"
-        return f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU + 3xTF32 tcgen05, FP64 refinement"
+        return (f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU with partial pivoting + 3xTF32 "
+                f"tcgen05 updates, FP64 refinement")
     if a.workload == "lu":
         return f"luSolve FP64 n={a.n} nrhs={a.nrhs}, A uniform[-1,1]"
     if a.workload == "chol":

@@ -176,15 +176,19 @@ int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const dou
 
 /* Factorisation used by the mixed-precision solves of a context (lm_dgesv_ir,
  * lm_lu_solve_ir_host and the serving loop's large requests).
- *   LM_IR_RBT (default): A is mixed by two random depth-2 butterfly
- *     transforms, Ar = U^T A V (Baboulin, Dongarra, Herrmann, Tomov 2013), and
- *     Ar is factored in FP32 without pivoting, so that everything but the
- *     128 x 128 diagonal blocks runs on the tensor cores; corrections are
- *     V Ar^-1 U^T r.  If its refinement stalls (two steps in a row do not
- *     reduce the worst backward error, or its contraction rate cannot reach
- *     tol within max_iter) or runs out of steps, the solve is redone with
- *     LM_IR_GEPP, and only that result is reported.
- *   LM_IR_GEPP: FP32 LU with partial pivoting, as described above.
+ *   LM_IR_GEPP (default): FP32 LU with partial pivoting (the FP64 path's pivot
+ *     rule), every Schur-complement update as 3xTF32 on the tensor cores, with
+ *     look-ahead; the FP32 substitutions solve their diagonal blocks by
+ *     substitution, so each correction is backward stable in FP32.
+ *   LM_IR_RBT: A is mixed by two random depth-2 butterfly transforms,
+ *     Ar = U^T A V (Baboulin, Dongarra, Herrmann, Tomov 2013), and Ar is
+ *     factored in FP32 without pivoting, so that everything but the 128 x 128
+ *     diagonal blocks runs on the tensor cores; corrections are V Ar^-1 U^T r.
+ *     Fast on matrices whose leading blocks stay well conditioned, but without
+ *     pivoting it stalls on dense ill-conditioned ones: if its refinement
+ *     stalls (two steps in a row do not reduce the worst backward error, or its
+ *     contraction rate cannot reach tol within max_iter) or runs out of steps,
+ *     the solve is redone with LM_IR_GEPP, and only that result is reported.
  * The stopping test, tolerance and FP64 residual are the same for both. */
 #define LM_IR_RBT 0
 #define LM_IR_GEPP 1

@@ -50,7 +50,7 @@ struct Ctx {
   void* ws[kWsSlots] = {};
   size_t ws_bytes[kWsSlots] = {};
   std::mutex mu;
-  int ir_method = LM_IR_RBT;  // lm_ctx_set_ir_method
+  int ir_method = LM_IR_GEPP;  // lm_ctx_set_ir_method
   int ir_last = -1;           // method of the last mixed-precision result
   std::vector<double> ir_hist;  // worst backward error after each refinement step (ctx_ir_history)
   // batch kernel panel width per precision and size bucket (lm_batch_tune)
@@ -602,9 +602,9 @@ int finish_info(Ctx& c, int* info) {
   return r;
 }
 
-// Mixed-precision solve with the context's method: the randomised
-// no-pivoting factor first (LM_IR_RBT), partial pivoting when its refinement
-// stalls.  A zero pivot of the randomised factor only triggers the fallback;
+// Mixed-precision solve with the context's method: partial pivoting
+// (LM_IR_GEPP, the default), or the randomised no-pivoting factor first
+// (LM_IR_RBT) with partial pivoting when its refinement stalls.  A zero pivot of the randomised factor only triggers the fallback;
 // the reported info is that of the method whose result is returned.
 int ir_solve(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters, double* berr, const char* tag) {

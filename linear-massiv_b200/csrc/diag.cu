@@ -145,7 +145,15 @@ __device__ void inv_lower_smem(T* S, T* tmp, bool unit, bool half, int t, int ba
   if (!half) inv_combine<T, 64>(S, tmp, t, bar);
 }
 
-__device__ __forceinline__ float tf32_hi_part(float a) { return __uint_as_float(__float_as_uint(a) & 0xFFFFE000u); }
+// High part of the 3xTF32 split: a rounded to the nearest TF32 value (ties
+// away from zero), so that the remainder a - hi is exact in FP32 and at most
+// 2^-11 |a|; the remainder is rounded the same way before it is stored, and
+// the tensor core then reads both parts without further loss.
+__device__ __forceinline__ float tf32_hi_part(float a) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
+  return __uint_as_float(r);
+}
 
 // Xout (w x w, ldx) <- inv(lower triangle of L) with zeros above the
 // diagonal; for FP32 with `lo` given, Xout receives the TF32 high part and
@@ -217,7 +225,7 @@ __global__ void __launch_bounds__(512, 1)
       if (lo) {
         const float h = tf32_hi_part(v);
         Xout[(long long)i * ldx + j] = h;
-        lo[(long long)i * ldx + j] = v - h;
+        lo[(long long)i * ldx + j] = tf32_hi_part(v - h);
         continue;
       }
     }
@@ -347,9 +355,9 @@ __global__ void __launch_bounds__(512, 1)
     const float uf = (j <= i) ? S[j * DLD + i] : 0.f;
     const float lh = tf32_hi_part(lf), uh = tf32_hi_part(uf);
     LFhi[(long long)i * ldi + j] = lh;
-    LFlo[(long long)i * ldi + j] = lf - lh;
+    LFlo[(long long)i * ldi + j] = tf32_hi_part(lf - lh);
     UFThi[(long long)i * ldi + j] = uh;
-    UFTlo[(long long)i * ldi + j] = uf - uh;
+    UFTlo[(long long)i * ldi + j] = tf32_hi_part(uf - uh);
   }
 }
 
@@ -420,7 +428,7 @@ __global__ void __launch_bounds__(512, 1)
         if (i < w && j < w) {
           const float lh = tf32_hi_part(li);
           Lhi[(long long)i * ldi + j] = lh;
-          Llo[(long long)i * ldi + j] = li - lh;
+          Llo[(long long)i * ldi + j] = tf32_hi_part(li - lh);
         }
       } else {
         const float ut = (j <= i) ? (float)S[i * DLD + j] : 0.f;  // inv(U)^T(i, j)
@@ -428,7 +436,7 @@ __global__ void __launch_bounds__(512, 1)
         if (i < w && j < w) {
           const float uh = tf32_hi_part(ut);
           UThi[(long long)i * ldi + j] = uh;
-          UTlo[(long long)i * ldi + j] = ut - uh;
+          UTlo[(long long)i * ldi + j] = tf32_hi_part(ut - uh);
         }
       }
     }

@@ -61,11 +61,13 @@ template <typename T>
 int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaStream_t st);
 // X (n x nrhs) <- U^-1 L^-1 X, two persistent launches per pass (FP64:
 // nrhs <= 4; FP32: any nrhs, in passes of 16 beyond 4); `sync` is 4 ints of
-// device scratch.  FP32: corr (two flags per 128-row block: L, U), when
-// given, limits the diagonal-block correction step to flagged blocks.
+// device scratch.  FP64, and FP32 with `exact`, solve the diagonal blocks by
+// substitution; FP32 otherwise multiplies by the block inverses, and corr
+// (two flags per 128-row block: L, U), when given, limits the diagonal-block
+// correction step to flagged blocks.
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-            int* sync, int* status, cudaStream_t st, const int* corr = nullptr);
+            int* sync, int* status, cudaStream_t st, const int* corr = nullptr, bool exact = false);
 
 // --- FP64 GEMM (dgemm.cu) ----------------------------------------------------
 // C = alpha * op(A) * op(B) + beta * C, row-major.

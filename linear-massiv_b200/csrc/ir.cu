@@ -45,10 +45,18 @@ __global__ void d2s_kernel(float* dst, long long ldd, const double* src, long lo
   }
 }
 
-__device__ __forceinline__ float tf32_hi(float a) { return __uint_as_float(__float_as_uint(a) & 0xFFFFE000u); }
+// High part of the 3xTF32 split: a rounded to the nearest TF32 value (ties
+// away from zero), so that the remainder a - hi is exact in FP32 and at most
+// 2^-11 |a|; the remainder is rounded the same way before it is stored, and
+// the tensor core then reads both parts without further loss.
+__device__ __forceinline__ float tf32_hi(float a) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
+  return __uint_as_float(r);
+}
 
-// Split for 3xTF32: hi = a with the 13 low mantissa bits cleared (exactly
-// representable in TF32), lo = a - hi (exact in FP32).
+// Split for 3xTF32: hi = a rounded to TF32, lo = a - hi (exact in FP32)
+// rounded to TF32; hi + lo carries a to within 2^-22 |a|.
 // dst_hi/dst_lo (cols x rows) = split(src (rows x cols))^T.
 // With `gate` given and *gate == 0 nothing is written (a correction step
 // switched off on the device, inside a captured sequence, whose consumers are
@@ -75,7 +83,7 @@ __global__ void transpose_split_kernel(float* dhi, float* dlo, long long ldd, co
       const float a = tile[threadIdx.x][j];
       const float h = tf32_hi(a);
       dhi[(long long)r * ldd + c] = h;
-      dlo[(long long)r * ldd + c] = a - h;
+      dlo[(long long)r * ldd + c] = tf32_hi(a - h);
     }
   }
 }
@@ -93,7 +101,7 @@ __global__ void split_kernel(float* dhi, float* dlo, long long ldd, const float*
     if (cpy != nullptr) cpy[(long long)r * ldc + c] = a;
     const float h = tf32_hi(a);
     dhi[(long long)r * ldd + c] = h;
-    dlo[(long long)r * ldd + c] = a - h;
+    dlo[(long long)r * ldd + c] = tf32_hi(a - h);
   }
 }
 
@@ -174,7 +182,7 @@ struct SScratch {
 // in one fused FP32 launch; otherwise the inverse of the diagonal block (one
 // CTA) times B on the tensor cores as 3xTF32.
 int s_trsm_unit_lower(Ctx& c, const float* L11, long long lda, int w, float* B, long long ldb, int ncols,
-                      SScratch& s, cudaStream_t st) {
+                      SScratch& s, cudaStream_t st, int max_ctas = 0) {
   if (w <= 0 || ncols <= 0) return LM_OK;
   if (w <= 64 && ncols <= 128) {
     Prof p(c, kPhaseTrsm, (double)w * w * ncols, 4.0 * ((double)w * w / 2 + 2.0 * w * ncols), st);
@@ -188,22 +196,24 @@ int s_trsm_unit_lower(Ctx& c, const float* L11, long long lda, int w, float* B, 
   transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, B, ldb, w, ncols);
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());
-  return sgemm_tf32(c, w, ncols, w, 1.0f, s.Lhi, kNB, s.Bhi, s.ld, 0.0f, B, ldb, st, s.Llo, s.Blo);
+  return sgemm_tf32(c, w, ncols, w, 1.0f, s.Lhi, kNB, s.Bhi, s.ld, 0.0f, B, ldb, st, s.Llo, s.Blo, max_ctas);
 }
 
 int s_update(Ctx& c, int m, int n, int k, float* A21, long long lda, const float* U12, float* C, SScratch& s,
-             cudaStream_t st) {
+             cudaStream_t st, int max_ctas = 0) {
   // C -= A21 (m x k) * U12 (k x n), as 3xTF32 on the tensor cores
   dim3 tb(32, 8), tg(cdiv(n, 32), cdiv(k, 32));
   transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, U12, lda, k, n);
   split_kernel<<<grid_of((long long)m * k), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, k);
   count_launch(2);
   LM_CUDA_TRY(cudaGetLastError());
-  return sgemm_tf32(c, m, n, k, -1.0f, s.Ahi, s.ld, s.Bhi, s.ld, 1.0f, C, lda, st, s.Alo, s.Blo);
+  return sgemm_tf32(c, m, n, k, -1.0f, s.Ahi, s.ld, s.Bhi, s.ld, 1.0f, C, lda, st, s.Alo, s.Blo, max_ctas);
 }
 
+// max_ctas caps the grids of the panel's own GEMMs (0 = no cap), so that a
+// panel factored beside a trailing update fits on the SMs that update leaves.
 int sgetrf_panel_rec(Ctx& c, float* A, long long lda, int n, int c0, int w, int pc0, int pw, int* ipiv, SScratch& s,
-                     cudaStream_t st) {
+                     cudaStream_t st, int max_ctas = 0) {
   const int R = n - c0;
   const int wmax = panel_leaf_max_width_for(c, R);
   if (wmax <= 0) return LM_ERR_UNSUPPORTED;
@@ -214,40 +224,87 @@ int sgetrf_panel_rec(Ctx& c, float* A, long long lda, int n, int c0, int w, int 
   int w1 = (w >= 16) ? std::max(8, (w / 2) & ~7) : std::max(4, (w / 2) & ~3);
   if (w1 >= w) w1 = w - 4;
   const int w2 = w - w1;
-  LM_TRY(sgetrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st));
+  LM_TRY(sgetrf_panel_rec(c, A, lda, n, c0, w1, pc0, pw, ipiv, s, st, max_ctas));
   float* A11 = A + (long long)c0 * lda + c0;
-  LM_TRY(s_trsm_unit_lower(c, A11, lda, w1, A11 + w1, lda, w2, s, st));
-  LM_TRY(s_update(c, R - w1, w2, w1, A11 + (long long)w1 * lda, lda, A11 + w1, A11 + (long long)w1 * lda + w1, s, st));
-  return sgetrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st);
+  LM_TRY(s_trsm_unit_lower(c, A11, lda, w1, A11 + w1, lda, w2, s, st, max_ctas));
+  LM_TRY(s_update(c, R - w1, w2, w1, A11 + (long long)w1 * lda, lda, A11 + w1, A11 + (long long)w1 * lda + w1, s, st,
+                  max_ctas));
+  return sgetrf_panel_rec(c, A, lda, n, c0 + w1, w2, pc0, pw, ipiv, s, st, max_ctas);
 }
 
-}  // namespace
-
-int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
-  void* ws = nullptr;
-  SScratch s;
+// Split-operand scratch set carved from `p` (4 n x 128 + 2 128 x 128 floats,
+// then the interchange plan); returns the end of the set.
+char* carve_scratch(SScratch& s, char* p, int n) {
   s.ld = kNB;
-  LM_TRY(ctx_workspace(c, 1, sizeof(float) * (4 * (size_t)n * kNB + 2 * (size_t)kNB * kNB) + sizeof(int) * kSwapPlanInts,
-                       &ws));
-  s.Ahi = static_cast<float*>(ws);
+  s.Ahi = reinterpret_cast<float*>(p);
   s.Alo = s.Ahi + (size_t)n * kNB;
   s.Bhi = s.Alo + (size_t)n * kNB;
   s.Blo = s.Bhi + (size_t)n * kNB;
   s.Lhi = s.Blo + (size_t)n * kNB;
   s.Llo = s.Lhi + (size_t)kNB * kNB;
   s.plan = reinterpret_cast<int*>(s.Llo + (size_t)kNB * kNB);
+  return reinterpret_cast<char*>(s.plan) + ((sizeof(int) * kSwapPlanInts + 255) / 256) * 256;
+}
+
+size_t scratch_set_bytes(int n) {
+  return sizeof(float) * (4 * (size_t)n * kNB + 2 * (size_t)kNB * kNB) + ((sizeof(int) * kSwapPlanInts + 255) / 256) * 256;
+}
+
+// SMs left to a panel factored beside the trailing update (the widest panel
+// leaf is a cluster of 16 CTAs of one SM each), and the order from which that
+// look-ahead is used.
+constexpr int kSLookaheadSms = 16;
+constexpr int kSLookaheadMinN = 2048;
+
+}  // namespace
+
+// FP32 LU with partial pivoting (the same pivot rule as the FP64 path), 128-
+// column panels factored by cluster leaves, U12 = inv(L11) A12 and every
+// Schur-complement update as 3xTF32 on tcgen05.  Look-ahead as in dgetrf:
+// once the next panel's columns are updated, that panel is factored on the
+// priority stream (its own GEMMs capped to the SMs left free) while the rest
+// of the trailing update runs; its interchanges reach the columns right of it
+// after the join.  The two streams use separate split-operand scratch.
+int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
+  const int nsm = ctx_num_sms(c);
+  const bool la = n >= kSLookaheadMinN && nsm > 2 * kSLookaheadSms;
+  void* ws = nullptr;
+  LM_TRY(ctx_workspace(c, 1, (la ? 2 : 1) * scratch_set_bytes(n), &ws));
+  SScratch s, sa;
+  char* p = carve_scratch(s, static_cast<char*>(ws), n);
+  if (la) carve_scratch(sa, p, n);
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  if (la) LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
+  LM_TRY(sgetrf_panel_rec(c, A, lda, n, 0, std::min(kNB, n), 0, std::min(kNB, n), ipiv, s, st));
   for (int k0 = 0; k0 < n; k0 += kNB) {
     const int w = std::min(kNB, n - k0);
-    LM_TRY(sgetrf_panel_rec(c, A, lda, n, k0, w, k0, w, ipiv, s, st));
     {
-      Prof p(c, kPhaseSwap, 0.0, 16.0 * w * (n - w), st);
+      Prof p2(c, kPhaseSwap, 0.0, 16.0 * w * (n - w), st);
       LM_TRY(laswp<float>(A, lda, n, ipiv, k0, k0 + w, 0, k0, k0 + w, n, ctx_status(c), st, s.plan));
     }
-    if (k0 + w < n) {
-      float* A11 = A + (long long)k0 * lda + k0;
-      LM_TRY(s_trsm_unit_lower(c, A11, lda, w, A11 + w, lda, n - k0 - w, s, st));
-      LM_TRY(s_update(c, n - k0 - w, n - k0 - w, w, A11 + (long long)w * lda, lda, A11 + w,
-                      A11 + (long long)w * lda + w, s, st));
+    if (k0 + w >= n) break;
+    const int m = n - k0 - w;
+    const int wn = std::min(kNB, m);  // next panel
+    float* A11 = A + (long long)k0 * lda + k0;
+    LM_TRY(s_trsm_unit_lower(c, A11, lda, w, A11 + w, lda, m, s, st));
+    // A22 -= L21 U12: the next panel's columns first
+    LM_TRY(s_update(c, m, wn, w, A11 + (long long)w * lda, lda, A11 + w, A11 + (long long)w * lda + w, s, st));
+    const int rest = m - wn;
+    if (la) {
+      LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
+      LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
+      LM_TRY(sgetrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, sa, aux, kSLookaheadSms));
+      LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
+      if (rest > 0)
+        LM_TRY(s_update(c, m, rest, w, A11 + (long long)w * lda, lda, A11 + w + wn, A11 + (long long)w * lda + w + wn,
+                        s, st, nsm - kSLookaheadSms));
+      LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+    } else {
+      if (rest > 0)
+        LM_TRY(s_update(c, m, rest, w, A11 + (long long)w * lda, lda, A11 + w + wn, A11 + (long long)w * lda + w + wn,
+                        s, st));
+      LM_TRY(sgetrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, st));
     }
   }
   return LM_OK;
@@ -400,32 +457,25 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   const size_t r_bytes = sizeof(double) * (size_t)n * ldr;
   const size_t d_bytes = sizeof(float) * (size_t)n * ldr;
   const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(2 + 3 * 64);  // 16-byte multiple
-  const size_t inv_elems = trsv_inv_elems<float>(n);
-  const size_t inv_bytes = 2 * sizeof(float) * inv_elems;  // diagonal-block inverses of L and U
   const size_t sync_bytes = 64;
   const size_t w_bytes = sizeof(float) * (size_t)n * ldr;  // gather scratch of the interchanges
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes + sync_bytes + w_bytes,
-                       &ws));
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + sync_bytes + w_bytes, &ws));
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   int* ipiv = reinterpret_cast<int*>(p + a32_bytes);
   double* R = reinterpret_cast<double*>(p + a32_bytes + piv_bytes);
   float* D = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes);
   unsigned long long* nrm = reinterpret_cast<unsigned long long*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes);
-  float* DinvL = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes);
-  float* DinvU = DinvL + inv_elems;
-  int* tsync = reinterpret_cast<int*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes);
-  float* Wg = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + inv_bytes +
-                                       sync_bytes);
+  int* tsync = reinterpret_cast<int*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes);
+  float* Wg = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + sync_bytes);
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
 
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
   // factor fl32(A)
   LM_TRY(run("factor", [&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
-    LM_TRY(sgetrf(c, n, A32, lda32, ipiv, s));
-    return tri_inv_blocks<float>(A32, lda32, n, DinvL, DinvU, s);
+    return sgetrf(c, n, A32, lda32, ipiv, s);
   }));
   return refine(c, n, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, false, R, ldr, D, nrm, iters_out, berr_out, st, run,
                 [&](float* Dd, cudaStream_t s) {
@@ -433,8 +483,12 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
                     Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
                     LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
                   }
+                  // diagonal blocks by substitution: with partial pivoting U's
+                  // blocks carry the small pivots of an ill-conditioned A, and a
+                  // product with their inverse would not be backward stable
                   Prof pt(c, kPhaseTrsm, 2.0 * n * n * nrhs, 4.0 * n * n, s);
-                  return trsv_lu<float>(A32, lda32, n, nrhs, DinvL, DinvU, Dd, ldr, tsync, ctx_status(c), s);
+                  return trsv_lu<float>(A32, lda32, n, nrhs, nullptr, nullptr, Dd, ldr, tsync, ctx_status(c), s,
+                                        nullptr, true);
                 });
 }
 

@@ -45,23 +45,24 @@ struct TrsvCfg;
 template <>
 struct TrsvCfg<float> {
   static constexpr int BS = 128, NT = 512, VEC = 4;  // VEC elements per 16-byte load
-  static constexpr bool EXACT = false;               // diagonal block by its inverse
 };
 template <>
 struct TrsvCfg<double> {
   static constexpr int BS = 64, NT = 256, VEC = 2;
-  static constexpr bool EXACT = true;                // diagonal block by substitution
 };
 
-// Shared memory of trsv_kernel: the diagonal block only when it is solved by
-// substitution.
-template <typename T, bool EXACT>
+// Dynamic shared memory of trsv_kernel when the diagonal block is solved by
+// substitution.  Lane l of the solving warp owns the RPL consecutive rows
+// RPL l .. RPL l + RPL - 1; the block is stored as RPL x RPL tiles, tile (l, s)
+// (rows of lane l, columns of lane s) at tile index s * 32 + l, padded so that
+// the 16-byte loads of one tile row by consecutive lanes hit distinct banks.
+template <typename T>
 struct TrsvDiag {
-  T t[TrsvCfg<T>::BS][TrsvCfg<T>::BS + 1];
+  static constexpr int RPL = TrsvCfg<T>::BS / 32;
+  static constexpr int TS = RPL * RPL + 16 / (int)sizeof(T);  // tile stride in elements
+  T tile[32 * 32 * TS];
   T rdiag[TrsvCfg<T>::BS];  // 1 / T_kk, formed before the first wait
 };
-template <typename T>
-struct TrsvDiag<T, false> {};
 
 __device__ __forceinline__ int ld_acquire(const int* p) {
   int v;
@@ -152,26 +153,29 @@ __device__ __forceinline__ void load_row_share(T* out, const T* src, int c0, int
 // One direction of the blocked substitution.  forward: L unit lower, blocks in
 // increasing order; backward: U upper, blocks in decreasing order.
 // sync[0] = progress counter, sync[1] = ticket dispenser (both zero at launch).
-// corr (FP32 only): per-block flags at stride 2; when given, the correction
-// step on the diagonal block runs only for blocks whose flag is set.  The
-// 16-column variant never takes the correction step.
-template <typename T, int RHS>
+// EXACT: the diagonal block is solved by substitution (backward stable, as
+// the reference's substitutions are); otherwise it is multiplied by its
+// precomputed inverse Dinv.
+// corr (inverse form only): per-block flags at stride 2; when given, the
+// correction step on the diagonal block runs only for blocks whose flag is
+// set.  The 16-column variant never takes the correction step.
+template <typename T, int RHS, bool EXACT>
 __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
                                                              int nrhs, int forward, const T* __restrict__ Dinv,
                                                              T* X, long long ldx, int* sync, int* status,
                                                              int vec_ok, const int* corr) {
   constexpr int MAX_RHS = RHS;
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
-  constexpr bool EXACT = TrsvCfg<T>::EXACT;
+  constexpr int RPL = BS / 32;  // rows per lane of the one-warp substitution
   static_assert(NT == 4 * BS, "four threads per row");
-  static_assert(!EXACT || BS == 64, "the one-warp substitution holds two rows per lane");
   __shared__ int tk_sh, prog_sh;
   // rows padded by one element: the four threads of a row read columns 4 q
   // apart, which an unpadded power-of-two row length puts in one bank
   constexpr int XS = MAX_RHS + 1;
   __shared__ T xj[2][BS][XS];
   __shared__ T ys[BS][XS];
-  __shared__ TrsvDiag<T, EXACT> diag;
+  extern __shared__ __align__(16) unsigned char trsv_dyn[];
+  TrsvDiag<T>& diag = *reinterpret_cast<TrsvDiag<T>*>(trsv_dyn);
   const int nb = (n + BS - 1) / BS;
   if (threadIdx.x == 0) tk_sh = atomicAdd(sync + 1, 1);
   __syncthreads();
@@ -191,6 +195,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
   if constexpr (EXACT) {
     // T_bb with the unit (forward) or the stored (backward) diagonal; the
     // padding of a ragged last block is the identity.
+    constexpr int TS = TrsvDiag<T>::TS;
     for (int i = threadIdx.x; i < BS * BS; i += NT) {
       const int rr = i / BS, cc = i % BS;
       T v = T(0);
@@ -200,7 +205,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
       } else if (rr == cc) {
         v = T(1);
       }
-      diag.t[rr][cc] = v;
+      diag.tile[((cc / RPL) * 32 + rr / RPL) * TS + (rr % RPL) * RPL + cc % RPL] = v;
       if (rr == cc) diag.rdiag[rr] = T(1) / v;
     }
   } else {
@@ -258,48 +263,76 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
     for (int h = 0; h < MAX_RHS; ++h) ys[r][h] = row_ok ? rhs[h] - acc[h] : T(0);
   __syncthreads();
   if constexpr (EXACT) {
-    // warp 0: column-sweep substitution, lane l holding rows l and l + 32
+    // warp 0: blocked column sweep in 32 dependent steps of RPL rows.  Step s:
+    // lane s solves its RPL x RPL diagonal tile exactly (sequentially, in
+    // registers), the RPL values go to every lane by shuffles, and the lanes
+    // on the unsolved side subtract tile (l, s) times them from their rows.
     if (threadIdx.x < 32) {
+      constexpr int TS = TrsvDiag<T>::TS;
       const int l = threadIdx.x;
-      T y0[MAX_RHS], y1[MAX_RHS];
+      T y[RPL][MAX_RHS];
 #pragma unroll
-      for (int h = 0; h < MAX_RHS; ++h) y0[h] = ys[l][h], y1[h] = ys[l + 32][h];
+      for (int i = 0; i < RPL; ++i)
+#pragma unroll
+        for (int h = 0; h < MAX_RHS; ++h) y[i][h] = ys[RPL * l + i][h];
+      T rd[RPL];
+#pragma unroll
+      for (int i = 0; i < RPL; ++i) rd[i] = forward ? T(1) : diag.rdiag[RPL * l + i];
       // (nrhs is uniform across the warp, so the guarded shuffles are too)
-      if (forward) {
-        for (int k = 0; k < BS; ++k) {
-          const T a0 = diag.t[l][k], a1 = diag.t[l + 32][k];
+#pragma unroll 1
+      for (int st = 0; st < 32; ++st) {
+        const int sl = forward ? st : 31 - st;  // lane whose rows are solved now
+        // tile (l, sl): this lane's rows, the solved lane's columns
+        T tl[RPL][RPL];
+        const T* tp = diag.tile + (sl * 32 + l) * TS;
 #pragma unroll
-          for (int h = 0; h < MAX_RHS; ++h)
-            if (h < nrhs) {
-              const T xk = __shfl_sync(0xffffffffu, k < 32 ? y0[h] : y1[h], k & 31);
-              if (l > k) y0[h] = fma(-a0, xk, y0[h]);
-              if (l + 32 > k) y1[h] = fma(-a1, xk, y1[h]);
-            }
-        }
-      } else {
-        // x_k = y_k / T_kk as a product with the reciprocal formed off the
-        // critical path (within one rounding of the quotient)
-        for (int k = BS - 1; k >= 0; --k) {
-          const T a0 = diag.t[l][k], a1 = diag.t[l + 32][k], rk = diag.rdiag[k];
+        for (int i = 0; i < RPL; ++i)
 #pragma unroll
-          for (int h = 0; h < MAX_RHS; ++h)
-            if (h < nrhs) {
-              const T xk = __shfl_sync(0xffffffffu, k < 32 ? y0[h] : y1[h], k & 31) * rk;
-              if (l == (k & 31)) {
-                if (k < 32) y0[h] = xk;
-                else y1[h] = xk;
+          for (int j = 0; j < RPL; ++j) tl[i][j] = tp[i * RPL + j];
+        if (l == sl) {
+          // the diagonal tile, solved in place: forward unit lower, backward upper
+          if (forward) {
+#pragma unroll
+            for (int i = 1; i < RPL; ++i)
+#pragma unroll
+              for (int j = 0; j < i; ++j)
+#pragma unroll
+                for (int h = 0; h < MAX_RHS; ++h) y[i][h] = fma(-tl[i][j], y[j][h], y[i][h]);
+          } else {
+#pragma unroll
+            for (int i = RPL - 1; i >= 0; --i)
+#pragma unroll
+              for (int h = 0; h < MAX_RHS; ++h) {
+                T v = y[i][h];
+#pragma unroll
+                for (int j = i + 1; j < RPL; ++j) v = fma(-tl[i][j], y[j][h], v);
+                y[i][h] = v * rd[i];
               }
-              if (l < k) y0[h] = fma(-a0, xk, y0[h]);
-              if (l + 32 < k) y1[h] = fma(-a1, xk, y1[h]);
-            }
+          }
         }
+#pragma unroll
+        for (int h = 0; h < MAX_RHS; ++h)
+          if (h < nrhs) {
+            T xv[RPL];
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) xv[j] = __shfl_sync(0xffffffffu, y[j][h], sl);
+            if (forward ? l > sl : l < sl) {
+#pragma unroll
+              for (int i = 0; i < RPL; ++i) {
+                T v = y[i][h];
+#pragma unroll
+                for (int j = 0; j < RPL; ++j) v = fma(-tl[i][j], xv[j], v);
+                y[i][h] = v;
+              }
+            }
+          }
       }
 #pragma unroll
       for (int h = 0; h < MAX_RHS; ++h)
-        if (h < nrhs) {
-          if (l < rows) X[(long long)(r0 + l) * ldx + h] = y0[h];
-          if (l + 32 < rows) X[(long long)(r0 + l + 32) * ldx + h] = y1[h];
-        }
+        if (h < nrhs)
+#pragma unroll
+          for (int i = 0; i < RPL; ++i)
+            if (RPL * l + i < rows) X[(long long)(r0 + RPL * l + i) * ldx + h] = y[i][h];
     }
   } else {
     // x_b = inv(T_bb) y, then one correction x_b += inv(T_bb) (y - T_bb x_b):
@@ -409,43 +442,64 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
   return LM_OK;
 }
 
-// X (n x nrhs) <- U^-1 L^-1 X with the packed factor and (FP32) its block
-// inverses; FP64 ignores DinvL / DinvU and takes nrhs <= 4, FP32 takes any
-// nrhs (more than 4 in passes of 16 columns).  `sync` holds 4 ints of device
-// scratch.  FP32: corr, when given, holds two flags per diagonal block (L, U);
-// only flagged blocks take the correction step, all blocks do without it.
-// Passes of the 16-column variant (nrhs > 4) multiply by the inverse only.
+// X (n x nrhs) <- U^-1 L^-1 X with the packed factor.  FP64 and FP32 with
+// `exact` solve the diagonal blocks by substitution (DinvL / DinvU unused);
+// FP32 otherwise multiplies by the block inverses DinvL / DinvU.  FP64 takes
+// nrhs <= 4; FP32 any nrhs (more than 4 in passes of 16 columns).  `sync`
+// holds 4 ints of device scratch.  corr (inverse form), when given, holds two
+// flags per diagonal block (L, U); only flagged blocks take the correction
+// step, all blocks do without it.  Passes of the 16-column variant multiply by
+// the inverse only.
+template <typename T, int RHS, bool EXACT>
+int trsv_pass(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
+              int* sync, int* status, cudaStream_t st, const int* corr, int vec_ok) {
+  constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT;
+  const int nb = (n + BS - 1) / BS;
+  const int smem = EXACT ? (int)sizeof(TrsvDiag<T>) : 0;
+  if (EXACT) {
+    static bool attr_set[kMaxDevices] = {};
+    int dev = 0;
+    LM_CUDA_TRY(cudaGetDevice(&dev));
+    if (!attr_set[dev]) {
+      LM_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<T, RHS, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      attr_set[dev] = true;
+    }
+  }
+  LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
+  trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok, corr);
+  trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok,
+                                                   corr ? corr + 1 : nullptr);
+  count_launch(2);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-            int* sync, int* status, cudaStream_t st, const int* corr) {
-  constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC;
+            int* sync, int* status, cudaStream_t st, const int* corr, bool exact) {
+  constexpr int VEC = TrsvCfg<T>::VEC;
   if (n <= 0 || nrhs <= 0) return LM_OK;
-  if (!TrsvCfg<T>::EXACT && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
+  constexpr bool kF64 = sizeof(T) == 8;
+  exact = exact || kF64;
+  if (!exact && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
     return LM_ERR_ARG;
-  const int nb = (n + BS - 1) / BS;
   const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
   if (nrhs <= MAX_RHS) {
-    LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok, corr);
-    trsv_kernel<T, MAX_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok,
-                                               corr ? corr + 1 : nullptr);
-    count_launch(2);
-    LM_CUDA_TRY(cudaGetLastError());
-    return LM_OK;
+    if (exact) return trsv_pass<T, MAX_RHS, true>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, nullptr, vec_ok);
+    return trsv_pass<T, MAX_RHS, false>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, corr, vec_ok);
   }
-  // more right-hand sides: the FP32 wide variant, WIDE_RHS columns per pass
-  if constexpr (TrsvCfg<T>::EXACT) {
+  if constexpr (kF64) {
     return LM_ERR_UNSUPPORTED;
   } else {
+    // more right-hand sides: the FP32 wide variant, WIDE_RHS columns per pass
     for (int c0 = 0; c0 < nrhs; c0 += WIDE_RHS) {
       const int nc = std::min(WIDE_RHS, nrhs - c0);
-      LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 1, DinvL, X + c0, ldx, sync, status, vec_ok,
-                                                  corr);
-      trsv_kernel<T, WIDE_RHS><<<nb, NT, 0, st>>>(LU, lda, n, nc, 0, DinvU, X + c0, ldx, sync + 2, status, vec_ok,
-                                                  corr ? corr + 1 : nullptr);
-      count_launch(2);
-      LM_CUDA_TRY(cudaGetLastError());
+      if (exact)
+        LM_TRY((trsv_pass<T, WIDE_RHS, true>(LU, lda, n, nc, DinvL, DinvU, X + c0, ldx, sync, status, st, nullptr,
+                                             vec_ok)));
+      else
+        LM_TRY((trsv_pass<T, WIDE_RHS, false>(LU, lda, n, nc, DinvL, DinvU, X + c0, ldx, sync, status, st, corr,
+                                              vec_ok)));
     }
     return LM_OK;
   }
@@ -456,8 +510,8 @@ template size_t trsv_inv_elems<double>(int);
 template int tri_inv_blocks<float>(const float*, long long, int, float*, float*, cudaStream_t);
 template int tri_inv_blocks<double>(const double*, long long, int, double*, double*, cudaStream_t);
 template int trsv_lu<float>(const float*, long long, int, int, const float*, const float*, float*, long long, int*,
-                            int*, cudaStream_t, const int*);
+                            int*, cudaStream_t, const int*, bool);
 template int trsv_lu<double>(const double*, long long, int, int, const double*, const double*, double*, long long,
-                             int*, int*, cudaStream_t, const int*);
+                             int*, int*, cudaStream_t, const int*, bool);
 
 }  // namespace lm

@@ -201,7 +201,7 @@ class Context:
     PHASES = ("gemm", "panel", "swap", "trsm", "other")
 
     def set_ir_method(self, method: int):
-        """IR_RBT (randomised, no pivoting; default) or IR_GEPP for the mixed-precision solves."""
+        """IR_GEPP (FP32 partial pivoting; default) or IR_RBT (randomised, no pivoting) for the mixed-precision solves."""
         _check(_lib().lm_ctx_set_ir_method(self.h, int(method)), "lm_ctx_set_ir_method")
 
     def ir_history(self) -> list:

@@ -1,8 +1,8 @@
 """GPU tests of the mixed-precision path: FP32 LU with tcgen05 TF32 updates,
-refined in FP64 (lm_dgesv_ir), for both factorisations: the randomised
-butterfly + no-pivoting factor (LM_IR_RBT, the default, falling back to
-partial pivoting when refinement stalls) and FP32 partial pivoting
-(LM_IR_GEPP).  Bars: normwise backward error <= 1e-15 n (the target of the
+refined in FP64 (lm_dgesv_ir), for both factorisations: FP32 partial
+pivoting (LM_IR_GEPP, the default) and the randomised butterfly +
+no-pivoting factor (LM_IR_RBT, falling back to partial pivoting when
+refinement stalls).  Bars: normwise backward error <= 1e-15 n (the target of the
 FP64 path) and forward error against the FP64 oracle within what that
 stopping rule allows: 8 kappa * 1e-15 n (plus the 1e-12 floor of the FP64
 path)."""
@@ -27,7 +27,7 @@ def dev(a):
 def ir_method(request, ctx):
     ctx.set_ir_method(request.param)
     yield request.param
-    ctx.set_ir_method(lmb200.IR_RBT)
+    ctx.set_ir_method(lmb200.IR_GEPP)
 
 
 def sigma_spectrum(g, n, kappa, reflectors=4):
@@ -107,16 +107,41 @@ def test_ir_few_rhs_persistent_substitution(ctx, ir_method, n, nrhs):
     assert rel_forward(Xn, Xo) <= max(1e-12, 8 * 1e2 * 1e-15 * n)
 
 
-@pytest.mark.parametrize("n,kappa", [(1024, 1e6), (2051, 1e4), (4096, 1e6)])
-def test_ir_sigma_spectrum_rbt_path(ctx, n, kappa):
-    """The benchmark's matrix class through the default method: the randomised
-    factor must converge by itself (no fallback) to the FP64 bar."""
-    g = philox(9400 + n)
-    A = sigma_spectrum(g, n, kappa)
+@pytest.mark.parametrize("n,kappa", [(4096, 1e2), (4096, 1e4), (4096, 1e6), (8192, 1e2), (8192, 1e4),
+                                     (8192, 1e6)])
+def test_ir_dense_randsvd_vs_oracle(ctx, n, kappa):
+    """The mixed-precision workload's matrix class: A = U diag(sigma) V^T with
+    U, V dense random orthogonal (the reference's randsvd,
+    test/Test/Types.hs:196-213), through the default method (FP32 partial
+    pivoting), which must answer by itself, against the oracle's luSolveP."""
+    O.set_threads(0)
+    g = philox(9700 + n + int(np.log10(kappa)))
+    A = gen_randsvd(g, n, kappa)
     b = g.uniform(-1, 1, n)
     x, iters, berr, st = lmb200.luSolveIR(dev(A), dev(b), ctx=ctx)
     assert st == 0 and berr <= 1e-15 * n, f"status {st}, {iters} iterations, berr {berr}"
-    assert ctx.ir_last_method() == lmb200.IR_RBT
+    assert ctx.ir_last_method() == lmb200.IR_GEPP
+    assert iters <= 12, f"{iters} refinement steps"
+    xn = x.cpu().numpy()
+    assert backward_error(A, xn, b) <= 1e-15 * n
+    xo, _, _ = O.lu_solve_p(A, b)
+    assert rel_forward(xn, xo) <= max(1e-12, 8 * kappa * 1e-15 * n)
+
+
+@pytest.mark.parametrize("n,kappa", [(1024, 1e6), (2051, 1e4), (4096, 1e6)])
+def test_ir_sigma_spectrum_rbt_path(ctx, n, kappa):
+    """The nearly diagonal class (4 reflectors per side) through the randomised
+    method: it must converge by itself (no fallback) to the FP64 bar."""
+    g = philox(9400 + n)
+    A = sigma_spectrum(g, n, kappa)
+    b = g.uniform(-1, 1, n)
+    ctx.set_ir_method(lmb200.IR_RBT)
+    try:
+        x, iters, berr, st = lmb200.luSolveIR(dev(A), dev(b), ctx=ctx)
+        assert st == 0 and berr <= 1e-15 * n, f"status {st}, {iters} iterations, berr {berr}"
+        assert ctx.ir_last_method() == lmb200.IR_RBT
+    finally:
+        ctx.set_ir_method(lmb200.IR_GEPP)
     xn = x.cpu().numpy()
     assert backward_error(A, xn, b) <= 1e-15 * n
     xo = np.linalg.solve(A, b)
@@ -131,7 +156,11 @@ def test_ir_fallback_to_partial_pivoting(ctx):
     n = 256
     A = gen_randsvd(g, n, 1e13, -1.0, 1.0)
     b = g.uniform(-1, 1, n)
-    x, iters, berr, st = lmb200.luSolveIR(dev(A), dev(b), ctx=ctx, max_iter=6)
+    ctx.set_ir_method(lmb200.IR_RBT)
+    try:
+        x, iters, berr, st = lmb200.luSolveIR(dev(A), dev(b), ctx=ctx, max_iter=6)
+    finally:
+        ctx.set_ir_method(lmb200.IR_GEPP)
     assert st == lmb200.LM_ERR_NOT_CONVERGED
     assert ctx.ir_last_method() == lmb200.IR_GEPP
     ctx.check()
@@ -144,6 +173,22 @@ def test_ir_rbt_bitwise_repeatable(ctx):
     n = 700
     A = dev(sigma_spectrum(g, n, 1e3))
     b = dev(g.uniform(-1, 1, n))
+    ctx.set_ir_method(lmb200.IR_RBT)
+    try:
+        xs = [lmb200.luSolveIR(A, b, ctx=ctx)[0].cpu().numpy() for _ in range(3)]
+        assert ctx.ir_last_method() == lmb200.IR_RBT
+    finally:
+        ctx.set_ir_method(lmb200.IR_GEPP)
+    assert np.array_equal(xs[0], xs[1]) and np.array_equal(xs[1], xs[2])
+
+
+def test_ir_gepp_bitwise_repeatable(ctx):
+    """Partial pivoting with look-ahead: the same system gives the same bits
+    on every solve (eager first call, captured graph, replays)."""
+    g = philox(9601)
+    n = 2500
+    A = dev(gen_randsvd(g, n, 1e5))
+    b = dev(g.uniform(-1, 1, n))
     xs = [lmb200.luSolveIR(A, b, ctx=ctx)[0].cpu().numpy() for _ in range(3)]
-    assert ctx.ir_last_method() == lmb200.IR_RBT
+    assert ctx.ir_last_method() == lmb200.IR_GEPP
     assert np.array_equal(xs[0], xs[1]) and np.array_equal(xs[1], xs[2])
