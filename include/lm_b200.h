@@ -323,6 +323,48 @@ int lm_server_reset_stats(lm_server* server);
 /* Finishes admitted requests, cancels queued ones, frees everything. */
 int lm_server_destroy(lm_server* server);
 
+/* ---- matvec and norms ----------------------------------------------------------
+ * lm_dgemv: y (m) = A (m x n, lda) x (n), device pointers, asynchronous on the
+ * context's stream.  Replaces matvec / matvecP (L2.hs:123-139, rewritten to
+ * matvecP by the RULE "matvec/P/Double") and rawGemv / rawDot
+ * (K.hs:84-134), in their floating-point order: every y_i is bitwise the
+ * reference's (four FMA accumulators over j = 4s + l, combined as
+ * ((a0 + a1) + a2) + a3, the last n mod 4 columns added with separately
+ * rounded products). */
+int lm_dgemv(lm_ctx* ctx, int m, int n, const double* A, int lda, const double* x, double* y);
+/* Host-buffer form of lm_dgemv (matvec on host arrays, A dense row-major). */
+int lm_matvec_host(lm_ctx* ctx, int m, int n, const double* A, const double* x, double* y);
+/* lm_dnorm_inf: normInf (Norms.hs:135-141), the largest row sum of |a_ij|,
+ * each row a left fold from 0 in column order (bitwise the reference's); A on
+ * the device, *result on the host (synchronises).  vnormInf (Norms.hs:94-96)
+ * of a vector x is lm_dnorm_inf of x as an n x 1 matrix.  0 for an empty A. */
+int lm_dnorm_inf(lm_ctx* ctx, int m, int n, const double* A, int lda, double* result);
+int lm_norm_inf_host(lm_ctx* ctx, int m, int n, const double* A, double* result);
+
+/* ---- adjacent solvers -------------------------------------------------------------
+ * lm_dgetrf_nopiv: luNoPivot (LU.hs:196-214), LU without row interchanges of
+ * the n x n device matrix A in place (unit L below the diagonal, U on and
+ * above), blocked: 128 x 128 diagonal blocks factored without interchanges,
+ * the panels and the trailing update on the DMMA GEMM.  As in the reference
+ * the caller must supply a matrix that needs no pivoting (e.g. diagonally
+ * dominant); a zero pivot is reported as info = k + 1 and, like the
+ * reference's division by it, leaves Inf/NaN in the result. */
+int lm_dgetrf_nopiv(lm_ctx* ctx, int n, double* A, int lda, int* info);
+/* Host-buffer form: LU (n x n) receives the packed factor. */
+int lm_lu_nopivot_host(lm_ctx* ctx, int n, const double* A, double* LU, int* info);
+/* choleskyGaxpy (Chol.hs:173-204): the same G as cholesky (lower, zeros
+ * above), from the device Cholesky factorisation; host buffers. */
+int lm_cholesky_gaxpy_host(lm_ctx* ctx, int n, const double* A, double* G, int* info);
+/* lm_dtridiag_solve: tridiagSolve (Solve/Banded.hs:292-342), x = A^-1 b for
+ * the symmetric positive definite tridiagonal A with diagonal diag (n) and
+ * superdiagonal supdiag (entries 0 .. n-2 are read), device pointers, by
+ * parallel cyclic reduction: ceil(log2 n) fully parallel elimination steps
+ * instead of the reference's sequential LDL^T sweep (the same solution to
+ * within rounding). */
+int lm_dtridiag_solve(lm_ctx* ctx, int n, const double* diag, const double* supdiag, const double* b, double* x);
+int lm_tridiag_solve_host(lm_ctx* ctx, int n, const double* diag, const double* supdiag, const double* b,
+                          double* x);
+
 /* ---- residual (IR and the reference's scaled residual) ---------------------
  * R = B - A X in FP64 (device), n x nrhs; replaces matvec / rawGemv
  * (L2.hs:123-144, K.hs:119-134) on the refinement path. */

@@ -762,6 +762,55 @@ int lm_dresidual(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const d
   });
 }
 
+int lm_dgemv(lm_ctx* ctx, int m, int n, const double* A, int lda, const double* x, double* y) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (m < 0 || n < 0) return LM_ERR_ARG;
+    if (m == 0) return LM_OK;
+    if (!y || (n > 0 && (!A || !x || lda < n))) return LM_ERR_ARG;
+    return lm::dgemv_exact(m, n, A, lda, x, y, c.stream);
+  });
+}
+
+int lm_dnorm_inf(lm_ctx* ctx, int m, int n, const double* A, int lda, double* result) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (m < 0 || n < 0 || !result || (m > 0 && n > 0 && (!A || lda < n))) return LM_ERR_ARG;
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 2, 64, &ws));
+    unsigned long long* d = static_cast<unsigned long long*>(ws);
+    LM_TRY(lm::dnorm_inf_exact(m, n, A, lda, d, c.stream));
+    unsigned long long h = 0;
+    LM_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    std::memcpy(result, &h, sizeof h);
+    return LM_OK;
+  });
+}
+
+int lm_dgetrf_nopiv(lm_ctx* ctx, int n, double* A, int lda, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!A || lda < n))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::run_graphed(c, lm::gkey("getrf_nopiv", {n, (long long)A, lda}), [&](cudaStream_t s) {
+      return with_aligned(c, n, A, lda, s, [&](double* A2, long long l2) { return lm::dgetrf_nopiv(c, n, A2, l2, s); });
+    }));
+    return finish_info(c, info);
+  });
+}
+
+int lm_dtridiag_solve(lm_ctx* ctx, int n, const double* diag, const double* supdiag, const double* b, double* x) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!diag || !b || !x || (n > 1 && !supdiag)))) return LM_ERR_ARG;
+    if (n == 0) return LM_OK;
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 2, sizeof(double) * 8 * (size_t)n, &ws));
+    return lm::dtridiag_pcr(n, diag, n > 1 ? supdiag : diag, b, x, static_cast<double*>(ws), c.stream);
+  });
+}
+
 int lm_ipiv_to_perm(int n, const int* ipiv, int* perm) {
   if (n < 0 || (n > 0 && (!ipiv || !perm))) return LM_ERR_ARG;
   for (int i = 0; i < n; ++i) perm[i] = i;
@@ -971,6 +1020,97 @@ int lm_cholesky_host(lm_ctx* ctx, int n, const double* A, double* G, int* info) 
     int r = lm::read_status(c, &inf);
     if (info) *info = inf;
     return r;
+  });
+}
+
+int lm_lu_nopivot_host(lm_ctx* ctx, int n, const double* A, double* LU, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!A || !LU))) return LM_ERR_ARG;
+    if (n == 0) {
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    HostBufs hb;
+    LM_TRY(host_bufs(c, n, 0, hb));
+    LM_TRY(h2d_2d(c, hb.A, hb.lda, A, n, n, n));
+    LM_TRY(lm::reset_info(c));
+    LM_TRY(lm::dgetrf_nopiv(c, n, hb.A, hb.lda, c.stream));
+    LM_TRY(d2h_2d(c, LU, n, hb.A, hb.lda, n, n));
+    int inf = 0;
+    int r = lm::read_status(c, &inf);
+    if (info) *info = inf;
+    return r;
+  });
+}
+
+int lm_cholesky_gaxpy_host(lm_ctx* ctx, int n, const double* A, double* G, int* info) {
+  // choleskyGaxpy computes the same G as cholesky; on the device both are the
+  // blocked right-looking factorisation
+  return lm_cholesky_host(ctx, n, A, G, info);
+}
+
+int lm_matvec_host(lm_ctx* ctx, int m, int n, const double* A, const double* x, double* y) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (m < 0 || n < 0 || (m > 0 && !y) || (m > 0 && n > 0 && (!A || !x))) return LM_ERR_ARG;
+    if (m == 0) return LM_OK;
+    const long long lda = rup(std::max(n, 1), 8);
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 3, sizeof(double) * ((size_t)m * lda + rup(std::max(n, 1), 8) + rup(m, 8)), &ws));
+    double* dA = static_cast<double*>(ws);
+    double* dx = dA + (size_t)m * lda;
+    double* dy = dx + rup(std::max(n, 1), 8);
+    LM_TRY(h2d_2d(c, dA, lda, A, n, m, n));
+    if (n > 0) LM_CUDA_TRY(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+    LM_TRY(lm::dgemv_exact(m, n, dA, lda, dx, dy, c.stream));
+    LM_CUDA_TRY(cudaMemcpyAsync(y, dy, sizeof(double) * m, cudaMemcpyDeviceToHost, c.stream));
+    int r = lm::read_status(c, nullptr);
+    return r < 0 ? r : LM_OK;
+  });
+}
+
+int lm_norm_inf_host(lm_ctx* ctx, int m, int n, const double* A, double* result) {
+  if (m < 0 || n < 0 || !result || (m > 0 && n > 0 && !A)) return LM_ERR_ARG;
+  if (m == 0 || n == 0) {
+    *result = 0.0;
+    return LM_OK;
+  }
+  return guarded(ctx, [&](Ctx& c) {
+    const long long lda = rup(n, 8);
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 3, sizeof(double) * ((size_t)m * lda + 8), &ws));
+    double* dA = static_cast<double*>(ws);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(dA + (size_t)m * lda);
+    LM_TRY(h2d_2d(c, dA, lda, A, n, m, n));
+    LM_TRY(lm::dnorm_inf_exact(m, n, dA, lda, d, c.stream));
+    unsigned long long h = 0;
+    LM_CUDA_TRY(cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, c.stream));
+    LM_CUDA_TRY(cudaStreamSynchronize(c.stream));
+    std::memcpy(result, &h, sizeof h);
+    return LM_OK;
+  });
+}
+
+int lm_tridiag_solve_host(lm_ctx* ctx, int n, const double* diag, const double* supdiag, const double* b,
+                          double* x) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || (n > 0 && (!diag || !b || !x || (n > 1 && !supdiag)))) return LM_ERR_ARG;
+    if (n == 0) return LM_OK;
+    const size_t nn = (size_t)rup(n, 8);
+    void* ws = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 3, sizeof(double) * 4 * nn, &ws));
+    double* d = static_cast<double*>(ws);
+    double* sp = d + nn;
+    double* rb = sp + nn;
+    double* dx = rb + nn;
+    void* scr = nullptr;
+    LM_TRY(lm::ctx_workspace(c, 2, sizeof(double) * 8 * (size_t)n, &scr));
+    LM_CUDA_TRY(cudaMemcpyAsync(d, diag, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+    if (n > 1) LM_CUDA_TRY(cudaMemcpyAsync(sp, supdiag, sizeof(double) * (n - 1), cudaMemcpyHostToDevice, c.stream));
+    LM_CUDA_TRY(cudaMemcpyAsync(rb, b, sizeof(double) * n, cudaMemcpyHostToDevice, c.stream));
+    LM_TRY(lm::dtridiag_pcr(n, d, sp, rb, dx, static_cast<double*>(scr), c.stream));
+    LM_CUDA_TRY(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, c.stream));
+    int r = lm::read_status(c, nullptr);
+    return r < 0 ? r : LM_OK;
   });
 }
 

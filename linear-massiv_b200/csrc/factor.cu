@@ -211,6 +211,59 @@ int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st) {
   return zero_upper<double>(A, lda, n, st);
 }
 
+// luNoPivot (LU.hs:196-214) blocked: right-looking with 128-wide diagonal
+// blocks, each factored without interchanges in one CTA (registers); then
+// U12 = inv(L11) A12 and L21 = A21 inv(U11) as products with the blocks'
+// inverses on the DMMA GEMM (the reference's precondition, e.g. diagonal
+// dominance, keeps the diagonal blocks well conditioned), and
+// A22 -= L21 U12.  A zero pivot is recorded in status[1] and, as in the
+// reference, the division by it still happens.
+int dgetrf_nopiv(Ctx& c, int n, double* A, long long lda, cudaStream_t st) {
+  void* ws = nullptr;
+  const size_t blk = (size_t)kNB * kNB;
+  LM_TRY(ctx_workspace(c, 1, sizeof(double) * (3 * blk + (size_t)n * kNB) + sizeof(int) * kSwapPlanInts, &ws));
+  double* Linv = static_cast<double*>(ws);
+  double* Ut = Linv + blk;
+  double* Uinv = Ut + blk;
+  double* W21 = Uinv + blk;
+  TrsmScratch s;
+  s.Linv = Linv;
+  s.plan = reinterpret_cast<int*>(W21 + (size_t)n * kNB);
+  for (int j0 = 0; j0 < n; j0 += kNB) {
+    const int w = std::min(kNB, n - j0);
+    const int R = n - j0 - w;
+    double* A11 = A + (long long)j0 * lda + j0;
+    {
+      Prof p(c, kPhasePanel, 2.0 / 3.0 * w * w * w, 16.0 * w * w, st);
+      LM_TRY(lu_nopiv_block(A11, lda, w, j0, ctx_status(c), st));
+    }
+    if (R <= 0) break;
+    double* A12 = A11 + w;
+    double* A21 = A11 + (long long)w * lda;
+    LM_TRY(trsm_unit_lower_gemm(c, A11, lda, w, A12, lda, R, s, st));
+    {
+      Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 24.0 * (double)w * w, st);
+      LM_TRY(transpose_block(Ut, kNB, A11, lda, w, st));
+      LM_TRY(tri_inv_lower<double>(Ut, kNB, w, false, Uinv, kNB, nullptr, st));
+    }
+    {
+      Prof p(c, kPhaseOther, 0.0, 16.0 * R * w, st);
+      LM_TRY(copy2d<double>(W21, kNB, A21, lda, R, w, st));
+    }
+    GemmDesc t;  // L21 = A21 inv(U11) = W21 (inv(U11^T))^T
+    t.m = R; t.n = w; t.k = w; t.alpha = 1.0; t.beta = 0.0;
+    t.A = W21; t.lda = kNB; t.B = Uinv; t.ldb = kNB; t.b_trans = true;
+    t.C = A21; t.ldc = lda;
+    LM_TRY(dgemm(c, t, st));
+    GemmDesc d;  // A22 -= L21 U12
+    d.m = R; d.n = R; d.k = w; d.alpha = -1.0; d.beta = 1.0;
+    d.A = A21; d.lda = lda; d.B = A12; d.ldb = lda;
+    d.C = A21 + w; d.ldc = lda;
+    LM_TRY(dgemm(c, d, st));
+  }
+  return LM_OK;
+}
+
 namespace {
 
 // Copy to even-stride, 16-byte aligned buffers when the caller's are not

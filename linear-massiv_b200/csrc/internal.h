@@ -149,8 +149,24 @@ int set_identity(T* A, long long lda, int rows, int cols, cudaStream_t st);
 template <typename T>
 int zero_upper(T* A, long long lda, int n, cudaStream_t st);
 
+// --- adjacent entry points (aux_solvers.cu) -----------------------------------
+// y = A x in rawGemv's floating-point order (bitwise the reference's matvecP).
+int dgemv_exact(int m, int n, const double* A, long long lda, const double* x, double* y, cudaStream_t st);
+// normInf of A (bitwise the reference's row folds) as the bits of a
+// non-negative double in *out (device).
+int dnorm_inf_exact(int m, int n, const double* A, long long lda, unsigned long long* out, cudaStream_t st);
+// LU without interchanges of one w x w block (w <= 128) in place; the first
+// zero pivot goes to status[1] as base + k + 1.
+int lu_nopiv_block(double* A, long long lda, int w, int base, int* status, cudaStream_t st);
+// dst (w x w) = src^T.
+int transpose_block(double* dst, long long ldd, const double* src, long long lds, int w, cudaStream_t st);
+// SPD tridiagonal solve by parallel cyclic reduction; W is 8 n doubles.
+int dtridiag_pcr(int n, const double* diag, const double* sup, const double* rhs, double* x, double* W,
+                 cudaStream_t st);
+
 // --- factorisations and solves ---------------------------------------------
 int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st);
+int dgetrf_nopiv(Ctx& c, int n, double* A, long long lda, cudaStream_t st);
 int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* ipiv, double* B,
            long long ldb, cudaStream_t st);
 int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st);

@@ -3,6 +3,7 @@
 // when every check passes.
 #include <cmath>
 #include <cstdio>
+#include <string>
 
 #include "massiv.hpp"
 
@@ -15,7 +16,10 @@ static void expect(bool ok, const char* what) {
   if (!ok) ++failures;
 }
 
-int main() {
+static int solve_file(const char* in, const char* out);
+
+int main(int argc, char** argv) {
+  if (argc == 4 && std::string(argv[1]) == "solve") return solve_file(argv[2], argv[3]);
   // test_luKnown (test/Test/Solve.hs:107-119)
   auto a = Matrix<3, 3>::fromHost({2, 1, 1, 4, 3, 3, 8, 7, 9});
   auto b = Vector<3>::fromHost({1, 1, 1});
@@ -75,9 +79,74 @@ int main() {
   double d = det(S);
   expect(std::fabs(d - 29.0) / 29.0 < 1e-12, "det diag(4,3,2,1)+0.1 = 29");
   // runtime-size entry (SomeMatrix)
-  SomeMatrix sm{3, 3, {2, 1, 1, 4, 3, 3, 8, 7, 9}};
+  SomeMatrixHost sm{3, 3, {2, 1, 1, 4, 3, 3, 8, 7, 9}};
   auto xr = luSolveSome(sm, {1, 1, 1});
   expect(approx(xr[0], 1) && approx(xr[1], -1) && approx(xr[2], 0), "luSolveSome runtime size");
+  auto xs2 = luSolve(forget(a), someVector({1, 1, 1})).toHost();
+  expect(approx(xs2[0], 1) && approx(xs2[1], -1) && approx(xs2[2], 0), "luSolve on forget(Matrix<3,3>)");
+  // matvec with the identity (test/Test/BLAS.hs:71-74)
+  auto mv = matvec(I3, Vector<3>::fromHost({1.5, -2, 7})).toHost();
+  expect(mv[0] == 1.5 && mv[1] == -2 && mv[2] == 7, "matvec identity");
+  // normInf / vnormInf
+  expect(normInf(Matrix<2, 3>::fromHost({1, -2, 3, -4, 5, -6})) == 15.0, "normInf 2x3 = 15");
+  expect(vnormInf(Vector<3>::fromHost({1, -9, 3})) == 9.0, "vnormInf = 9");
+  // luNoPivot on test_luKnown's matrix reordered to need no pivoting: L U = A
+  auto A4 = Matrix<3, 3>::fromHost({8, 7, 9, 4, 3, 3, 2, 1, 1});
+  auto lun = luNoPivot(A4).toHost();
+  auto a4 = A4.toHost();
+  ok = true;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k <= std::min(i, j); ++k) s += (k == i ? 1.0 : lun[i * 3 + k]) * lun[k * 3 + j];
+      ok = ok && approx(s, a4[i * 3 + j]);
+    }
+  expect(ok, "luNoPivot L U = A");
+  auto Gg = choleskyGaxpy(S).toHost();
+  ok = true;
+  for (int i = 0; i < 16; ++i) ok = ok && approx(Gg[i], G[i]);
+  expect(ok, "choleskyGaxpy = cholesky");
+  // test_tridiagKnown (test/Test/Solve.hs:138-150)
+  auto xt = tridiagSolve(Vector<3>::fromHost({2, 2, 2}), Vector<3>::fromHost({-1, -1, 0}),
+                         Vector<3>::fromHost({1, 0, 1})).toHost();
+  expect(approx(xt[0], 1) && approx(xt[1], 1) && approx(xt[2], 1), "tridiagSolve known");
   std::printf("%d failure(s)\n", failures);
   return failures ? 1 : 0;
+}
+
+// Runtime-size solve of a system read from a file (int32 kind, int32 n, then
+// A as n*n and b as n doubles; kind 0 = LU, 1 = Cholesky), written as n
+// doubles.  Sizes among the reify candidates go through the typed API after
+// reifyDim, the others through the SomeMatrix operations.
+static int solve_file(const char* in, const char* out) {
+  std::FILE* f = std::fopen(in, "rb");
+  if (!f) return 2;
+  int hdr[2];
+  if (std::fread(hdr, sizeof(int), 2, f) != 2) return 2;
+  const std::size_t n = (std::size_t)hdr[1];
+  std::vector<double> A(n * n), b(n);
+  if (std::fread(A.data(), sizeof(double), n * n, f) != n * n || std::fread(b.data(), sizeof(double), n, f) != n)
+    return 2;
+  std::fclose(f);
+  SomeMatrix sa = someMatrix(n, n, A);
+  SomeVector sb = someVector(b);
+  std::vector<double> x;
+  bool typed = false;
+  try {
+    x = reifyDim<3, 64, 300>(n, [&](auto N) {
+      constexpr std::size_t K = decltype(N)::value;
+      auto ta = unsafeTyped<K>(sa);
+      auto tb = Vector<K>::fromHost(b);
+      return hdr[0] == 0 ? luSolve(ta, tb).toHost() : choleskySolve(ta, tb).toHost();
+    });
+    typed = true;
+  } catch (const Error&) {
+    x = (hdr[0] == 0 ? luSolve(sa, sb) : choleskySolve(sa, sb)).toHost();
+  }
+  std::FILE* g = std::fopen(out, "wb");
+  if (!g) return 2;
+  std::fwrite(x.data(), sizeof(double), n, g);
+  std::fclose(g);
+  std::printf("solved n=%zu kind=%d via %s\n", n, hdr[0], typed ? "reifyDim + typed API" : "SomeMatrix");
+  return 0;
 }

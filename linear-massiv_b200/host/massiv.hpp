@@ -15,8 +15,12 @@
 // the *Info variants.  CUDA or argument errors throw massiv::Error (the
 // Haskell binding turns the same statuses into exceptions).
 //
-// File references: Types.hs, Internal.hs (src/Numeric/LinearAlgebra/Massiv/),
-// L3.hs = BLAS/Level3.hs, LU.hs = Solve/LU.hs, Chol.hs = Solve/Cholesky.hs.
+// Runtime-size values (the reference's SomeMatrix / SomeVector existentials)
+// are massiv::SomeMatrix / SomeVector, with someMatrix, forget and reifyDim.
+//
+// File references: Types.hs, Internal.hs, Norms.hs (src/Numeric/LinearAlgebra/Massiv/),
+// L2.hs = BLAS/Level2.hs, L3.hs = BLAS/Level3.hs, LU.hs = Solve/LU.hs,
+// Chol.hs = Solve/Cholesky.hs.
 #pragma once
 
 #include <lm_b200.h>
@@ -25,6 +29,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
@@ -228,28 +233,191 @@ Vector<N> choleskySolve(const Matrix<N, N>& a, const Vector<N>& b) {
   return Vector<N>::fromHost(X);
 }
 
-// ---- runtime sizes: SomeMatrix (Types.hs:165-178) ----------------------------
-// A matrix whose dimensions are known only at run time (serving).
-struct SomeMatrix {
-  std::size_t rows = 0, cols = 0;
-  std::vector<double> host;  // row-major
-};
+// ---- BLAS-2, norms, adjacent solvers -------------------------------------------
+// matvec (L2.hs:123-127; matvecP via its RULE, L2.hs:131-144): bitwise the
+// reference's rawGemv order.
+template <std::size_t M, std::size_t N>
+Vector<M> matvec(const Matrix<M, N>& a, const Vector<N>& x) {
+  Vector<M> y;
+  check(lm_dgemv(context(), (int)M, (int)N, a.data(), (int)N, x.data(), y.data()), "matvec");
+  return y;
+}
 
-inline std::vector<double> luSolveSome(const SomeMatrix& a, const std::vector<double>& b) {
-  if (a.rows != a.cols || b.size() != a.rows) throw Error(LM_ERR_ARG, "luSolveSome: dimension mismatch");
-  std::vector<double> x(a.rows);
+// normInf (Norms.hs:135-141) and vnormInf (Norms.hs:94-96).
+template <std::size_t M, std::size_t N>
+double normInf(const Matrix<M, N>& a) {
+  double r = 0.0;
+  check(lm_dnorm_inf(context(), (int)M, (int)N, a.data(), (int)N, &r), "normInf");
+  return r;
+}
+template <std::size_t N>
+double vnormInf(const Vector<N>& x) {
+  double r = 0.0;
+  check(lm_dnorm_inf(context(), (int)N, 1, x.data(), 1, &r), "vnormInf");
+  return r;
+}
+
+// luNoPivot (LU.hs:196-214): packed unit-L / U, no interchanges.
+template <std::size_t N>
+Matrix<N, N> luNoPivot(const Matrix<N, N>& a, int* info_out = nullptr) {
+  std::vector<double> A = a.toHost(), LU(N * N);
   int info = 0;
-  check(lm_lu_solve_host(context(), (int)a.rows, 1, a.host.data(), b.data(), x.data(), &info), "luSolveSome");
+  check(lm_lu_nopivot_host(context(), (int)N, A.data(), LU.data(), &info), "luNoPivot");
+  if (info_out) *info_out = info;
+  return Matrix<N, N>::fromHost(LU);
+}
+
+// choleskyGaxpy (Chol.hs:173-204): the same G as cholesky.
+template <std::size_t N>
+Matrix<N, N> choleskyGaxpy(const Matrix<N, N>& a, int* info_out = nullptr) {
+  std::vector<double> A = a.toHost(), G(N * N);
+  int info = 0;
+  check(lm_cholesky_gaxpy_host(context(), (int)N, A.data(), G.data(), &info), "choleskyGaxpy");
+  if (info_out) *info_out = info;
+  return Matrix<N, N>::fromHost(G);
+}
+
+// tridiagSolve (Solve/Banded.hs:292-342): SPD tridiagonal from its diagonal and
+// superdiagonal (entries 0 .. N-2 read).
+template <std::size_t N>
+Vector<N> tridiagSolve(const Vector<N>& diag, const Vector<N>& supdiag, const Vector<N>& b) {
+  Vector<N> x;
+  check(lm_dtridiag_solve(context(), (int)N, diag.data(), supdiag.data(), b.data(), x.data()), "tridiagSolve");
   return x;
 }
 
-inline std::vector<double> choleskySolveSome(const SomeMatrix& a, const std::vector<double>& b) {
-  if (a.rows != a.cols || b.size() != a.rows) throw Error(LM_ERR_ARG, "choleskySolveSome: dimension mismatch");
-  std::vector<double> x(a.rows);
-  int info = 0;
-  check(lm_chol_solve_host(context(), (int)a.rows, 1, a.host.data(), b.data(), x.data(), &info),
-        "choleskySolveSome");
+// ---- runtime sizes: SomeMatrix / someMatrix / reifyDim -----------------------------
+// The reference wraps arrays whose dimensions are known only at run time in
+// existentials (SomeMatrix, SomeVector; someMatrix / someVector, Types.hs:165-178)
+// and turns a runtime Int into a type-level Nat with reifyDim / reifyDim2
+// (Internal.hs:123-129).  Here SomeMatrix / SomeVector carry their dimensions
+// as values (device-resident like Matrix); forget() is the existential's
+// constructor, reifyDim<Ns...> recovers a compile-time size from a runtime one
+// over a list of candidate sizes (C++ cannot mint a new type at run time), and
+// the operations on SomeMatrix check dimensions at run time where the
+// reference's checks happen at compile time.
+class SomeMatrix {
+ public:
+  SomeMatrix() = default;
+  SomeMatrix(std::size_t rows, std::size_t cols) : rows_(rows), cols_(cols), buf_(rows * cols) {}
+  std::size_t rows() const { return rows_; }
+  std::size_t cols() const { return cols_; }
+  double* data() const { return buf_.data(); }
+  std::vector<double> toHost() const {
+    std::vector<double> v(rows_ * cols_);
+    if (!v.empty()) check(lm_d2h(context(), v.data(), data(), v.size() * sizeof(double)), "lm_d2h");
+    return v;
+  }
+
+ private:
+  std::size_t rows_ = 0, cols_ = 0;
+  DeviceBuffer buf_;
+};
+
+class SomeVector {
+ public:
+  SomeVector() = default;
+  explicit SomeVector(std::size_t n) : n_(n), buf_(n) {}
+  std::size_t size() const { return n_; }
+  double* data() const { return buf_.data(); }
+  std::vector<double> toHost() const {
+    std::vector<double> v(n_);
+    if (n_) check(lm_d2h(context(), v.data(), data(), n_ * sizeof(double)), "lm_d2h");
+    return v;
+  }
+
+ private:
+  std::size_t n_ = 0;
+  DeviceBuffer buf_;
+};
+
+// someMatrix (Types.hs:170-174): wrap row-major host values of a rows x cols array.
+inline SomeMatrix someMatrix(std::size_t rows, std::size_t cols, const std::vector<double>& v) {
+  if (v.size() != rows * cols) throw Error(LM_ERR_ARG, "someMatrix: wrong size");
+  SomeMatrix m(rows, cols);
+  if (!v.empty()) check(lm_h2d(context(), m.data(), v.data(), v.size() * sizeof(double)), "lm_h2d");
+  return m;
+}
+// someVector (Types.hs:176-178)
+inline SomeVector someVector(const std::vector<double>& v) {
+  SomeVector x(v.size());
+  if (!v.empty()) check(lm_h2d(context(), x.data(), v.data(), v.size() * sizeof(double)), "lm_h2d");
   return x;
+}
+// The existential's constructor: forget the static dimensions.
+template <std::size_t M, std::size_t N>
+SomeMatrix forget(const Matrix<M, N>& a) {
+  return someMatrix(M, N, a.toHost());
+}
+
+// reifyDim (Internal.hs:123-125): call f(std::integral_constant<size_t, N>{})
+// for the candidate N equal to n; Error(LM_ERR_ARG) when none is.
+template <std::size_t... Ns, typename F>
+auto reifyDim(std::size_t n, F&& f) {
+  using R = decltype(f(std::integral_constant<std::size_t, 1>{}));
+  bool hit = false;
+  if constexpr (std::is_void_v<R>) {
+    ((n == Ns ? (f(std::integral_constant<std::size_t, Ns>{}), hit = true) : false), ...);
+    if (!hit) throw Error(LM_ERR_ARG, "reifyDim: size not among the candidates");
+  } else {
+    R out{};
+    ((n == Ns ? (out = f(std::integral_constant<std::size_t, Ns>{}), hit = true) : false), ...);
+    if (!hit) throw Error(LM_ERR_ARG, "reifyDim: size not among the candidates");
+    return out;
+  }
+}
+// Recover a typed Matrix<N, N> from a SomeMatrix whose size is one of Ns.
+template <std::size_t N>
+Matrix<N, N> unsafeTyped(const SomeMatrix& a) {
+  if (a.rows() != N || a.cols() != N) throw Error(LM_ERR_ARG, "typed: dimension mismatch");
+  return Matrix<N, N>::fromHost(a.toHost());
+}
+
+// Operations on runtime-size values (the reference's functions applied inside
+// a SomeMatrix pattern match).
+inline SomeVector luSolve(const SomeMatrix& a, const SomeVector& b, int* info_out = nullptr) {
+  if (a.rows() != a.cols() || b.size() != a.rows()) throw Error(LM_ERR_ARG, "luSolve: dimension mismatch");
+  const int n = (int)a.rows();
+  std::vector<double> A = a.toHost(), B = b.toHost(), X(n);
+  int info = 0;
+  check(lm_lu_solve_host(context(), n, 1, A.data(), B.data(), X.data(), &info), "luSolve");
+  if (info_out) *info_out = info;
+  return someVector(X);
+}
+inline SomeVector choleskySolve(const SomeMatrix& a, const SomeVector& b, int* info_out = nullptr) {
+  if (a.rows() != a.cols() || b.size() != a.rows()) throw Error(LM_ERR_ARG, "choleskySolve: dimension mismatch");
+  const int n = (int)a.rows();
+  std::vector<double> A = a.toHost(), B = b.toHost(), X(n);
+  int info = 0;
+  check(lm_chol_solve_host(context(), n, 1, A.data(), B.data(), X.data(), &info), "choleskySolve");
+  if (info_out) *info_out = info;
+  return someVector(X);
+}
+inline SomeMatrix matMul(const SomeMatrix& a, const SomeMatrix& b) {
+  if (a.cols() != b.rows()) throw Error(LM_ERR_ARG, "matMul: dimension mismatch");
+  SomeMatrix c(a.rows(), b.cols());
+  check(lm_dgemm(context(), (int)a.rows(), (int)b.cols(), (int)a.cols(), 1.0, a.data(), (int)a.cols(), b.data(),
+                 (int)b.cols(), 0.0, c.data(), (int)b.cols()),
+        "matMul");
+  return c;
+}
+inline SomeVector matvec(const SomeMatrix& a, const SomeVector& x) {
+  if (a.cols() != x.size()) throw Error(LM_ERR_ARG, "matvec: dimension mismatch");
+  SomeVector y(a.rows());
+  check(lm_dgemv(context(), (int)a.rows(), (int)a.cols(), a.data(), (int)a.cols(), x.data(), y.data()), "matvec");
+  return y;
+}
+
+// Earlier host-vector spellings of the runtime-size solves.
+struct SomeMatrixHost {
+  std::size_t rows = 0, cols = 0;
+  std::vector<double> host;  // row-major
+};
+inline std::vector<double> luSolveSome(const SomeMatrixHost& a, const std::vector<double>& b) {
+  return luSolve(someMatrix(a.rows, a.cols, a.host), someVector(b)).toHost();
+}
+inline std::vector<double> choleskySolveSome(const SomeMatrixHost& a, const std::vector<double>& b) {
+  return choleskySolve(someMatrix(a.rows, a.cols, a.host), someVector(b)).toHost();
 }
 
 }  // namespace massiv

@@ -43,6 +43,8 @@ EXPORTS = [
     "lm_batch_factors", "lm_batch_solve_host", "lm_batch_tune", "lm_batch_tune_get", "lm_batch_tune_set",
     "lm_server_default_config", "lm_server_create", "lm_server_submit", "lm_server_test", "lm_server_wait",
     "lm_server_cancel", "lm_server_drain", "lm_server_stats", "lm_server_reset_stats", "lm_server_destroy",
+    "lm_dgemv", "lm_matvec_host", "lm_dnorm_inf", "lm_norm_inf_host", "lm_dgetrf_nopiv", "lm_lu_nopivot_host",
+    "lm_cholesky_gaxpy_host", "lm_dtridiag_solve", "lm_tridiag_solve_host",
 ]
 
 IR_RBT = 0
@@ -140,6 +142,15 @@ def _lib():
                 "lm_server_stats": ([vp, vp], i),
                 "lm_server_reset_stats": ([vp], i),
                 "lm_server_destroy": ([vp], i),
+                "lm_dgemv": ([vp, i, i, vp, i, vp, vp], i),
+                "lm_matvec_host": ([vp, i, i, dp, dp, dp], i),
+                "lm_dnorm_inf": ([vp, i, i, vp, i, dp], i),
+                "lm_norm_inf_host": ([vp, i, i, dp, dp], i),
+                "lm_dgetrf_nopiv": ([vp, i, vp, i, ip], i),
+                "lm_lu_nopivot_host": ([vp, i, dp, dp, ip], i),
+                "lm_cholesky_gaxpy_host": ([vp, i, dp, dp, ip], i),
+                "lm_dtridiag_solve": ([vp, i, vp, vp, vp, vp], i),
+                "lm_tridiag_solve_host": ([vp, i, dp, dp, dp, dp], i),
             }
             for name, (args, res) in sigs.items():
                 fn = getattr(L, name)
@@ -381,6 +392,62 @@ def det(A, ctx: Context | None = None) -> float:
     _check(_lib().lm_det_host(ctx.h, a.shape[0], a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                               ctypes.byref(out)), "lm_det_host")
     return out.value
+
+
+def matvec(A, x, ctx: Context | None = None):
+    """matvec / matvecP (Level2.hs:123-139): y = A x, bitwise the reference's
+    rawGemv order."""
+    import torch
+
+    ctx = ctx or default_context(A.device.index or 0)
+    _mat(A, "A")
+    m, n = A.shape
+    x = x.contiguous()
+    if x.dim() != 1 or x.shape[0] != n or x.dtype != torch.float64 or not x.is_cuda:
+        raise ValueError("x must be a float64 CUDA vector of length A.shape[1]")
+    y = torch.empty(m, dtype=torch.float64, device=A.device)
+    _check(_lib().lm_dgemv(ctx.h, m, n, _ptr(A), A.stride(0), _ptr(x), _ptr(y)), "lm_dgemv")
+    return y
+
+
+def normInf(A, ctx: Context | None = None) -> float:
+    """normInf (Norms.hs:135-141); a 1-D tensor gives vnormInf (Norms.hs:94-96)."""
+    ctx = ctx or default_context(A.device.index or 0)
+    M = A.unsqueeze(1).contiguous() if A.dim() == 1 else A
+    _mat(M, "A")
+    out = ctypes.c_double(0.0)
+    _check(_lib().lm_dnorm_inf(ctx.h, M.shape[0], M.shape[1], _ptr(M), M.stride(0), ctypes.byref(out)),
+           "lm_dnorm_inf")
+    return out.value
+
+
+def luNoPivot(A, ctx: Context | None = None):
+    """luNoPivot (LU.hs:196-214): packed unit-L / U without interchanges; returns (LU, info)."""
+    ctx = ctx or default_context(A.device.index or 0)
+    LU = A.clone()
+    _mat(LU, "A")
+    info = ctypes.c_int(0)
+    _check(_lib().lm_dgetrf_nopiv(ctx.h, LU.shape[0], _ptr(LU), LU.stride(0), ctypes.byref(info)),
+           "lm_dgetrf_nopiv")
+    return LU, info.value
+
+
+def choleskyGaxpy(A, ctx: Context | None = None):
+    """choleskyGaxpy (Chol.hs:173-204): the same G as cholesky."""
+    return cholesky(A, ctx)
+
+
+def tridiagSolve(diag, supdiag, b, ctx: Context | None = None):
+    """tridiagSolve (Solve/Banded.hs:292-342): SPD tridiagonal solve from the
+    diagonal and the superdiagonal (length n, entries 0..n-2 used)."""
+    import torch
+
+    ctx = ctx or default_context(b.device.index or 0)
+    diag, supdiag, b = diag.contiguous(), supdiag.contiguous(), b.contiguous()
+    x = torch.empty_like(b)
+    _check(_lib().lm_dtridiag_solve(ctx.h, b.shape[0], _ptr(diag), _ptr(supdiag), _ptr(b), _ptr(x)),
+           "lm_dtridiag_solve")
+    return x
 
 
 def ipiv_to_perm(ipiv):

@@ -174,3 +174,54 @@ def test_pivot_tie_first_wins():
     assert ipiv[0] == 0
     _, perm = O.lu_generic(A)
     assert list(perm) == [1, 0]
+
+
+# ---- adjacent solvers: known answers and independent checks ---------------------
+
+def test_tridiag_known_answer():
+    # test_tridiagKnown (test/Test/Solve.hs:138-150): x = [1, 1, 1] for
+    # A = tridiag(-1, 2, -1), b = [1, 0, 1], with the suite's (~=) tolerance
+    x = O.tridiag_solve(np.full(3, 2.0), np.array([-1.0, -1.0, 0.0]), np.array([1.0, 0.0, 1.0]))
+    assert np.all(np.abs(x - 1.0) < 1e-8 * (2 + np.abs(x)))
+
+
+@pytest.mark.parametrize("n", [1, 2, 9, 200])
+def test_tridiag_vs_dense_solve(n):
+    g = philox(800 + n)
+    sup = g.uniform(-1, 1, n)
+    d = 2.5 + g.uniform(0, 1, n)
+    b = g.uniform(-1, 1, n)
+    T = np.diag(d) + np.diag(sup[:n - 1], 1) + np.diag(sup[:n - 1], -1)
+    assert np.abs(O.tridiag_solve(d, sup, b) - np.linalg.solve(T, b)).max() < 1e-13
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 70])
+def test_lu_nopivot_reconstructs(n):
+    g = philox(900 + n)
+    A = g.uniform(-1, 1, (n, n)) + n * np.eye(n)
+    LU = O.lu_nopivot(A)
+    L, U = np.tril(LU, -1) + np.eye(n), np.triu(LU)
+    assert O.scaled_residual_lu(A, LU, np.arange(n)) < 10
+    # without pivoting on a diagonally dominant matrix, GEPP picks the diagonal
+    # too, so the P path gives the same factor up to rounding
+    _, LUp, ipiv = O.lu_solve_p(A, np.ones(n))
+    assert np.array_equal(ipiv, np.arange(n))
+    assert np.abs(LU - LUp).max() < 1e-12 * np.abs(LU).max()
+    assert np.abs(L @ U - A).max() < 1e-12 * np.abs(A).max()
+
+
+@pytest.mark.parametrize("n", [1, 3, 40])
+def test_cholesky_gaxpy_matches_cholesky(n):
+    g = philox(1000 + n)
+    B = g.uniform(-1, 1, (n, n))
+    S = B @ B.T + n * np.eye(n)
+    G = O.cholesky_gaxpy(S)
+    assert np.all(np.triu(G, 1) == 0.0)
+    assert np.abs(G - O.cholesky_generic(S)).max() < 1e-13 * np.abs(G).max()
+
+
+def test_norm_inf_matches_numpy():
+    g = philox(1100)
+    A = g.uniform(-3, 3, (37, 53))
+    assert abs(O.norm_inf(A) - np.abs(A).sum(axis=1).max()) < 1e-13 * O.norm_inf(A)
+    assert O.norm_inf(np.array([[1.0, -2.0, 3.0], [-4.0, 5.0, -6.0]])) == 15.0
