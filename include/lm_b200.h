@@ -209,13 +209,15 @@ int lm_ctx_ir_history(lm_ctx* ctx, double* berr, int max_steps, int* steps);
  * pool owns every allocation, a real-time loop that forbids allocation, a
  * plugin host that only hands out pre-registered buffers).  Same result as
  * lm_dpotrf on `stream` (cudaStream_t as void*, 0 = legacy default stream),
- * on the current device, synchronising to report info.  Its scratch is one
- * static device array of the library, about 4.3 MB held by every GPU that
- * loads the library until exit; it limits n to 4096 (larger n returns
- * LM_ERR_ARG) and needs A 16-byte aligned with an even lda.  The first call
- * on a device looks up the array's device address: make that call before any
- * stream capture.  All calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller. */
+ * on the current device; it synchronises `stream` to report info.  Its
+ * scratch is one static device array of the library, about 4.3 MB per
+ * device, reserved when the first call on that device looks up its address
+ * (CUDA loads device code lazily by default) and held until exit: make that
+ * first call (n = 0 does only this) before any region that must not
+ * allocate and before any stream capture.  The array limits n to 4096
+ * (larger n returns LM_ERR_ARG) and A must be 16-byte aligned with an even
+ * lda.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller. */
 int lm_dpotrf_noalloc(void* stream, int n, double* A, int lda, int* info);
 
 /* ---- batched uneven-size solves in one persistent launch -----------------------

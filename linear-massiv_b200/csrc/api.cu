@@ -34,6 +34,7 @@ struct Ctx {
   long long ws_generation = 0;
   cudaStream_t side = nullptr;  // capture stream when the caller's stream is the legacy default
   cudaStream_t aux = nullptr;   // look-ahead stream of the factorisations (ctx_aux)
+  bool allow_aux = true;        // false: the factorisations run without look-ahead
   cudaEvent_t ev_la[2] = {};    // its fork / join events
   void* pinned = nullptr;       // ctx_pinned
   size_t pinned_bytes = 0;
@@ -136,7 +137,10 @@ int ctx_pinned(Ctx& c, size_t bytes, void** ptr) {
   return LM_OK;
 }
 
+bool ctx_lookahead(Ctx& c) { return c.allow_aux; }
+
 int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join) {
+  if (!c.allow_aux) return LM_ERR_UNSUPPORTED;
   if (!c.aux) {
     int lo = 0, hi = 0;
     LM_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&lo, &hi));
@@ -298,6 +302,7 @@ int dpotrf_borrowed(int device, int num_sms, cudaStream_t st, int n, double* A, 
   c.num_sms = num_sms;
   c.stream = st;
   c.graphs = false;
+  c.allow_aux = false;  // one stream, no CUDA objects created on the caller's behalf
   c.d_status = d_status;
   c.ws[1] = scratch;  // grow-only workspace that never needs to grow
   c.ws_bytes[1] = scratch_bytes;

@@ -83,7 +83,8 @@ __global__ void __launch_bounds__(256) norm_inf_exact_kernel(int m, int n, const
 // luNoPivot of the w x w block at A (w <= 128) in place: thread (ty, tx) of a
 // 16 x 32 grid holds elements (ty + 16 a, tx + 32 b), a < 8, b < 4, in
 // registers.  Step k: the owners of row k publish it, the owners of column k
-// form the multipliers a_ik / a_kk, every thread subtracts l_ik * u_kj with a
+// form the multipliers a_ik / a_kk (as products with 1 / a_kk, within an ulp
+// of the quotients), every thread subtracts l_ik * u_kj with a
 // separately rounded product (the reference's `aij - aik * akj`).  Rows and
 // columns past w are the identity.  The first zero pivot is recorded as
 // base + k + 1 in status[1]; the division still runs, as in the reference.
@@ -114,6 +115,7 @@ __global__ void __launch_bounds__(512) lu_nopiv_block_kernel(double* A, long lon
     const double ukk = urow[buf][k];
     if (tx == (k & 31)) {
       if (ty == 0 && ukk == 0.0) atomicCAS(status + 1, 0, base + k + 1);
+      const double rkk = 1.0 / ukk;  // one division per column: the multipliers are products with it
 #pragma unroll
       for (int b = 0; b < 4; ++b)
         if (b == bk)
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(512) lu_nopiv_block_kernel(double* A, long lon
           for (int a = 0; a < 8; ++a) {
             const int i = ty + 16 * a;
             if (i > k) {
-              const double lik = v[a][b] / ukk;
+              const double lik = v[a][b] * rkk;
               v[a][b] = lik;
               lcol[buf][i] = lik;
             }
@@ -195,6 +197,26 @@ __global__ void pcr_finish_kernel(int n, const double* b, const double* d, doubl
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) x[i] = d[i] / b[i];
 }
 
+// P = G on and below the diagonal, G^T above it (n x n), from the lower
+// triangle of G: 32 x 32 tiles, the tiles above the diagonal transposed
+// through shared memory so both the reads and the writes are coalesced.
+__global__ void pack_lower_sym_kernel(double* P, long long ldp, const double* G, long long ldg, int n) {
+  __shared__ double t[32][33];
+  const int bi = blockIdx.y * 32, bj = blockIdx.x * 32;  // tile of P
+  const bool upper = bj > bi;
+  const int si = upper ? bj : bi, sj = upper ? bi : bj;  // tile of G that it comes from
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = si + r, j = sj + threadIdx.x;
+    t[r][threadIdx.x] = (i < n && j < n) ? G[(long long)i * ldg + j] : 0.0;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    const int i = bi + r, j = bj + threadIdx.x;
+    if (i >= n || j >= n) continue;
+    P[(long long)i * ldp + j] = upper ? t[threadIdx.x][r] : (j <= i ? t[r][threadIdx.x] : G[(long long)j * ldg + i]);
+  }
+}
+
 int grid_for(long long total, int per) { return (int)std::max<long long>(1, std::min<long long>(cdivll(total, per), 4096)); }
 
 }  // namespace
@@ -220,6 +242,15 @@ int lu_nopiv_block(double* A, long long lda, int w, int base, int* status, cudaS
   if (w <= 0) return LM_OK;
   if (w > 128) return LM_ERR_ARG;
   lu_nopiv_block_kernel<<<1, 512, 0, st>>>(A, lda, w, base, status);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+int pack_lower_sym(double* P, long long ldp, const double* G, long long ldg, int n, cudaStream_t st) {
+  if (n <= 0) return LM_OK;
+  dim3 tb(32, 8), tg(cdiv(n, 32), cdiv(n, 32));
+  pack_lower_sym_kernel<<<tg, tb, 0, st>>>(P, ldp, G, ldg, n);
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;

@@ -118,7 +118,7 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
   // capped to fit there.  Nothing waits across the two streams inside a
   // kernel; at worst the panel starts when the update ends.
   const int nsm = ctx_num_sms(c);
-  const bool la = n >= kLookaheadMinN && nsm > 2 * kLookaheadSms;
+  const bool la = n >= kLookaheadMinN && nsm > 2 * kLookaheadSms && ctx_lookahead(c);
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   if (la) LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
@@ -173,39 +173,92 @@ int dgetrf(Ctx& c, int n, double* A, long long lda, int* ipiv, cudaStream_t st) 
   return LM_OK;
 }
 
+namespace {
+
+// L21 = A21 inv(L11)^T for the block column at j0 (w wide, R rows below):
+// inv(L11) in one CTA, then the product with a copy of A21 on the DMMA GEMM.
+int potrf_panel(Ctx& c, double* A, long long lda, int j0, int w, int R, double* Linv, double* W21, cudaStream_t st,
+                int max_sms = 0) {
+  double* A11 = A + (long long)j0 * lda + j0;
+  double* A21 = A11 + (long long)w * lda;
+  {
+    Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 16.0 * w * w, st);
+    LM_TRY(tri_inv_lower<double>(A11, lda, w, false, Linv, kNB, nullptr, st));
+  }
+  {
+    Prof p(c, kPhaseOther, 0.0, 16.0 * R * w, st);
+    LM_TRY(copy2d<double>(W21, kNB, A21, lda, R, w, st));
+  }
+  GemmDesc t;  // L21 = A21 * L11^-T
+  t.m = R; t.n = w; t.k = w; t.alpha = 1.0; t.beta = 0.0;
+  t.A = W21; t.lda = kNB; t.B = Linv; t.ldb = kNB; t.b_trans = true;
+  t.C = A21; t.ldc = lda;
+  t.max_sms = max_sms;
+  return dgemm(c, t, st);
+}
+
+}  // namespace
+
+// Right-looking blocked Cholesky with look-ahead: once the trailing update
+// has reached the next block column (its diagonal block and everything
+// below), that column is factored on the priority stream (diagonal block,
+// inverse, L21) while the rest of the lower-triangle update runs on the
+// other SMs.  The two streams touch disjoint columns: the update reads the
+// current L21 and writes columns right of the next block column.
 int dpotrf(Ctx& c, int n, double* A, long long lda, cudaStream_t st) {
+  const size_t blk = (size_t)kNB * kNB;
+  void* ws = nullptr;
+  LM_TRY(ctx_workspace(c, 1, sizeof(double) * (blk + (size_t)n * kNB), &ws));
+  double* Linv = static_cast<double*>(ws);
+  double* W21 = Linv + blk;
+  const int nsm = ctx_num_sms(c);
+  const bool la = n >= kLookaheadMinN && nsm > 2 * kLookaheadSms && ctx_lookahead(c);
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  if (la) LM_TRY(ctx_aux(c, &aux, &ev_fork, &ev_join));
+  auto factor_column = [&](int j0, cudaStream_t s, int max_sms) {
+    const int w = std::min(kNB, n - j0);
+    const int R = n - j0 - w;
+    {
+      Prof p(c, kPhasePanel, (double)w * w * w / 3.0, 8.0 * w * w, s);
+      LM_TRY(potrf_block<double>(c, A + (long long)j0 * lda + j0, lda, w, j0, s));
+    }
+    if (R > 0) LM_TRY(potrf_panel(c, A, lda, j0, w, R, Linv, W21, s, max_sms));
+    return LM_OK;
+  };
+  LM_TRY(factor_column(0, st, 0));
   for (int j0 = 0; j0 < n; j0 += kNB) {
     const int w = std::min(kNB, n - j0);
     const int R = n - j0 - w;
-    double* A11 = A + (long long)j0 * lda + j0;
-    {
-      Prof p(c, kPhasePanel, (double)w * w * w / 3.0, 8.0 * w * w, st);
-      LM_TRY(potrf_block<double>(c, A11, lda, w, j0, st));
-    }
-    if (R > 0) {
-      void* ws = nullptr;
-      LM_TRY(ctx_workspace(c, 1, sizeof(double) * ((size_t)kNB * kNB + (size_t)R * kNB), &ws));
-      double* Linv = static_cast<double*>(ws);
-      double* W21 = Linv + (size_t)kNB * kNB;
-      double* A21 = A11 + (long long)w * lda;
-      {
-        Prof p(c, kPhaseTrsm, (double)w * w * w / 3.0, 16.0 * w * w, st);
-        LM_TRY(tri_inv_lower<double>(A11, lda, w, false, Linv, kNB, nullptr, st));
+    if (R <= 0) break;
+    double* A21 = A + (long long)(j0 + w) * lda + j0;
+    double* A22 = A21 + w;
+    const int wn = std::min(kNB, R);  // next block column
+    // A22 -= L21 L21^T: the next block column first (all R rows of it)
+    GemmDesc d;
+    d.m = R; d.n = wn; d.k = w; d.alpha = -1.0; d.beta = 1.0;
+    d.A = A21; d.lda = lda; d.B = A21; d.ldb = lda; d.b_trans = true;
+    d.C = A22; d.ldc = lda;
+    LM_TRY(dgemm(c, d, st));
+    const int rest = R - wn;
+    GemmDesc r;  // then the lower triangle right of it
+    r.m = rest; r.n = rest; r.k = w; r.alpha = -1.0; r.beta = 1.0;
+    r.A = A21 + (long long)wn * lda; r.lda = lda; r.B = r.A; r.ldb = lda; r.b_trans = true;
+    r.lower_only = true;
+    r.C = A22 + (long long)wn * lda + wn; r.ldc = lda;
+    if (la) {
+      LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
+      LM_CUDA_TRY(cudaStreamWaitEvent(aux, ev_fork, 0));
+      LM_TRY(factor_column(j0 + w, aux, kLookaheadSms));
+      LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
+      if (rest > 0) {
+        r.max_sms = nsm - kLookaheadSms;
+        LM_TRY(dgemm(c, r, st));
       }
-      {
-        Prof p(c, kPhaseOther, 0.0, 16.0 * R * w, st);
-        LM_TRY(copy2d<double>(W21, kNB, A21, lda, R, w, st));
-      }
-      GemmDesc t;  // L21 = A21 * L11^-T
-      t.m = R; t.n = w; t.k = w; t.alpha = 1.0; t.beta = 0.0;
-      t.A = W21; t.lda = kNB; t.B = Linv; t.ldb = kNB; t.b_trans = true;
-      t.C = A21; t.ldc = lda;
-      LM_TRY(dgemm(c, t, st));
-      GemmDesc s;  // A22 -= L21 L21^T (lower triangle)
-      s.m = R; s.n = R; s.k = w; s.alpha = -1.0; s.beta = 1.0;
-      s.A = A21; s.lda = lda; s.B = A21; s.ldb = lda; s.b_trans = true; s.lower_only = true;
-      s.C = A21 + w; s.ldc = lda;
-      LM_TRY(dgemm(c, s, st));
+      LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
+    } else {
+      if (rest > 0) LM_TRY(dgemm(c, r, st));
+      LM_TRY(factor_column(j0 + w, st, 0));
     }
   }
   return zero_upper<double>(A, lda, n, st);
@@ -371,6 +424,22 @@ int dgetrs(Ctx& c, int n, int nrhs, const double* LU, long long lda, const int* 
 
 int dpotrs(Ctx& c, int n, int nrhs, const double* G, long long lda, double* B, long long ldb,
            cudaStream_t st) {
+  if (nrhs <= 4) {
+    // few right-hand sides: G packed with G^T above the diagonal, then one
+    // persistent launch per direction (the same kernels as dgetrs, with the
+    // stored diagonal of G)
+    const long long ldp = (n + 7) / 8 * 8;
+    void* ws = nullptr;
+    LM_TRY(ctx_workspace(c, 2, 256 + sizeof(double) * (size_t)n * ldp, &ws));
+    int* sync = static_cast<int*>(ws);
+    double* P = reinterpret_cast<double*>(static_cast<char*>(ws) + 256);
+    {
+      Prof p(c, kPhaseOther, 0.0, 16.0 * n * n, st);
+      LM_TRY(pack_lower_sym(P, ldp, G, lda, n, st));
+    }
+    Prof p(c, kPhaseTrsm, 2.0 * n * n * nrhs, 8.0 * n * n, st);
+    return trsv_lu<double>(P, ldp, n, nrhs, nullptr, nullptr, B, ldb, sync, ctx_status(c), st, nullptr, true, false);
+  }
   SolveBufs sb;
   LM_TRY(solve_bufs(c, n, nrhs, G, lda, B, ldb, sb, st));
   LM_TRY(forward_blocked(c, n, nrhs, sb.M, sb.ldm, false, sb.X, sb.ldx, st));

@@ -26,6 +26,9 @@ int ctx_workspace(Ctx& c, int slot, size_t bytes, void** ptr);
 // The context's look-ahead stream (highest priority, created on first use,
 // which must not be inside a stream capture) and its fork / join events.
 int ctx_aux(Ctx& c, cudaStream_t* aux, cudaEvent_t* fork, cudaEvent_t* join);
+// Whether the factorisations may fork onto the look-ahead stream (false for
+// the borrowed contexts of the entry points without allocation).
+bool ctx_lookahead(Ctx& c);
 // Worst backward error after each refinement step of the context's last
 // mixed-precision solve (both methods, in order).
 std::vector<double>& ctx_ir_history(Ctx& c);
@@ -65,9 +68,12 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
 // substitution; FP32 otherwise multiplies by the block inverses, and corr
 // (two flags per 128-row block: L, U), when given, limits the diagonal-block
 // correction step to flagged blocks.
+// unit_lower = false reads L's stored diagonal (a Cholesky factor G packed
+// with G^T above the diagonal).
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-            int* sync, int* status, cudaStream_t st, const int* corr = nullptr, bool exact = false);
+            int* sync, int* status, cudaStream_t st, const int* corr = nullptr, bool exact = false,
+            bool unit_lower = true);
 
 // --- FP64 GEMM (dgemm.cu) ----------------------------------------------------
 // C = alpha * op(A) * op(B) + beta * C, row-major.
@@ -158,6 +164,8 @@ int dnorm_inf_exact(int m, int n, const double* A, long long lda, unsigned long 
 // LU without interchanges of one w x w block (w <= 128) in place; the first
 // zero pivot goes to status[1] as base + k + 1.
 int lu_nopiv_block(double* A, long long lda, int w, int base, int* status, cudaStream_t st);
+// P (n x n) = G on and below the diagonal, G^T above it.
+int pack_lower_sym(double* P, long long ldp, const double* G, long long ldg, int n, cudaStream_t st);
 // dst (w x w) = src^T.
 int transpose_block(double* dst, long long ldd, const double* src, long long lds, int w, cudaStream_t st);
 // SPD tridiagonal solve by parallel cyclic reduction; W is 8 n doubles.

@@ -267,7 +267,7 @@ constexpr int kSLookaheadMinN = 2048;
 // after the join.  The two streams use separate split-operand scratch.
 int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
   const int nsm = ctx_num_sms(c);
-  const bool la = n >= kSLookaheadMinN && nsm > 2 * kSLookaheadSms;
+  const bool la = n >= kSLookaheadMinN && nsm > 2 * kSLookaheadSms && ctx_lookahead(c);
   void* ws = nullptr;
   LM_TRY(ctx_workspace(c, 1, (la ? 2 : 1) * scratch_set_bytes(n), &ws));
   SScratch s, sa;

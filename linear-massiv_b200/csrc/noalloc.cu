@@ -7,8 +7,10 @@
 //
 // Scratch: the 128 x 128 inverse of the current diagonal block plus a copy of
 // the panel below it, (128 + kNoAllocMaxN) x 128 doubles, and two status words
-// — about 4.3 MB that every GPU which loads this library holds until the
-// process exits.
+// — about 4.3 MB per device.  CUDA loads a library's device code lazily by
+// default, so the array is reserved on a device when the first call there
+// looks up its address (a call with n = 0 does only that); from then on the
+// device holds it until the process exits.
 #include <mutex>
 
 #include "common.cuh"
@@ -59,17 +61,17 @@ extern "C" int lm_dpotrf_noalloc(void* stream, int n, double* A, int lda, int* i
                        std::to_string(kNoAllocMaxN));
     return LM_ERR_ARG;
   }
-  if ((reinterpret_cast<uintptr_t>(A) & 15) || (lda & 1)) {
+  if (n > 0 && ((reinterpret_cast<uintptr_t>(A) & 15) || (lda & 1))) {
     lm::set_last_error("lm_dpotrf_noalloc: A must be 16-byte aligned with an even leading dimension");
     return LM_ERR_UNSUPPORTED;
   }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= lm::kMaxDevices) return LM_ERR_CUDA;
+  LM_TRY(setup(dev));  // also for n = 0: the warm-up call that reserves the array
   if (n == 0) {
     if (info) *info = 0;
     return LM_OK;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= lm::kMaxDevices) return LM_ERR_CUDA;
-  LM_TRY(setup(dev));
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   double* base = g_scratch_dev[dev];
   int* status = reinterpret_cast<int*>(base);  // error word, info word

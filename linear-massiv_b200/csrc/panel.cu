@@ -23,7 +23,7 @@
 //   NaN rule of the reference scan: if |a_jj| is NaN it stays the pivot; NaNs
 //   below it never win.
 //
-// potrf_block — Cholesky of one <=128 x 128 diagonal block in SMEM
+// potrf_block — Cholesky of one <=128 x 128 diagonal block in registers
 //   (rawCholColumnSIMDFrom, K.hs:2137-2195, for a diagonal panel).
 #include <climits>
 
@@ -499,42 +499,88 @@ template int panel_leaf<double>(Ctx&, double*, long long, int, int, int, int, in
 template int panel_leaf<float>(Ctx&, float*, long long, int, int, int, int, int, int*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
-// Cholesky of one diagonal block (w <= 128), right-looking in SMEM.
+// Cholesky of one diagonal block (w <= 128), right-looking in registers.
 // ---------------------------------------------------------------------------
 namespace {
 
+// Cholesky of the w x w block at A (w <= 128, lower triangle) in place.
+// Thread (ty, tx) of a 16 x 32 grid holds elements (ty + 16 a, tx + 32 b),
+// a < 8, b < 4, in registers.  Step k: the owner of a_kk publishes
+// 1 / sqrt(a_kk); the owners of column k form l_ik = a_ik / sqrt(a_kk) as
+// products with it and publish them; every thread subtracts l_ik l_jk from its lower elements
+// (i, j > k).  Two barriers per column, nothing re-read from memory.  A
+// non-positive (or NaN) pivot is recorded as base + k + 1 in status[1]; the
+// square root still runs, leaving the NaN the reference's arithmetic would.
 template <typename T>
 __global__ void __launch_bounds__(512) potrf_block_kernel(T* A, long long lda, int w, int base, int* status) {
-  extern __shared__ __align__(16) unsigned char sm[];
-  T* S = reinterpret_cast<T*>(sm);
-  const int ld = w + 1;
-#pragma unroll 8
-  for (int i = threadIdx.x; i < w * w; i += blockDim.x) {
-    const int r = i / w, c = i % w;
-    if (c <= r) S[r * ld + c] = A[(long long)r * lda + c];
-  }
-  __syncthreads();
+  __shared__ T rk[2];
+  __shared__ T lcol[2][128];
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  T v[8][4];
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 32 * b;
+      v[a][b] = (i < w && j <= i) ? A[(long long)i * lda + j] : (i == j ? T(1) : T(0));
+    }
+#pragma unroll 1
   for (int k = 0; k < w; ++k) {
-    if (threadIdx.x == 0) {
-      const T d = S[k * ld + k];
-      if (!(d > T(0))) atomicCAS(status + 1, 0, base + k + 1);
-      S[k * ld + k] = sqrt(d);
+    const int buf = k & 1;
+    const int ak = k >> 4, bk = k >> 5;
+    if (ty == (k & 15) && tx == (k & 31)) {
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+        if (a == ak)
+#pragma unroll
+          for (int b = 0; b < 4; ++b)
+            if (b == bk) {
+              const T d = v[a][b];
+              if (!(d > T(0))) atomicCAS(status + 1, 0, base + k + 1);
+              // 1 / sqrt(d) once, then sqrt(d) = d / sqrt(d) and every
+              // multiplier a product with it (within an ulp of the quotients)
+              const T r = rsqrt(d);
+              v[a][b] = d * r;
+              rk[buf] = r;
+            }
     }
     __syncthreads();
-    const T skk = S[k * ld + k];
-    for (int i = k + 1 + threadIdx.x; i < w; i += blockDim.x) S[i * ld + k] = S[i * ld + k] / skk;
-    __syncthreads();
-    const int m = w - k - 1;
-    for (int idx = threadIdx.x; idx < m * m; idx += blockDim.x) {
-      const int i = k + 1 + idx / m, jj = k + 1 + idx % m;
-      if (jj <= i) S[i * ld + jj] = fma(-S[i * ld + k], S[jj * ld + k], S[i * ld + jj]);
+    if (tx == (k & 31)) {
+      const T r = rk[buf];
+#pragma unroll
+      for (int b = 0; b < 4; ++b)
+        if (b == bk)
+#pragma unroll
+          for (int a = 0; a < 8; ++a) {
+            const int i = ty + 16 * a;
+            if (i > k) {
+              const T l = v[a][b] * r;
+              v[a][b] = l;
+              lcol[buf][i] = l;
+            }
+          }
     }
     __syncthreads();
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int i = ty + 16 * a;
+      if (i > k) {
+        const T li = lcol[buf][i];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int j = tx + 32 * b;
+          if (j > k && j <= i) v[a][b] = fma(-li, lcol[buf][j], v[a][b]);
+        }
+      }
+    }
   }
-  for (int i = threadIdx.x; i < w * w; i += blockDim.x) {
-    const int r = i / w, c = i % w;
-    if (c <= r) A[(long long)r * lda + c] = S[r * ld + c];
-  }
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int i = ty + 16 * a, j = tx + 32 * b;
+      if (i < w && j <= i) A[(long long)i * lda + j] = v[a][b];
+    }
 }
 
 }  // namespace
@@ -543,15 +589,7 @@ template <typename T>
 int potrf_block(Ctx& c, T* A, long long lda, int w, int base, cudaStream_t st) {
   if (w <= 0) return LM_OK;
   if (w > 128) return LM_ERR_ARG;
-  const size_t smem = sizeof(T) * (size_t)w * (w + 1);
-  static bool attr_set[kMaxDevices] = {};
-  const int dev = ctx_device(c);
-  if (!attr_set[dev]) {
-    LM_CUDA_TRY(cudaFuncSetAttribute(potrf_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(sizeof(T) * 128 * 129)));
-    attr_set[dev] = true;
-  }
-  potrf_block_kernel<T><<<1, 512, smem, st>>>(A, lda, w, base, ctx_status(c));
+  potrf_block_kernel<T><<<1, 512, 0, st>>>(A, lda, w, base, ctx_status(c));
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;

@@ -163,7 +163,7 @@ template <typename T, int RHS, bool EXACT>
 __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
                                                              int nrhs, int forward, const T* __restrict__ Dinv,
                                                              T* X, long long ldx, int* sync, int* status,
-                                                             int vec_ok, const int* corr) {
+                                                             int vec_ok, const int* corr, int unit_l) {
   constexpr int MAX_RHS = RHS;
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
   constexpr int RPL = BS / 32;  // rows per lane of the one-warp substitution
@@ -200,8 +200,8 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
       const int rr = i / BS, cc = i % BS;
       T v = T(0);
       if (rr < rows && cc < rows) {
-        if (forward ? cc < rr : cc >= rr) v = LU[(long long)(r0 + rr) * lda + r0 + cc];
-        if (forward && cc == rr) v = T(1);
+        if (forward ? (cc < rr || (!unit_l && cc == rr)) : cc >= rr) v = LU[(long long)(r0 + rr) * lda + r0 + cc];
+        if (forward && unit_l && cc == rr) v = T(1);
       } else if (rr == cc) {
         v = T(1);
       }
@@ -277,7 +277,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
         for (int h = 0; h < MAX_RHS; ++h) y[i][h] = ys[RPL * l + i][h];
       T rd[RPL];
 #pragma unroll
-      for (int i = 0; i < RPL; ++i) rd[i] = forward ? T(1) : diag.rdiag[RPL * l + i];
+      for (int i = 0; i < RPL; ++i) rd[i] = (forward && unit_l) ? T(1) : diag.rdiag[RPL * l + i];
       // (nrhs is uniform across the warp, so the guarded shuffles are too)
 #pragma unroll 1
       for (int st = 0; st < 32; ++st) {
@@ -290,14 +290,18 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
 #pragma unroll
           for (int j = 0; j < RPL; ++j) tl[i][j] = tp[i * RPL + j];
         if (l == sl) {
-          // the diagonal tile, solved in place: forward unit lower, backward upper
+          // the diagonal tile, solved in place: forward lower (unit, or
+          // scaled by the reciprocal diagonal), backward upper
           if (forward) {
 #pragma unroll
-            for (int i = 1; i < RPL; ++i)
+            for (int i = 0; i < RPL; ++i)
 #pragma unroll
-              for (int j = 0; j < i; ++j)
+              for (int h = 0; h < MAX_RHS; ++h) {
+                T v = y[i][h];
 #pragma unroll
-                for (int h = 0; h < MAX_RHS; ++h) y[i][h] = fma(-tl[i][j], y[j][h], y[i][h]);
+                for (int j = 0; j < i; ++j) v = fma(-tl[i][j], y[j][h], v);
+                y[i][h] = unit_l ? v : v * rd[i];
+              }
           } else {
 #pragma unroll
             for (int i = RPL - 1; i >= 0; --i)
@@ -442,8 +446,10 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
   return LM_OK;
 }
 
-// X (n x nrhs) <- U^-1 L^-1 X with the packed factor.  FP64 and FP32 with
-// `exact` solve the diagonal blocks by substitution (DinvL / DinvU unused);
+// X (n x nrhs) <- U^-1 L^-1 X with the packed factor (L unit lower, or with
+// its stored diagonal when unit_lower is false, as for a Cholesky factor
+// packed with its transpose).  FP64 and FP32 with `exact` solve the diagonal
+// blocks by substitution (DinvL / DinvU unused);
 // FP32 otherwise multiplies by the block inverses DinvL / DinvU.  FP64 takes
 // nrhs <= 4; FP32 any nrhs (more than 4 in passes of 16 columns).  `sync`
 // holds 4 ints of device scratch.  corr (inverse form), when given, holds two
@@ -452,7 +458,7 @@ int tri_inv_blocks(const T* LU, long long lda, int n, T* DinvL, T* DinvU, cudaSt
 // the inverse only.
 template <typename T, int RHS, bool EXACT>
 int trsv_pass(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-              int* sync, int* status, cudaStream_t st, const int* corr, int vec_ok) {
+              int* sync, int* status, cudaStream_t st, const int* corr, int vec_ok, int unit_l) {
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT;
   const int nb = (n + BS - 1) / BS;
   const int smem = EXACT ? (int)sizeof(TrsvDiag<T>) : 0;
@@ -466,9 +472,10 @@ int trsv_pass(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const
     }
   }
   LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-  trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok, corr);
+  trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok, corr,
+                                                   unit_l);
   trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok,
-                                                   corr ? corr + 1 : nullptr);
+                                                   corr ? corr + 1 : nullptr, unit_l);
   count_launch(2);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;
@@ -476,17 +483,19 @@ int trsv_pass(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const
 
 template <typename T>
 int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T* DinvU, T* X, long long ldx,
-            int* sync, int* status, cudaStream_t st, const int* corr, bool exact) {
+            int* sync, int* status, cudaStream_t st, const int* corr, bool exact, bool unit_lower) {
   constexpr int VEC = TrsvCfg<T>::VEC;
   if (n <= 0 || nrhs <= 0) return LM_OK;
   constexpr bool kF64 = sizeof(T) == 8;
-  exact = exact || kF64;
+  exact = exact || kF64 || !unit_lower;
+  const int ul = unit_lower ? 1 : 0;
   if (!exact && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
     return LM_ERR_ARG;
   const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
   if (nrhs <= MAX_RHS) {
-    if (exact) return trsv_pass<T, MAX_RHS, true>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, nullptr, vec_ok);
-    return trsv_pass<T, MAX_RHS, false>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, corr, vec_ok);
+    if (exact)
+      return trsv_pass<T, MAX_RHS, true>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, nullptr, vec_ok, ul);
+    return trsv_pass<T, MAX_RHS, false>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, corr, vec_ok, ul);
   }
   if constexpr (kF64) {
     return LM_ERR_UNSUPPORTED;
@@ -496,10 +505,10 @@ int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T
       const int nc = std::min(WIDE_RHS, nrhs - c0);
       if (exact)
         LM_TRY((trsv_pass<T, WIDE_RHS, true>(LU, lda, n, nc, DinvL, DinvU, X + c0, ldx, sync, status, st, nullptr,
-                                             vec_ok)));
+                                             vec_ok, ul)));
       else
         LM_TRY((trsv_pass<T, WIDE_RHS, false>(LU, lda, n, nc, DinvL, DinvU, X + c0, ldx, sync, status, st, corr,
-                                              vec_ok)));
+                                              vec_ok, ul)));
     }
     return LM_OK;
   }
@@ -510,8 +519,8 @@ template size_t trsv_inv_elems<double>(int);
 template int tri_inv_blocks<float>(const float*, long long, int, float*, float*, cudaStream_t);
 template int tri_inv_blocks<double>(const double*, long long, int, double*, double*, cudaStream_t);
 template int trsv_lu<float>(const float*, long long, int, int, const float*, const float*, float*, long long, int*,
-                            int*, cudaStream_t, const int*, bool);
+                            int*, cudaStream_t, const int*, bool, bool);
 template int trsv_lu<double>(const double*, long long, int, int, const double*, const double*, double*, long long,
-                             int*, int*, cudaStream_t, const int*, bool);
+                             int*, int*, cudaStream_t, const int*, bool, bool);
 
 }  // namespace lm
