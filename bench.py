@@ -65,13 +65,16 @@ def parse():
     p.add_argument("--workload", choices=["lu", "chol", "gemm", "ir", "batch", "serve"], default="ir")
     p.add_argument("--rate", type=float, default=2000.0, help="serve: Poisson arrival rate (requests/s)")
     p.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals")
-    p.add_argument("--pool", type=int, default=48, help="serve: distinct pregenerated systems")
+    p.add_argument("--pool", type=int, default=512,
+                   help="serve: pregenerated systems (each of its own order, log-uniform)")
     p.add_argument("--max-n", type=int, default=4096, help="serve: largest order")
     p.add_argument("--workers", type=int, default=8, help="serve: concurrent large solves")
     p.add_argument("--count", type=int, default=10000, help="batch: number of instances")
     p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
     p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
     p.add_argument("--kappa", type=float, default=1e6, help="ir: condition number of A (0 = uniform A)")
+    p.add_argument("--prec", choices=["tf32x3", "tf32", "bf16"], default="tf32x3",
+                   help="ir: precision of the factor's trailing updates (tf32 and bf16 are refined by GMRES-IR)")
     p.add_argument("--reflectors", type=int, default=0,
                    help="ir: Householder reflectors per side (0 = dense Haar-random orthogonal U, V)")
     p.add_argument("--n", type=int, default=16384)
@@ -90,8 +93,8 @@ def workload_name(a):
     if a.workload == "serve":
         return (f"serving loop, Poisson arrivals at {a.rate:g} req/s for {a.duration:g} s, n log-uniform in "
                 f"[16,{a.max_n}], nrhs in {{1,8,32}}, 70% general / 30% SPD, kappa log-uniform in [1e1,1e6] "
-                f"(sigma-spectrum, {a.pool} pregenerated systems), mixed-precision IR with FP64 fallback, "
-                f"HBM-budget admission")
+                f"(sigma-spectrum, 8 reflectors per side; {a.pool} pregenerated systems of continuous order), "
+                f"mixed-precision IR with FP64 fallback at padded bucket orders, HBM-budget admission")
     if a.workload == "batch":
         return (f"batched solves, {a.count} instances in one persistent launch, n uniform in [8,256], nrhs uniform "
                 f"in [1,16], half SPD (B B^T + n I, Cholesky) half general (uniform[-1,1], LU), "
@@ -104,8 +107,10 @@ def workload_name(a):
                     f"(Q of seeded Gaussian, n Householder reflectors each)")
         else:
             spec = f"A = U diag(sigma) V^T, kappa={a.kappa:g}, {a.reflectors} Householder reflectors per side"
-        return (f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU with partial pivoting + 3xTF32 "
-                f"tcgen05 updates, FP64 refinement")
+        upd = {"tf32x3": "3xTF32 tcgen05 updates, FP64 refinement",
+               "tf32": "1xTF32 tcgen05 trailing updates, FP64 GMRES-IR",
+               "bf16": "BF16 tcgen05 trailing updates, FP64 GMRES-IR"}[a.prec]
+        return f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU with partial pivoting + {upd}"
     if a.workload == "lu":
         return f"luSolve FP64 n={a.n} nrhs={a.nrhs}, A uniform[-1,1]"
     if a.workload == "chol":
@@ -255,27 +260,29 @@ def run_batch(a, world, rank, local):
 
 
 def serve_pool(a, torch):
-    """Pregenerated request systems: (A pinned, kind, kappa) with n log-uniform."""
+    """Pregenerated request systems: (A pinned, kind, kappa), n drawn continuously
+    log-uniform in [16, max_n] (so almost every system has its own order), A =
+    U diag(sigma) V^T with U, V products of 8 seeded Householder reflectors and
+    sigma geometric from 1 to 1/kappa (V = U for SPD requests)."""
     g = np.random.Generator(np.random.Philox(a.seed + 4242))
     pool = []
     for _ in range(a.pool):
-        n = int(np.exp(g.uniform(np.log(16), np.log(a.max_n))))
+        n = int(np.exp(g.uniform(np.log(16), np.log(a.max_n + 1))))
+        n = max(16, min(n, a.max_n))
         spd = g.uniform() < 0.3
         kappa = float(np.exp(g.uniform(np.log(1e1), np.log(1e6))))
         s = torch.from_numpy(kappa ** (-np.arange(n) / max(n - 1, 1))).cuda()
-        U = torch.eye(n, dtype=torch.float64, device="cuda")
-        for _ in range(4):
-            v = torch.from_numpy(g.standard_normal(n)).cuda()
-            v /= torch.linalg.norm(v)
-            U -= 2.0 * torch.outer(v, v @ U)
-        if spd:
-            V = U
-        else:
-            V = torch.eye(n, dtype=torch.float64, device="cuda")
-            for _ in range(4):
+
+        def reflectors():
+            Q = torch.eye(n, dtype=torch.float64, device="cuda")
+            for _ in range(8):
                 v = torch.from_numpy(g.standard_normal(n)).cuda()
                 v /= torch.linalg.norm(v)
-                V -= 2.0 * torch.outer(v, v @ V)
+                Q -= 2.0 * torch.outer(v, v @ Q)
+            return Q
+
+        U = reflectors()
+        V = U if spd else reflectors()
         A = ((U * s) @ V.T).cpu().pin_memory()
         pool.append((A, 1 if spd else 0, kappa))
     return pool
@@ -311,11 +318,16 @@ def run_serve(a, world, rank, local):
     def submit(i, out):
         return submit_sys(int(picks[i]), int(nrhs_of[i]), out)
 
-    # warm-up: every pool system once with each right-hand-side count
-    for j in range(len(pool)):
-        for r in (1, 8, 32):
-            srv.wait(submit_sys(j, r, outs[0]), 120.0)
-    srv.drain(120.0)
+    # warm-up (untimed): every pool system with each right-hand-side count, in
+    # two bursts, so that every worker sees the order buckets twice (the first
+    # run of a launch sequence is eager, the second is captured as a graph)
+    for _ in range(2):
+        k = 0
+        for j in range(len(pool)):
+            for r in (1, 8, 32):
+                submit_sys(j, r, outs[k % 64])
+                k += 1
+        srv.drain(600.0)
     srv.reset_stats()
     clocks = Clocks(local)
     launches0 = lmb200.launch_count()
@@ -663,13 +675,14 @@ def run_reference(a, world, rank):
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes per unit of algorithmic work of the dominant kernel, from the ncu
-# captures summarised under profiles/ (dram__bytes_read.sum + write.sum of one
-# launch divided by that launch's algorithmic bytes); the per-launch traffic
-# of this run is that ratio times its own average algorithmic bytes per launch.
+# DRAM bytes per algorithmic byte of the dominant kernel: dram__bytes_read.sum
+# + dram__bytes_write.sum of one captured launch (ncu, one trailing update of
+# the same kernel at n = 8192) divided by that launch's algorithmic bytes.  A
+# run's per-launch traffic is this ratio times its own algorithmic bytes per
+# launch (the traffic of these launches grows in proportion to their size).
 DRAM_PER_ALGO_BYTE = {
-    "dgemm": 1.11e9 / 1.090e9,     # profiles/dgemm_dmma_k128_n8192.md
-    "sgemm": 481.2e6 / 528.0e6,    # profiles/sgemm_tf32_trailing_ir_n8192.md
+    "dgemm": 1.11e9 / 1.090e9,
+    "sgemm": 481.2e6 / 528.0e6,
 }
 
 
@@ -715,8 +728,13 @@ def run_ours(a, world, rank, local):
     def step():
         if a.workload == "ir":
             it, be, info = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_int(0)
-            st = lib.lm_dgesv_ir(ctx.h, n, nrhs, P(A_d), n, P(B_d), nrhs, P(X), nrhs, 0.0, 50, ctypes.byref(it),
-                                 ctypes.byref(be), ctypes.byref(info))
+            if a.prec == "tf32x3":
+                st = lib.lm_dgesv_ir(ctx.h, n, nrhs, P(A_d), n, P(B_d), nrhs, P(X), nrhs, 0.0, 50, ctypes.byref(it),
+                                     ctypes.byref(be), ctypes.byref(info))
+            else:
+                pr = {"tf32": lmb200.IR_PREC_TF32, "bf16": lmb200.IR_PREC_BF16}[a.prec]
+                st = lib.lm_dgesv_ir_prec(ctx.h, n, nrhs, P(A_d), n, P(B_d), nrhs, P(X), nrhs, pr, 0.0, 50,
+                                          ctypes.byref(it), ctypes.byref(be), ctypes.byref(info))
             ir_stats["iters"] = it.value
             ir_stats["berr"] = be.value
             if st < 0:
@@ -806,12 +824,14 @@ def run_ours(a, world, rank, local):
             if st < 0:
                 raise lmb200.LMError(st, "fp64 step")
         Xf = torch.empty_like(B_d)
-        for _ in range(2):
+        # three warm-up solves: a workspace that grows on the first one renews
+        # the graph keys, so capture can happen as late as the third
+        for _ in range(3):
             fp64_step()
         torch.cuda.synchronize()
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record()
-        kf = max(2, a.steps // 2)
+        kf = max(3, a.steps // 2)
         for _ in range(kf):
             fp64_step()
         f1.record()
@@ -862,14 +882,21 @@ def run_ours(a, world, rank, local):
     total_ms = sum(p["ms"] for p in phases.values()) if phases else 0.0
     extra = {}
     if a.workload == "ir":
-        # the k = 128 trailing updates read and write C once per step: HBM-bound
+        # 3xTF32 trailing updates: about 190 MMA flops per byte of C traffic at
+        # k = 256, above the TF32 ridge, so the kernel is tensor-bound; the
+        # algorithmic rate counts the logical 2 m n k of each product once,
+        # the MMA-issue rate all three TF32 products
         roof_kernel = "sgemm_tf32_kernel (tcgen05 kind::tf32, 3xTF32 split: 3 MMAs per logical product)"
-        bound, unit = "hbm", "GB/s"
-        achieved = gp["bytes"] / (gp["ms"] * 1e-3) / 1e9 if gp["ms"] > 0 else None
-        peak, peak_src = measured_hbm_gbs()
-        tf32 = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
-        extra = {"tf32_mma_tflops": tf32, "tf32_peak_tflops": tf32_peak,
-                 "tf32_peak_source": "cuBLAS TF32 GEMM (FP32 storage, allow_tf32) 8192^3 measured in this run"}
+        bound, unit = "tensor", "TFLOP/s"
+        mma = gp["flops"] / (gp["ms"] * 1e-3) / 1e12 if gp["ms"] > 0 else None
+        achieved = mma / 3.0 if mma else None
+        peak = tf32_peak
+        peak_src = ("cuBLAS TF32 GEMM (FP32 storage, allow_tf32) 8192^3 measured in this run (MEASURED_PEAKS.json "
+                    "has no TF32 figure)")
+        hbm_peak, hbm_src = measured_hbm_gbs()
+        gbs = gp["bytes"] / (gp["ms"] * 1e-3) / 1e9 if gp["ms"] > 0 else None
+        extra = {"mma_issue_tflops": mma, "mma_issue_frac": (mma / peak) if (mma and peak) else None,
+                 "hbm_gbs": gbs, "hbm_frac": (gbs / hbm_peak) if gbs else None, "hbm_peak_source": hbm_src}
     else:
         roof_kernel = "dgemm_dmma_kernel (FP64 DMMA)"
         bound, unit = "tensor", "TFLOP/s"

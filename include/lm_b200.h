@@ -192,7 +192,26 @@ int lm_lu_solve_ir_host(lm_ctx* ctx, int n, int nrhs, const double* A, const dou
  * The stopping test, tolerance and FP64 residual are the same for both. */
 #define LM_IR_RBT 0
 #define LM_IR_GEPP 1
+/* Precision of the partial-pivoting factor's trailing updates (lm_dgesv_ir_prec):
+ *   LM_IR_PREC_TF32X3  three TF32 products per element (close to FP32), refined
+ *                      by classical refinement (the default of lm_dgesv_ir);
+ *   LM_IR_PREC_TF32    one TF32 product (kind::tf32), refined by GMRES-IR;
+ *   LM_IR_PREC_BF16    one BF16 product (kind::f16), refined by GMRES-IR.
+ * GMRES-IR (Carson and Higham): each correction solves A d = r with
+ * right-preconditioned flexible GMRES in FP64 (up to 30 steps, until the
+ * correction's residual falls by 1e-4), the low-precision LU applied in FP32
+ * as the preconditioner; the outer residual, update and stopping test are those
+ * of lm_dgesv_ir.  Lower precision trades factor speed for refinement steps
+ * and a smaller range of condition numbers. */
+#define LM_IR_PREC_TF32X3 0
+#define LM_IR_PREC_TF32 1
+#define LM_IR_PREC_BF16 2
 int lm_ctx_set_ir_method(lm_ctx* ctx, int method);
+/* lm_dgesv_ir with the factor precision `prec` (LM_IR_PREC_*) and partial
+ * pivoting whatever the context's method; iters counts the outer refinement
+ * steps. */
+int lm_dgesv_ir_prec(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* B, int ldb, double* X,
+                     int ldx, int prec, double tol, int max_iter, int* iters, double* berr, int* info);
 /* Method that produced the last mixed-precision result on this context
  * (LM_IR_RBT, or LM_IR_GEPP after a fallback); -1 before the first solve. */
 int lm_ctx_ir_last_method(lm_ctx* ctx, int* method);
@@ -271,13 +290,18 @@ int lm_batch_tune_set(lm_ctx* ctx, const int* nb /* [2][4] */);
  * `hbm_budget` bytes (0 = a quarter of the free memory after start-up) from
  * which every admitted request takes one block (its A, B, X, factor and
  * pivots).  Requests are admitted as soon as an execution slot and a block are
- * free; small ones (n <= small_max_n, nrhs <= 16) are run as micro-batches of
- * the persistent batch kernel (batch_lanes streams, each micro-batch taking
- * every small request queued when its lane frees up), larger ones each take
+ * free; small ones (n <= small_max_n, nrhs <= 16) run on the device-resident
+ * request loop (device_loop, below) or as micro-batches of the persistent
+ * batch kernel (batch_lanes streams, each micro-batch taking every small
+ * request queued when its lane frees up), larger ones each take
  * one of `large_workers` contexts (own stream; workspaces pre-grown at start-up
  * for max_n x max_nrhs): with large_precision LM_PREC_FP32_IR the
  * mixed-precision solve of lm_dgesv_ir (FP32 factor + FP64 refinement, for
- * general and SPD matrices alike), then FP64 LU (general) or FP64 Cholesky
+ * general and SPD matrices alike, method ir_method) at a padded order (n
+ * rounded up to a multiple of 64, 128 or 256, the system embedded with a
+ * small identity block and zero right-hand-side rows, so that requests of
+ * nearby orders replay the same captured CUDA graphs; the stopping test is
+ * that of the original order), then FP64 LU (general) or FP64 Cholesky
  * (SPD) when refinement does not converge; with LM_PREC_FP64 FP64 LU or
  * Cholesky directly.  A, B (read) and X (written) are the
  * caller's host buffers (pinned for asynchronous copies) and must stay valid
@@ -294,6 +318,18 @@ typedef struct {
   int max_n;            /* largest admissible order (default 4096) */
   int max_nrhs;         /* most right-hand sides (default 64, <= 64) */
   int nb[4];            /* batch-kernel panel width per size bucket (default 16) */
+  int ir_method;        /* factorisation of the large mixed-precision solves: LM_IR_GEPP
+                           (default) or LM_IR_RBT (solved at the request's own order: the
+                           random butterflies would mix the padding into the system) */
+  int device_loop;      /* 1 (default): small requests run on the device-resident loop, a
+                           persistent kernel of loop_ctas CTAs that claims each posted
+                           request from a ring in device memory as soon as its data has
+                           arrived, and returns after a few ms without work (relaunched
+                           when work arrives); 0: micro-batches of the batch kernel on the
+                           batch lanes.  The loop solves in FP64 (small_precision
+                           LM_PREC_FP64). */
+  int loop_ctas;        /* CTAs of the device-resident loop (default 16, which leaves every GPC
+                           room for the large solves' thread-block clusters) */
 } lm_server_config;
 typedef struct {
   long long completed, rejected, cancelled, failed, fp64_fallbacks;

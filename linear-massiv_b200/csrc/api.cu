@@ -125,7 +125,10 @@ int ctx_pinned(Ctx& c, size_t bytes, void** ptr) {
       c.pinned = nullptr;
       c.pinned_bytes = 0;
     }
-    const size_t want = std::max(bytes, (size_t)4096);
+    // 64 KB holds every user's words (the refinement norms, the GMRES dot
+    // products and coefficients), so the buffer normally never moves
+    const size_t want = std::max(bytes, (size_t)65536);
+    ++c.ws_generation;  // captured graphs that copy into the old buffer are stale
     if (cudaMallocHost(&c.pinned, want) != cudaSuccess) {
       cudaGetLastError();
       set_last_error("pinned host allocation failed");
@@ -748,6 +751,41 @@ int lm_dgesv_ir(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const do
     if (tol <= 0) tol = 1e-15 * n;
     LM_TRY(lm::reset_info(c));
     int r = ir_solve(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, "dev");
+    int inf = 0;
+    int s = lm::read_status(c, &inf);
+    if (s < 0) return s;
+    if (info) *info = inf;
+    if (r < 0) return r;
+    return inf;
+  });
+}
+
+int lm_dgesv_ir_prec(lm_ctx* ctx, int n, int nrhs, const double* A, int lda, const double* B, int ldb, double* X,
+                     int ldx, int prec, double tol, int max_iter, int* iters, double* berr, int* info) {
+  return guarded(ctx, [&](Ctx& c) {
+    if (n < 0 || nrhs < 0 || nrhs > 64 || max_iter < 1) return LM_ERR_ARG;
+    if (prec != LM_IR_PREC_TF32X3 && prec != LM_IR_PREC_TF32 && prec != LM_IR_PREC_BF16) return LM_ERR_ARG;
+    if (n == 0 || nrhs == 0) {
+      if (iters) *iters = 0;
+      if (berr) *berr = 0.0;
+      if (info) *info = 0;
+      return LM_OK;
+    }
+    if (!A || !B || !X || lda < n || ldb < nrhs || ldx < nrhs) return LM_ERR_ARG;
+    if (tol <= 0) tol = 1e-15 * n;
+    LM_TRY(lm::reset_info(c));
+    c.ir_hist.clear();
+    c.ir_last = LM_IR_GEPP;
+    auto runner = [&c, n, nrhs, A, lda, B, ldb, X, ldx, prec](const char* what,
+                                                             const std::function<int(cudaStream_t)>& body) {
+      const std::string k = std::string("gepp_p") + std::to_string(prec) + "_" + what;
+      const std::string key =
+          std::strncmp(what, "factor", 6) == 0
+              ? lm::gkey(k.c_str(), {n, (long long)A, lda})
+              : lm::gkey(k.c_str(), {n, nrhs, (long long)A, lda, (long long)B, ldb, (long long)X, ldx});
+      return lm::run_graphed(c, key, body);
+    };
+    int r = lm::dgesv_ir(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, iters, berr, c.stream, runner, prec);
     int inf = 0;
     int s = lm::read_status(c, &inf);
     if (s < 0) return s;

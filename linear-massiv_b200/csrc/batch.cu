@@ -438,7 +438,17 @@ __host__ __device__ inline Carve carve(int nmax, int rmax, int nbmax) {
   return c;
 }
 
+// Input loads: L2-only (ld.global.cg) for the device-resident consumer, whose
+// CTAs outlive the requests they read (an arena block is reused by later
+// requests, and an SM's L1 is not coherent with the copies that refill it).
+template <bool CG>
+__device__ __forceinline__ double ld_in(const double* p) {
+  if constexpr (CG) return __ldcg(p);
+  else return *p;
+}
+
 // Factor + solve one instance entirely in FP64.
+template <bool CG = false>
 __device__ void run_fp64(const BatchItem& it, const BatchArgs& g, unsigned char* sm, Fixed* fx, double* Xs,
                          int* info_out) {
   const Carve cv = carve(g.nmax, g.rmax, g.nbmax);
@@ -446,7 +456,7 @@ __device__ void run_fp64(const BatchItem& it, const BatchArgs& g, unsigned char*
   const int n = it.n, r = it.nrhs;
   double* F = g.F + it.f_off;
   int* ipiv = g.ipiv + it.p_off;
-  for (long long e = tid_(); e < (long long)n * n; e += kBT) F[e] = g.A[it.a_off + e];
+  for (long long e = tid_(); e < (long long)n * n; e += kBT) F[e] = ld_in<CG>(g.A + it.a_off + e);
   __syncthreads();
   const int info = it.kind == LM_BATCH_GENERAL ? lu_factor<double>(F, n, it.nb, ipiv, region, fx)
                                                : chol_factor<double>(F, n, it.nb, region, fx);
@@ -455,7 +465,7 @@ __device__ void run_fp64(const BatchItem& it, const BatchArgs& g, unsigned char*
   if (r == 0) return;
   double* V = Xs;
   double* Tb = reinterpret_cast<double*>(sm + cv.tb);
-  for (int e = tid_(); e < n * r; e += kBT) V[e] = g.B[it.b_off + e];
+  for (int e = tid_(); e < n * r; e += kBT) V[e] = ld_in<CG>(g.B + it.b_off + e);
   __syncthreads();
   solve_factored<double, double>(F, n, it.kind, ipiv, V, r, Tb);
 }
@@ -598,9 +608,86 @@ __global__ void __launch_bounds__(kBT, 2) batch_kernel(const BatchArgs g) {
   }
 }
 
+// Device-resident request loop (the serving loop's small requests): every CTA
+// claims the next posted request from a ring in device memory (head < tail),
+// solves it in FP64 exactly as batch_kernel would, writes X into the arena and
+// publishes info and a completion sequence number into pinned host memory.
+// An idle CTA sleeps between polls and returns after kServeIdlePolls polls
+// without work (the host relaunches the loop when new work arrives); the stop
+// word ends it at once.  No other wait.
+constexpr uint32_t kServeIdlePolls = 4000;  // x ~2 us of sleep: ~8 ms idle before returning
+
+__global__ void __launch_bounds__(kBT, 2) serve_loop_kernel(const BatchArgs g, const ServeRing rg) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  Fixed* fx = reinterpret_cast<Fixed*>(sm);
+  __shared__ int slot;
+  const Carve cv = carve(g.nmax, g.rmax, g.nbmax);
+  double* Xs = reinterpret_cast<double*>(sm + cv.xs);
+  for (;;) {
+    if (tid_() == 0) {
+      int claimed = -1;
+      for (uint32_t idle = 0; idle < kServeIdlePolls;) {
+        if (*reinterpret_cast<volatile const int*>(rg.stop) != 0) break;
+        const int h = *reinterpret_cast<volatile const int*>(rg.head);
+        const int t = *reinterpret_cast<volatile const int*>(rg.tail);
+        if (h < t) {
+          if (atomicCAS(rg.head, h, h + 1) == h) {
+            claimed = h;
+            break;
+          }
+          continue;  // another CTA took it: look again at once
+        }
+        __nanosleep(2000);
+        ++idle;
+      }
+      slot = claimed;
+    }
+    __syncthreads();
+    const int sq = slot;
+    __syncthreads();
+    if (sq < 0) return;
+    const int idx = sq % rg.cap;
+    BatchItem it;
+    {
+      const long long* src = reinterpret_cast<const long long*>(rg.items + idx);
+      long long* dst = reinterpret_cast<long long*>(&it);
+#pragma unroll
+      for (int w = 0; w < (int)(sizeof(BatchItem) / sizeof(long long)); ++w) dst[w] = __ldcg(src + w);
+    }
+    int info = 0;
+    if (it.n > 0) {
+      run_fp64<true>(it, g, sm, fx, Xs, &info);
+      __syncthreads();
+      for (int e = tid_(); e < it.n * it.nrhs; e += kBT) g.X[it.x_off + e] = Xs[e];
+    }
+    __syncthreads();
+    if (tid_() == 0) {
+      __threadfence();  // X visible in device memory before the host copies it out
+      rg.h_info[idx] = info;
+      __threadfence_system();
+      *reinterpret_cast<volatile int*>(rg.h_done + idx) = sq + 1;
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace
 
 size_t batch_smem_bytes(int nmax, int rmax, int nbmax) { return carve(nmax, rmax, nbmax).total; }
+
+int serve_loop_launch(const BatchArgs& g, const ServeRing& rg, int grid, size_t smem, cudaStream_t st) {
+  static size_t set_to[kMaxDevices] = {};
+  int dev = 0;
+  LM_CUDA_TRY(cudaGetDevice(&dev));
+  if (set_to[dev] < smem) {
+    LM_CUDA_TRY(cudaFuncSetAttribute(serve_loop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    set_to[dev] = smem;
+  }
+  serve_loop_kernel<<<grid, kBT, smem, st>>>(g, rg);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
 
 // Raise the kernel's dynamic shared-memory limit to `smem` (once per size and device).
 int batch_set_smem(size_t smem) {

@@ -198,15 +198,17 @@ int potrf_block(Ctx& c, T* A, long long lda, int w, int base, cudaStream_t st);
 // Mixed precision (ir.cu): FP32 LU with TF32 tensor-core updates, FP32
 // substitutions, FP64 refinement.  `factor_runner` runs the factorisation
 // body (so the caller can capture it into a CUDA graph).
-int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st);
+int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st, int prec = LM_IR_PREC_TF32X3);
 int sgetrs(Ctx& c, int n, int nrhs, const float* LU, long long lda, const int* ipiv, float* X, long long ldx,
            cudaStream_t st);
 // Runs a fixed launch sequence tagged "factor" or "iter" (the caller maps the
 // tag and the solve's buffers to a CUDA-graph key, or runs it eagerly).
 using IrRunner = std::function<int(const char* tag, const std::function<int(cudaStream_t)>& body)>;
+// prec (LM_IR_PREC_*): the factor's trailing-update precision; TF32 and
+// BF16 factors are refined by GMRES-IR, 3xTF32 by classical refinement.
 int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
-             const IrRunner& run);
+             const IrRunner& run, int prec = LM_IR_PREC_TF32X3);
 
 // Randomised variant (ir.cu, rbt.cu): depth-2 random butterflies on both
 // sides, FP32 LU without pivoting on the tensor cores, FP64 refinement.
@@ -274,6 +276,22 @@ struct BatchArgs {
   double tol;
   int max_iter;
 };
+// Ring of posted requests of the device-resident serving loop: descriptors
+// in device memory (items[seq % cap]), the next sequence number to claim
+// (head) and the number posted (tail), a stop word, and per slot in pinned
+// host memory the info and the completion word (seq + 1 when done).
+struct ServeRing {
+  const BatchItem* items;
+  int cap;
+  int* head;
+  const int* tail;
+  const int* stop;
+  int* h_info;
+  int* h_done;
+};
+// Launch the device-resident loop (FP64 solves of the posted requests).
+int serve_loop_launch(const BatchArgs& g, const ServeRing& rg, int grid, size_t smem, cudaStream_t st);
+
 // Dynamic shared memory of the batch kernel for the given maxima.
 size_t batch_smem_bytes(int nmax, int rmax, int nbmax);
 // Resident CTAs per SM of the batch kernel at that shared-memory size.

@@ -18,6 +18,8 @@
 #include <functional>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -30,6 +32,9 @@ void count_launch(int n);
 int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
                long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
                const float* Btlo, int max_ctas = 0, const int* gate = nullptr);
+// The same with BF16 operands (kind::f16), FP32 C and accumulation.
+int sgemm_bf16(Ctx& ctx, int m, int n, int k, float alpha, const void* A, long long lda, const void* Bt,
+               long long ldb, float beta, float* C, long long ldc, cudaStream_t st, int max_ctas = 0);
 
 
 namespace {
@@ -102,6 +107,32 @@ __global__ void split_kernel(float* dhi, float* dlo, long long ldd, const float*
     const float h = tf32_hi(a);
     dhi[(long long)r * ldd + c] = h;
     dlo[(long long)r * ldd + c] = tf32_hi(a - h);
+  }
+}
+
+// BF16 operands of the low-precision update: dst (rows x cols, ldd) =
+// bf16(src), and the transposed form dst (cols x rows) = bf16(src)^T.
+__global__ void to_bf16_kernel(__nv_bfloat16* dst, long long ldd, const float* src, long long lds, int rows,
+                               int cols) {
+  const long long total = (long long)rows * cols;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(i / cols), c = (int)(i % cols);
+    dst[(long long)r * ldd + c] = __float2bfloat16_rn(src[(long long)r * lds + c]);
+  }
+}
+__global__ void transpose_to_bf16_kernel(__nv_bfloat16* dst, long long ldd, const float* src, long long lds, int rows,
+                                         int cols) {
+  __shared__ float tile[32][33];
+  const int bx = blockIdx.x * 32, by = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = by + j, c = bx + threadIdx.x;
+    if (r < rows && c < cols) tile[j][threadIdx.x] = src[(long long)r * lds + c];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    const int r = bx + j, c = by + threadIdx.x;
+    if (r < cols && c < rows) dst[(long long)r * ldd + c] = __float2bfloat16_rn(tile[threadIdx.x][j]);
   }
 }
 
@@ -200,9 +231,26 @@ int s_trsm_unit_lower(Ctx& c, const float* L11, long long lda, int w, float* B, 
 }
 
 int s_update(Ctx& c, int m, int n, int k, float* A21, long long lda, const float* U12, float* C, SScratch& s,
-             cudaStream_t st, int max_ctas = 0) {
-  // C -= A21 (m x k) * U12 (k x n), as 3xTF32 on the tensor cores
+             cudaStream_t st, int max_ctas = 0, int prec = LM_IR_PREC_TF32X3) {
+  // C -= A21 (m x k) * U12 (k x n) on the tensor cores: 3xTF32, one TF32 or
+  // one BF16 product per element
   dim3 tb(32, 8), tg(cdiv(n, 32), cdiv(k, 32));
+  if (prec == LM_IR_PREC_BF16) {
+    auto* ab = reinterpret_cast<__nv_bfloat16*>(s.Ahi);
+    auto* bb = reinterpret_cast<__nv_bfloat16*>(s.Bhi);
+    transpose_to_bf16_kernel<<<tg, tb, 0, st>>>(bb, s.ld, U12, lda, k, n);
+    to_bf16_kernel<<<grid_of((long long)m * k), 256, 0, st>>>(ab, s.ld, A21, lda, m, k);
+    count_launch(2);
+    LM_CUDA_TRY(cudaGetLastError());
+    return sgemm_bf16(c, m, n, k, -1.0f, ab, s.ld, bb, s.ld, 1.0f, C, lda, st, max_ctas);
+  }
+  if (prec == LM_IR_PREC_TF32) {
+    transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, U12, lda, k, n);
+    split_kernel<<<grid_of((long long)m * k), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, k);
+    count_launch(2);
+    LM_CUDA_TRY(cudaGetLastError());
+    return sgemm_tf32(c, m, n, k, -1.0f, s.Ahi, s.ld, s.Bhi, s.ld, 1.0f, C, lda, st, nullptr, nullptr, max_ctas);
+  }
   transpose_split_kernel<<<tg, tb, 0, st>>>(s.Bhi, s.Blo, s.ld, U12, lda, k, n);
   split_kernel<<<grid_of((long long)m * k), 256, 0, st>>>(s.Ahi, s.Alo, s.ld, A21, lda, m, k);
   count_launch(2);
@@ -259,13 +307,14 @@ constexpr int kSLookaheadMinN = 2048;
 }  // namespace
 
 // FP32 LU with partial pivoting (the same pivot rule as the FP64 path), 128-
-// column panels factored by cluster leaves, U12 = inv(L11) A12 and every
-// Schur-complement update as 3xTF32 on tcgen05.  Look-ahead as in dgetrf:
+// column panels factored by cluster leaves, U12 = inv(L11) A12 and the
+// updates inside a panel as 3xTF32 on tcgen05; the trailing Schur-complement
+// update, where the flops are, at `prec` (3xTF32, TF32 or BF16).  Look-ahead as in dgetrf:
 // once the next panel's columns are updated, that panel is factored on the
 // priority stream (its own GEMMs capped to the SMs left free) while the rest
 // of the trailing update runs; its interchanges reach the columns right of it
 // after the join.  The two streams use separate split-operand scratch.
-int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
+int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st, int prec) {
   const int nsm = ctx_num_sms(c);
   const bool la = n >= kSLookaheadMinN && nsm > 2 * kSLookaheadSms && ctx_lookahead(c);
   void* ws = nullptr;
@@ -288,8 +337,9 @@ int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
     const int wn = std::min(kNB, m);  // next panel
     float* A11 = A + (long long)k0 * lda + k0;
     LM_TRY(s_trsm_unit_lower(c, A11, lda, w, A11 + w, lda, m, s, st));
-    // A22 -= L21 U12: the next panel's columns first
-    LM_TRY(s_update(c, m, wn, w, A11 + (long long)w * lda, lda, A11 + w, A11 + (long long)w * lda + w, s, st));
+    // A22 -= L21 U12 (at the factorisation's precision): the next panel's columns first
+    LM_TRY(s_update(c, m, wn, w, A11 + (long long)w * lda, lda, A11 + w, A11 + (long long)w * lda + w, s, st, 0,
+                    prec));
     const int rest = m - wn;
     if (la) {
       LM_CUDA_TRY(cudaEventRecord(ev_fork, st));
@@ -298,12 +348,12 @@ int sgetrf(Ctx& c, int n, float* A, long long lda, int* ipiv, cudaStream_t st) {
       LM_CUDA_TRY(cudaEventRecord(ev_join, aux));
       if (rest > 0)
         LM_TRY(s_update(c, m, rest, w, A11 + (long long)w * lda, lda, A11 + w + wn, A11 + (long long)w * lda + w + wn,
-                        s, st, nsm - kSLookaheadSms));
+                        s, st, nsm - kSLookaheadSms, prec));
       LM_CUDA_TRY(cudaStreamWaitEvent(st, ev_join, 0));
     } else {
       if (rest > 0)
         LM_TRY(s_update(c, m, rest, w, A11 + (long long)w * lda, lda, A11 + w + wn, A11 + (long long)w * lda + w + wn,
-                        s, st));
+                        s, st, 0, prec));
       LM_TRY(sgetrf_panel_rec(c, A, lda, n, k0 + w, wn, k0 + w, wn, ipiv, s, st));
     }
   }
@@ -442,6 +492,216 @@ int input_norms(int n, int nrhs, const double* A, long long lda, const double* B
   return LM_OK;
 }
 
+// ---- GMRES-IR ------------------------------------------------------------------
+// Correction equations A d = r solved by right-preconditioned flexible GMRES in
+// FP64 (Carson and Higham's GMRES-IR), the preconditioner being the low-
+// precision LU applied in FP32.  The columns of a multi-right-hand-side solve
+// run in lockstep, each with its own Krylov basis and Hessenberg matrix; the
+// Givens rotations and the small triangular solves run on the host.
+constexpr int kGmresM = 30;             // inner steps per correction
+constexpr double kGmresInnerTol = 1e-4; // relative residual of one correction
+constexpr int kDotBlocks = 128;         // CTAs of the deterministic dot products
+
+// partial[blk][p] = sum over this CTA's rows of V_i[r][c] W[r][c], p = i * nrhs + c
+// (i < count), one thread per (i, c) pair, rows in a fixed order.
+__global__ void gm_dots_kernel(int count, const double* V, long long vstride, const double* W, long long ldr, int n,
+                               int nrhs, double* partial) {
+  const int pairs = count * nrhs;
+  const int rows_per = (n + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * rows_per, r1 = min(n, r0 + rows_per);
+  for (int p = threadIdx.x; p < pairs; p += blockDim.x) {
+    const int i = p / nrhs, c = p % nrhs;
+    const double* v = V + (long long)i * vstride;
+    double acc = 0.0;
+    for (int r = r0; r < r1; ++r) acc = fma(v[(long long)r * ldr + c], W[(long long)r * ldr + c], acc);
+    partial[(long long)blockIdx.x * pairs + p] = acc;
+  }
+}
+__global__ void gm_reduce_kernel(const double* partial, int blocks, int pairs, double* out) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < pairs; p += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int b = 0; b < blocks; ++b) acc += partial[(long long)b * pairs + p];
+    out[p] = acc;
+  }
+}
+// W[r][c] (ldw) = sw * W[r][c] + sum_i coef[i * nrhs + c] * V_i[r][c] (ldr), i < count.
+__global__ void gm_combine_kernel(int count, const double* V, long long vstride, long long ldr, const double* coef,
+                                  double sw, double* W, long long ldw, int n, int nrhs) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int r = (int)(e / nrhs), c = (int)(e % nrhs);
+    double acc = sw * W[(long long)r * ldw + c];
+    for (int i = 0; i < count; ++i) acc = fma(coef[i * nrhs + c], V[(long long)i * vstride + (long long)r * ldr + c], acc);
+    W[(long long)r * ldw + c] = acc;
+  }
+}
+// Z (FP64) = D (FP32), n x nrhs, both with leading dimension ld.
+__global__ void s2d_kernel(double* Z, const float* D, long long ld, int n, int nrhs) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const long long o = (e / nrhs) * ld + e % nrhs;
+    Z[o] = (double)D[o];
+  }
+}
+
+struct GmresBufs {
+  double *V, *Z, *W, *zero, *partial, *dots, *coef;
+  long long vstride;
+  double* hdots;  // pinned host copy of dots
+};
+
+// Outer FP64 refinement with GMRES corrections.  R, D, nrm as in refine();
+// precond(D) turns D (FP32, n x ldr) into M^-1 D.  Returns LM_OK when every
+// column's normwise backward error is <= tol within max_iter corrections.
+int refine_gmres(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
+                 long long ldx, double tol, int max_iter, double* R, long long ldr, float* D, unsigned long long* nrm,
+                 GmresBufs& g, int* iters_out, double* berr_out, cudaStream_t st,
+                 const std::function<int(float*, cudaStream_t)>& precond) {
+  const int M = kGmresM;
+  const size_t hwords = 1 + 3 * 64;
+  unsigned long long* h = nullptr;
+  LM_TRY(ctx_pinned(c, sizeof(unsigned long long) * hwords + sizeof(double) * (size_t)(M + 1) * 64 * 2,
+                    reinterpret_cast<void**>(&h)));
+  double* hd = reinterpret_cast<double*>(h + hwords);       // dots from the device
+  double* hc = hd + (size_t)(M + 1) * 64;                    // coefficients to the device
+  auto dbl = [](unsigned long long u) {
+    double d;
+    std::memcpy(&d, &u, sizeof d);
+    return d;
+  };
+  LM_CUDA_TRY(cudaMemset2DAsync(X, sizeof(double) * ldx, 0, sizeof(double) * nrhs, n, st));
+  LM_TRY(copy2d<double>(R, ldr, B, ldb, n, nrhs, st));
+  LM_CUDA_TRY(cudaMemsetAsync(g.zero, 0, sizeof(double) * (size_t)n * ldr, st));
+  const int gr = grid_of((long long)n * nrhs);
+  // per-column dot products of W with V_0 .. V_{count-1} into hd (synchronises)
+  auto dots = [&](int count, const double* V, const double* W) -> int {
+    gm_dots_kernel<<<kDotBlocks, 256, 0, st>>>(count, V, g.vstride, W, ldr, n, nrhs, g.partial);
+    gm_reduce_kernel<<<cdiv(count * nrhs, 256), 256, 0, st>>>(g.partial, kDotBlocks, count * nrhs, g.dots);
+    count_launch(2);
+    LM_CUDA_TRY(cudaGetLastError());
+    LM_CUDA_TRY(cudaMemcpyAsync(hd, g.dots, sizeof(double) * count * nrhs, cudaMemcpyDeviceToHost, st));
+    LM_CUDA_TRY(cudaStreamSynchronize(st));
+    return LM_OK;
+  };
+  // W = sw W + sum_i hc[i] V_i
+  auto combine = [&](int count, const double* V, double sw, double* W, long long ldw) -> int {
+    LM_CUDA_TRY(cudaMemcpyAsync(g.coef, hc, sizeof(double) * count * nrhs, cudaMemcpyHostToDevice, st));
+    gm_combine_kernel<<<gr, 256, 0, st>>>(count, V, g.vstride, ldr, g.coef, sw, W, ldw, n, nrhs);
+    count_launch(1);
+    LM_CUDA_TRY(cudaGetLastError());
+    return LM_OK;
+  };
+  std::vector<double> H((size_t)nrhs * (M + 1) * M), cs((size_t)nrhs * M), sn((size_t)nrhs * M),
+      gv((size_t)nrhs * (M + 1)), beta(nrhs), y((size_t)nrhs * M);
+  double worst = 0.0;
+  int it = 0;
+  for (it = 1; it <= max_iter; ++it) {
+    // ---- one correction: d ~ A^-1 r by FGMRES(M) ----
+    LM_TRY(copy2d<double>(g.V, ldr, R, ldr, n, nrhs, st));
+    LM_TRY(dots(1, g.V, g.V));
+    for (int col = 0; col < nrhs; ++col) {
+      beta[col] = std::sqrt(std::max(hd[col], 0.0));
+      hc[col] = beta[col] > 0 ? 1.0 / beta[col] : 0.0;
+    }
+    LM_TRY(combine(1, g.V, 0.0, g.V, ldr));  // V_0 = r / beta
+    std::fill(H.begin(), H.end(), 0.0);
+    std::fill(gv.begin(), gv.end(), 0.0);
+    for (int col = 0; col < nrhs; ++col) gv[(size_t)col * (M + 1)] = beta[col];
+    int k = 0;
+    for (int j = 0; j < M; ++j) {
+      double* Vj = g.V + (long long)j * g.vstride;
+      double* Zj = g.Z + (long long)j * g.vstride;
+      // z_j = M^-1 v_j in FP32
+      LM_TRY(convert_d2s(D, ldr, Vj, ldr, n, nrhs, st));
+      LM_TRY(precond(D, st));
+      s2d_kernel<<<gr, 256, 0, st>>>(Zj, D, ldr, n, nrhs);
+      count_launch(1);
+      // w = A z_j (as -(0 - A z_j))
+      LM_TRY(dresidual(c, n, nrhs, A, lda, Zj, ldr, g.zero, ldr, g.W, ldr, st));
+      // classical Gram-Schmidt, twice: h = V^T w, w -= V h
+      for (int pass = 0; pass < 2; ++pass) {
+        LM_TRY(dots(j + 1, g.V, g.W));  // V^T (-w)
+        for (int col = 0; col < nrhs; ++col)
+          for (int i = 0; i <= j; ++i) {
+            const double hij = -hd[i * nrhs + col];
+            H[((size_t)col * (M + 1) + i) * M + j] += hij;
+            hc[i * nrhs + col] = hij;  // w -= h v, i.e. W = -w gains + h v
+          }
+        LM_TRY(combine(j + 1, g.V, 1.0, g.W, ldr));  // W = -w + ... stays the negated vector
+      }
+      LM_TRY(dots(1, g.W, g.W));
+      bool all_done = true;
+      for (int col = 0; col < nrhs; ++col) {
+        const double hn = std::sqrt(std::max(hd[col], 0.0));
+        H[((size_t)col * (M + 1) + j + 1) * M + j] = hn;
+        hc[col] = hn > 0 ? -1.0 / hn : 0.0;  // V_{j+1} = w / hn = -W / hn
+        // Givens rotations of this column's Hessenberg
+        double* Hcol = &H[(size_t)col * (M + 1) * M];
+        for (int i = 0; i < j; ++i) {
+          const double a = Hcol[i * M + j], b = Hcol[(i + 1) * M + j];
+          Hcol[i * M + j] = cs[(size_t)col * M + i] * a + sn[(size_t)col * M + i] * b;
+          Hcol[(i + 1) * M + j] = -sn[(size_t)col * M + i] * a + cs[(size_t)col * M + i] * b;
+        }
+        const double a = Hcol[j * M + j], b = Hcol[(j + 1) * M + j];
+        const double rr = std::hypot(a, b);
+        const double cc = rr > 0 ? a / rr : 1.0, ss = rr > 0 ? b / rr : 0.0;
+        cs[(size_t)col * M + j] = cc;
+        sn[(size_t)col * M + j] = ss;
+        Hcol[j * M + j] = rr;
+        Hcol[(j + 1) * M + j] = 0.0;
+        double* gc = &gv[(size_t)col * (M + 1)];
+        gc[j + 1] = -ss * gc[j];
+        gc[j] = cc * gc[j];
+        if (!(std::fabs(gc[j + 1]) <= kGmresInnerTol * beta[col]) && hn > 0) all_done = false;
+      }
+      k = j + 1;
+      if (all_done || k == M) break;
+      // V_{j+1} = -W / ||W||
+      double* Vn = g.V + (long long)(j + 1) * g.vstride;
+      LM_CUDA_TRY(cudaMemsetAsync(Vn, 0, sizeof(double) * (size_t)n * ldr, st));
+      LM_CUDA_TRY(cudaMemcpyAsync(g.coef, hc, sizeof(double) * nrhs, cudaMemcpyHostToDevice, st));
+      gm_combine_kernel<<<gr, 256, 0, st>>>(1, g.W, 0, ldr, g.coef, 0.0, Vn, ldr, n, nrhs);
+      count_launch(1);
+      LM_CUDA_TRY(cudaGetLastError());
+    }
+    // y = H^-1 g (k x k upper triangular per column), x += Z y
+    for (int col = 0; col < nrhs; ++col) {
+      const double* Hcol = &H[(size_t)col * (M + 1) * M];
+      const double* gc = &gv[(size_t)col * (M + 1)];
+      for (int i = k - 1; i >= 0; --i) {
+        double v = gc[i];
+        for (int l = i + 1; l < k; ++l) v -= Hcol[i * M + l] * y[(size_t)col * M + l];
+        y[(size_t)col * M + i] = Hcol[i * M + i] != 0 ? v / Hcol[i * M + i] : 0.0;
+      }
+      for (int i = 0; i < k; ++i) hc[i * nrhs + col] = y[(size_t)col * M + i];
+    }
+    LM_TRY(combine(k, g.Z, 1.0, X, ldx));
+    // ---- r = b - A x in FP64 and the stopping test ----
+    LM_TRY(dresidual(c, n, nrhs, A, lda, X, ldx, B, ldb, R, ldr, st));
+    LM_CUDA_TRY(cudaMemsetAsync(nrm + 1 + 64, 0, sizeof(unsigned long long) * 128, st));
+    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(R, ldr, n, nrhs, nrm + 1 + 64);
+    colmax_abs_kernel<<<grid_of((long long)n * nrhs), 256, 0, st>>>(X, ldx, n, nrhs, nrm + 1 + 128);
+    count_launch(2);
+    LM_CUDA_TRY(cudaMemcpyAsync(h, nrm, sizeof(unsigned long long) * hwords, cudaMemcpyDeviceToHost, st));
+    LM_CUDA_TRY(cudaStreamSynchronize(st));
+    const double anorm = dbl(h[0]);
+    worst = 0.0;
+    for (int col = 0; col < nrhs; ++col) {
+      const double rn = dbl(h[1 + 64 + col]), xn = dbl(h[1 + 128 + col]), bn = dbl(h[1 + col]);
+      const double den = anorm * xn + bn;
+      const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
+      worst = std::max(worst, (be != be) ? 1e300 : be);
+    }
+    ctx_ir_history(c).push_back(worst);
+    if (worst <= tol) break;
+  }
+  if (iters_out) *iters_out = std::min(it, max_iter);
+  if (berr_out) *berr_out = worst;
+  return worst <= tol ? LM_OK : LM_ERR_NOT_CONVERGED;
+}
+
 }  // namespace
 
 // Iterative refinement driver.  A, B, X are FP64 device buffers; X receives
@@ -449,7 +709,7 @@ int input_norms(int n, int nrhs, const double* A, long long lda, const double* B
 // LM_ERR_NOT_CONVERGED if some column misses tol after max_iter steps.
 int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const double* B, long long ldb, double* X,
              long long ldx, double tol, int max_iter, int* iters_out, double* berr_out, cudaStream_t st,
-             const IrRunner& run) {
+             const IrRunner& run, int prec) {
   const long long lda32 = (n + 31) / 32 * 32;
   const long long ldr = (nrhs + 7) / 8 * 8;
   const size_t a32_bytes = sizeof(float) * (size_t)n * lda32;
@@ -459,8 +719,17 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(2 + 3 * 64);  // 16-byte multiple
   const size_t sync_bytes = 64;
   const size_t w_bytes = sizeof(float) * (size_t)n * ldr;  // gather scratch of the interchanges
+  // GMRES-IR (low-precision factors): Krylov bases V (M + 1) and Z (M), W, a
+  // zero block, dot-product partials and coefficients
+  const bool gmres = prec != LM_IR_PREC_TF32X3;
+  const long long vstride = (long long)n * ldr;
+  const size_t gm_bytes =
+      gmres ? sizeof(double) * ((size_t)(2 * kGmresM + 3) * vstride + (size_t)kDotBlocks * (kGmresM + 1) * 64 +
+                                2 * (size_t)(kGmresM + 1) * 64)
+            : 0;
   void* ws = nullptr;
-  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + sync_bytes + w_bytes, &ws));
+  LM_TRY(ctx_workspace(c, 0, a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + sync_bytes + w_bytes + gm_bytes,
+                       &ws));
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   int* ipiv = reinterpret_cast<int*>(p + a32_bytes);
@@ -470,13 +739,33 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   int* tsync = reinterpret_cast<int*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes);
   float* Wg = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + sync_bytes);
   if (nrhs > 64) return LM_ERR_UNSUPPORTED;
+  GmresBufs gb{};
+  if (gmres) {
+    double* q = reinterpret_cast<double*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes + nrm_bytes + sync_bytes +
+                                          w_bytes);
+    gb.vstride = vstride;
+    gb.V = q;
+    gb.Z = gb.V + (size_t)(kGmresM + 1) * vstride;
+    gb.W = gb.Z + (size_t)kGmresM * vstride;
+    gb.zero = gb.W + vstride;
+    gb.partial = gb.zero + vstride;
+    gb.dots = gb.partial + (size_t)kDotBlocks * (kGmresM + 1) * 64;
+    gb.coef = gb.dots + (size_t)(kGmresM + 1) * 64;
+  }
 
   LM_TRY(input_norms(n, nrhs, A, lda, B, ldb, nrm, nrm_bytes, st));
   // factor fl32(A)
-  LM_TRY(run("factor", [&](cudaStream_t s) {
+  LM_TRY(run(gmres ? (prec == LM_IR_PREC_BF16 ? "factor_bf16" : "factor_tf32") : "factor", [&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
-    return sgetrf(c, n, A32, lda32, ipiv, s);
+    return sgetrf(c, n, A32, lda32, ipiv, s, prec);
   }));
+  auto precond = [&](float* Dd, cudaStream_t s) {
+    LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
+    return trsv_lu<float>(A32, lda32, n, nrhs, nullptr, nullptr, Dd, ldr, tsync, ctx_status(c), s, nullptr, true);
+  };
+  if (gmres)  // the host steers the Krylov steps: these run without graph capture
+    return refine_gmres(c, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, R, ldr, D, nrm, gb, iters_out, berr_out,
+                        st, precond);
   return refine(c, n, n, nrhs, A, lda, B, ldb, X, ldx, tol, max_iter, false, R, ldr, D, nrm, iters_out, berr_out, st, run,
                 [&](float* Dd, cudaStream_t s) {
                   {

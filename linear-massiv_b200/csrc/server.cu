@@ -3,15 +3,20 @@
 // Requests (A_i X_i = B_i, host buffers) are queued by lm_server_submit and
 // admitted as soon as an execution slot and enough of the device arena are
 // free; their work overlaps on the device:
-//   small requests (n <= small_max_n, nrhs <= 16) are gathered into
-//     micro-batches: whenever a batch lane is idle it takes every queued small
-//     request that fits and runs them as ONE launch of the persistent batch
-//     kernel (batch.cu) on its own stream; requests arriving meanwhile join
-//     the next micro-batch on whichever lane frees first;
+//   small requests (n <= small_max_n, nrhs <= 16) go to the device-resident
+//     request loop (device_loop): a persistent kernel whose CTAs each claim
+//     the next request posted into a ring in device memory, solve it and
+//     publish its completion into pinned host memory, so a request starts as
+//     soon as its data has arrived; or, with device_loop off, they are
+//     gathered into micro-batches: whenever a batch lane is idle it takes
+//     every queued small request that fits and runs them as ONE launch of the
+//     persistent batch kernel (batch.cu) on its own stream;
 //   larger requests each take a worker (own context, stream and pre-grown
 //     workspace): mixed-precision LU with FP64 refinement (lm_dgesv_ir) for
-//     general and SPD requests alike, then FP64 LU (general) or FP64 Cholesky
-//     (SPD) when refinement does not converge or the FP32 factor breaks down.
+//     general and SPD requests alike, solved at a padded bucket order so that
+//     the worker replays captured CUDA graphs for orders it has not seen, then
+//     FP64 LU (general) or FP64 Cholesky (SPD) when refinement does not
+//     converge or the FP32 factor breaks down.
 // Admission by HBM footprint: every admitted request holds one block of a
 // device arena (its A, B, X, factor and pivots); a request is admitted only
 // when its block can be carved from the free space (first fit, coalescing on
@@ -47,6 +52,34 @@ double now_s() {
 
 constexpr size_t kAlign = 256;
 size_t rup(size_t a) { return (a + kAlign - 1) / kAlign * kAlign; }
+
+// Order a large request is solved at: n rounded up to a multiple of 64 (up to
+// 1024), 128 (up to 2048) or 256.  Requests of every order in one of these
+// buckets run the same launch sequence on the same worker buffers, so their
+// captured CUDA graphs are replayed instead of re-launching every kernel:
+// with orders drawn from a continuum almost every request would otherwise be
+// a shape never seen before.  At most 6% extra order (from 1024 up; 1024 / n
+// below it, where the solves are short).
+int padded_order(int n) {
+  const int q = n <= 1024 ? 64 : n <= 2048 ? 128 : 256;
+  return (n + q - 1) / q * q;
+}
+
+// Diagonal of the padding: the system is embedded as [[A, 0], [0, c I]] with
+// B padded by zero rows, so the padded unknowns are exactly zero and the first
+// n rows of the solution are A's.  A small power of two keeps ||A_p||_inf =
+// ||A||_inf (the refinement's stopping test) for any A of norm >= c, and the
+// partial-pivoting search never prefers a padding row over a nonzero in A.
+constexpr double kPadDiag = 1.0 / (1 << 30);
+
+__global__ void embed_kernel(double* Ap, int np, const double* A, int n, double c) {
+  const long long total = (long long)np * np;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / np), j = (int)(e % np);
+    Ap[e] = (i < n && j < n) ? A[(long long)i * n + j] : (i == j ? c : 0.0);
+  }
+}
 
 // First-fit sub-allocator over one device allocation.
 struct Arena {
@@ -156,6 +189,37 @@ struct Worker {
   double *Aw = nullptr, *Bw = nullptr, *Xw = nullptr;
 };
 
+// Device-resident request loop for the small requests: the feeder thread
+// copies each admitted request into its arena block and posts its descriptor
+// into a ring in device memory, then advances the ring's tail, all on one copy
+// stream (so the device sees the data before the tail that announces it); the
+// loop kernel (serve_loop_kernel) claims and solves posted requests and writes
+// a completion word into pinned host memory, which the poller thread watches
+// before it copies X out and completes the request.  The kernel returns after
+// a few milliseconds without work; posting or polling relaunches it.
+struct DeviceLoop {
+  int cap = 0, ctas = 0;
+  size_t smem = 0;
+  cudaStream_t feed = nullptr, cons = nullptr, d2h = nullptr;
+  lm::BatchItem* d_items = nullptr;
+  int* d_ctl = nullptr;  // [0] head, [1] tail, [2] stop
+  lm::BatchItem* h_items = nullptr;
+  int* h_tail = nullptr;   // per slot: the tail value that posts it
+  int* h_info = nullptr;   // mapped: written by the loop
+  int* h_done = nullptr;   // mapped: seq + 1 once solved
+  cudaEvent_t ev_exit = nullptr;
+  std::mutex launch_mu;
+  bool running = false;    // a launch was made whose end has not been seen
+  long long launches = 0, solved = 0;
+  int next_seq = 0;
+  std::deque<Req*> to_post;          // admitted, waiting for the feeder
+  std::vector<Req*> posted;          // slot -> request (nullptr when free)
+  std::vector<int> seq_of;           // slot -> sequence number
+  int in_ring = 0;
+  std::thread feeder, poller;
+  std::condition_variable cv_feed, cv_poll;
+};
+
 }  // namespace
 
 struct lm_server {
@@ -169,6 +233,7 @@ struct lm_server {
   Arena arena;
   std::vector<Lane*> lanes;
   std::vector<Worker*> workers;
+  DeviceLoop* loop = nullptr;  // small requests on the device-resident loop (cfg.device_loop)
   std::vector<double> lat_ms;
   long long next_id = 1, completed = 0, rejected = 0, cancelled = 0, fallbacks = 0, failed = 0;
   long long ir_solves = 0, ir_gepp = 0, ir_iterations = 0;
@@ -215,6 +280,24 @@ bool admit(lm_server* s, Req* r) {  // under s->mu
 
 // Hand queued requests to idle lanes / workers.  Under s->mu.
 void pump(lm_server* s) {
+  // small requests on the device-resident loop: admitted in arrival order
+  // while the ring has room
+  if (s->loop) {
+    DeviceLoop* L = s->loop;
+    bool any = false;
+    for (auto it = s->pending.begin(); it != s->pending.end();) {
+      Req* r = *it;
+      if (!r->small) {
+        ++it;
+        continue;
+      }
+      if (L->in_ring + (int)L->to_post.size() >= L->cap || !admit(s, r)) break;
+      it = s->pending.erase(it);
+      L->to_post.push_back(r);
+      any = true;
+    }
+    if (any) L->cv_feed.notify_one();
+  }
   // small requests: one micro-batch per idle lane, in arrival order
   for (Lane* ln : s->lanes) {
     if (ln->busy) continue;
@@ -371,9 +454,20 @@ int worker_solve(lm_server* s, Worker* w, Req* r) {
   if (s->cfg.large_precision == LM_PREC_FP32_IR) {
     int it = 0;
     double be = 0;
-    LM_CUDA_TRY(cudaMemcpyAsync(w->Aw, dA, nn, cudaMemcpyDeviceToDevice, st));
+    // solved at the bucket order in the worker's fixed buffers (graph replay);
+    // the randomised method mixes every row and column, so it would mix the
+    // padding in too: it solves at the request's own order
+    const int np = s->cfg.ir_method == LM_IR_GEPP ? padded_order(r->n) : r->n;
+    const long long tot = (long long)np * np;
+    embed_kernel<<<(int)std::min<long long>((tot + 255) / 256, 4096), 256, 0, st>>>(w->Aw, np, dA, r->n, kPadDiag);
+    lm::count_launch(1);
+    LM_CUDA_TRY(cudaGetLastError());
     LM_CUDA_TRY(cudaMemcpyAsync(w->Bw, dB, nr, cudaMemcpyDeviceToDevice, st));
-    rc = lm_dgesv_ir(w->ctx, r->n, r->nrhs, w->Aw, r->n, w->Bw, r->nrhs, w->Xw, r->nrhs, 0.0, 30, &it, &be, &info);
+    if (np > r->n)
+      LM_CUDA_TRY(cudaMemsetAsync(w->Bw + (size_t)r->n * r->nrhs, 0, sizeof(double) * (size_t)(np - r->n) * r->nrhs, st));
+    // the stopping test of the original order: 1e-15 n
+    rc = lm_dgesv_ir(w->ctx, np, r->nrhs, w->Aw, np, w->Bw, r->nrhs, w->Xw, r->nrhs, 1e-15 * r->n, 30, &it, &be,
+                     &info);
     lm_ctx_ir_last_method(w->ctx, &r->ir_method);
     if (rc == LM_OK) {
       LM_CUDA_TRY(cudaMemcpyAsync(dX, w->Xw, nr, cudaMemcpyDeviceToDevice, st));
@@ -419,6 +513,161 @@ void worker_run(Worker* w) {
   }
 }
 
+lm::BatchArgs loop_args(lm_server* s) {
+  char* base = s->arena.base;
+  lm::BatchArgs g{};
+  g.items = nullptr;
+  g.count = 0;
+  g.prec = LM_PREC_FP64;
+  g.nmax = std::max(1, s->cfg.small_max_n);
+  g.rmax = 16;
+  g.nbmax = 32;
+  g.A = reinterpret_cast<const double*>(base);
+  g.B = reinterpret_cast<const double*>(base);
+  g.X = reinterpret_cast<double*>(base);
+  g.F = reinterpret_cast<double*>(base);
+  g.ipiv = reinterpret_cast<int*>(base);
+  g.tol = 0.0;
+  g.max_iter = 0;
+  return g;
+}
+
+// (Re)launch the loop kernel unless a launch is still running.
+int loop_ensure_running(lm_server* s) {
+  DeviceLoop* L = s->loop;
+  std::lock_guard<std::mutex> lk(L->launch_mu);
+  if (L->running) {
+    const cudaError_t q = cudaEventQuery(L->ev_exit);
+    if (q == cudaErrorNotReady) return LM_OK;
+    if (q != cudaSuccess) return LM_ERR_CUDA;
+    L->running = false;
+  }
+  lm::ServeRing rg;
+  rg.items = L->d_items;
+  rg.cap = L->cap;
+  rg.head = L->d_ctl;
+  rg.tail = L->d_ctl + 1;
+  rg.stop = L->d_ctl + 2;
+  rg.h_info = L->h_info;
+  rg.h_done = L->h_done;
+  LM_TRY(lm::serve_loop_launch(loop_args(s), rg, L->ctas, L->smem, L->cons));
+  LM_CUDA_TRY(cudaEventRecord(L->ev_exit, L->cons));
+  L->running = true;
+  ++L->launches;
+  return LM_OK;
+}
+
+void loop_feeder(lm_server* s) {
+  DeviceLoop* L = s->loop;
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    L->cv_feed.wait(lk, [&] { return !L->to_post.empty() || s->stopping; });
+    if (L->to_post.empty() && s->stopping) return;
+    std::vector<Req*> batch(L->to_post.begin(), L->to_post.end());
+    L->to_post.clear();
+    // slots: the next free sequence numbers (the ring has room: pump checked)
+    std::vector<int> slots;
+    for (Req* r : batch) {
+      const int sq = L->next_seq++;
+      const int idx = sq % L->cap;
+      L->posted[idx] = r;
+      L->seq_of[idx] = sq;
+      L->h_done[idx] = 0;
+      ++L->in_ring;
+      slots.push_back(sq);
+    }
+    lk.unlock();
+    char* base = s->arena.base;
+    int err = LM_OK;
+    for (size_t i = 0; i < batch.size() && err == LM_OK; ++i) {
+      Req* r = batch[i];
+      const int sq = slots[i], idx = sq % L->cap;
+      char* blk = base + r->off;
+      lm::BatchItem& it = L->h_items[idx];
+      it.a_off = (long long)((r->off + r->oA) / 8);
+      it.b_off = (long long)((r->off + r->oB) / 8);
+      it.x_off = (long long)((r->off + r->oX) / 8);
+      it.f_off = (long long)((r->off + r->oF) / 8);
+      it.p_off = (long long)((r->off + r->oP) / 4);
+      it.n = r->n;
+      it.nrhs = r->nrhs;
+      it.kind = r->kind;
+      it.nb = s->cfg.nb[lm::batch_bucket(std::max(r->n, 1))];
+      it.index = idx;
+      L->h_tail[idx] = sq + 1;
+      if (cudaMemcpyAsync(blk + r->oA, r->A, (size_t)r->n * r->n * 8, cudaMemcpyHostToDevice, L->feed) != cudaSuccess ||
+          cudaMemcpyAsync(blk + r->oB, r->B, (size_t)r->n * r->nrhs * 8, cudaMemcpyHostToDevice, L->feed) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(L->d_items + idx, &it, sizeof it, cudaMemcpyHostToDevice, L->feed) != cudaSuccess ||
+          cudaMemcpyAsync(L->d_ctl + 1, L->h_tail + idx, sizeof(int), cudaMemcpyHostToDevice, L->feed) != cudaSuccess)
+        err = LM_ERR_CUDA;
+    }
+    if (err == LM_OK) err = loop_ensure_running(s);
+    lk.lock();
+    if (err != LM_OK) {
+      // nothing of this batch is in the ring as far as the host is concerned
+      for (size_t i = 0; i < batch.size(); ++i) {
+        const int idx = slots[i] % L->cap;
+        L->posted[idx] = nullptr;
+        --L->in_ring;
+        batch[i]->status = err;
+        complete(s, batch[i]);
+      }
+      s->cv_done.notify_all();
+    }
+    L->cv_poll.notify_one();
+  }
+}
+
+void loop_poller(lm_server* s) {
+  DeviceLoop* L = s->loop;
+  cudaSetDevice(s->device);
+  std::unique_lock<std::mutex> lk(s->mu);
+  for (;;) {
+    L->cv_poll.wait_for(lk, std::chrono::microseconds(200), [&] { return L->in_ring > 0 || s->stopping; });
+    if (L->in_ring == 0) {
+      if (s->stopping) return;
+      continue;
+    }
+    // requests whose completion word is set
+    std::vector<std::pair<Req*, int>> done;
+    for (int idx = 0; idx < L->cap && (int)done.size() < L->in_ring; ++idx) {
+      Req* r = L->posted[idx];
+      if (r && *reinterpret_cast<volatile int*>(L->h_done + idx) == L->seq_of[idx] + 1) done.push_back({r, idx});
+    }
+    if (done.empty()) {
+      lk.unlock();
+      loop_ensure_running(s);  // a launch that ran out of idle polls before the post
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+      lk.lock();
+      continue;
+    }
+    lk.unlock();
+    int err = LM_OK;
+    char* base = s->arena.base;
+    for (auto& d : done) {
+      Req* r = d.first;
+      if (cudaMemcpyAsync(r->X, base + r->off + r->oX, (size_t)r->n * r->nrhs * 8, cudaMemcpyDeviceToHost, L->d2h) !=
+          cudaSuccess)
+        err = LM_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(L->d2h) != cudaSuccess) err = LM_ERR_CUDA;
+    lk.lock();
+    for (auto& d : done) {
+      Req* r = d.first;
+      L->posted[d.second] = nullptr;
+      --L->in_ring;
+      r->status = err != LM_OK ? err : L->h_info[d.second];
+      r->iters = 0;
+      ++L->solved;
+      complete(s, r);
+    }
+    pump(s);
+    s->cv_done.notify_all();
+  }
+}
+
 void server_stop(lm_server* s) {
   {
     std::unique_lock<std::mutex> lk(s->mu);
@@ -434,6 +683,20 @@ void server_stop(lm_server* s) {
     s->stopping = true;
     for (Lane* ln : s->lanes) ln->cv.notify_all();
     for (Worker* w : s->workers) w->cv.notify_all();
+    if (s->loop) {
+      s->loop->cv_feed.notify_all();
+      s->loop->cv_poll.notify_all();
+    }
+  }
+  if (s->loop) {
+    DeviceLoop* L = s->loop;
+    if (L->feeder.joinable()) L->feeder.join();
+    if (L->poller.joinable()) L->poller.join();
+    if (L->d_ctl) {
+      const int one = 1;  // end a running loop at once
+      cudaMemcpy(L->d_ctl + 2, &one, sizeof one, cudaMemcpyHostToDevice);
+      if (L->cons) cudaStreamSynchronize(L->cons);
+    }
   }
   for (Lane* ln : s->lanes)
     if (ln->th.joinable()) ln->th.join();
@@ -454,6 +717,18 @@ void server_free(lm_server* s) {
     if (ln->st) cudaStreamDestroy(ln->st);
     delete ln;
   }
+  if (DeviceLoop* L = s->loop) {
+    cudaFree(L->d_items);
+    cudaFree(L->d_ctl);
+    cudaFreeHost(L->h_items);
+    cudaFreeHost(L->h_tail);
+    cudaFreeHost(L->h_info);
+    cudaFreeHost(L->h_done);
+    if (L->ev_exit) cudaEventDestroy(L->ev_exit);
+    for (cudaStream_t x : {L->feed, L->cons, L->d2h})
+      if (x) cudaStreamDestroy(x);
+    delete L;
+  }
   for (Worker* w : s->workers) {
     if (w->ctx) lm_ctx_destroy(w->ctx);
     cudaFree(w->Aw);
@@ -469,7 +744,7 @@ void server_free(lm_server* s) {
 // Grow a worker context's workspaces to the largest admissible request with
 // one solve of each kind (SPD diagonal matrix, so every path succeeds).
 int prewarm(lm_server* s, Worker* w) {
-  const int n = s->cfg.max_n, r = s->cfg.max_nrhs;
+  const int n = padded_order(s->cfg.max_n), r = s->cfg.max_nrhs;
   double *A = nullptr, *B = nullptr, *X = nullptr;
   int* P = nullptr;
   const size_t nn = (size_t)n * n * 8, nr = (size_t)n * r * 8;
@@ -517,7 +792,9 @@ int server_init(lm_server* s) {
     s->workers.push_back(w);
     LM_TRY(lm_ctx_create(&w->ctx, s->device));
     lm::ctx_set_graph_cache(w->ctx, 256);
-    const size_t nn = (size_t)s->cfg.max_n * s->cfg.max_n, nr = (size_t)s->cfg.max_n * s->cfg.max_nrhs;
+    LM_TRY(lm_ctx_set_ir_method(w->ctx, s->cfg.ir_method));
+    const size_t np = (size_t)padded_order(s->cfg.max_n);
+    const size_t nn = np * np, nr = np * s->cfg.max_nrhs;
     LM_CUDA_TRY(cudaMalloc(&w->Aw, sizeof(double) * nn));
     LM_CUDA_TRY(cudaMalloc(&w->Bw, sizeof(double) * nr));
     LM_CUDA_TRY(cudaMalloc(&w->Xw, sizeof(double) * nr));
@@ -555,6 +832,29 @@ int server_init(lm_server* s) {
   // the batch kernel's shared-memory limit for the largest micro-batch shape
   int per_sm = 0;
   LM_TRY(lm::batch_occupancy(lm::batch_smem_bytes(s->cfg.small_max_n, 16, 32), &per_sm));
+  if (s->cfg.device_loop) {
+    DeviceLoop* L = new DeviceLoop;
+    s->loop = L;
+    L->cap = 8192;
+    L->ctas = std::max(1, std::min(s->cfg.loop_ctas, s->num_sms));
+    L->smem = lm::batch_smem_bytes(std::max(1, s->cfg.small_max_n), 16, 32);
+    L->posted.assign(L->cap, nullptr);
+    L->seq_of.assign(L->cap, -1);
+    LM_CUDA_TRY(cudaStreamCreateWithFlags(&L->feed, cudaStreamNonBlocking));
+    LM_CUDA_TRY(cudaStreamCreateWithFlags(&L->cons, cudaStreamNonBlocking));
+    LM_CUDA_TRY(cudaStreamCreateWithFlags(&L->d2h, cudaStreamNonBlocking));
+    LM_CUDA_TRY(cudaEventCreateWithFlags(&L->ev_exit, cudaEventDisableTiming));
+    LM_CUDA_TRY(cudaMalloc(&L->d_items, sizeof(lm::BatchItem) * L->cap));
+    LM_CUDA_TRY(cudaMalloc(&L->d_ctl, sizeof(int) * 4));
+    LM_CUDA_TRY(cudaMemset(L->d_ctl, 0, sizeof(int) * 4));
+    LM_CUDA_TRY(cudaMallocHost(&L->h_items, sizeof(lm::BatchItem) * L->cap));
+    LM_CUDA_TRY(cudaMallocHost(&L->h_tail, sizeof(int) * L->cap));
+    LM_CUDA_TRY(cudaHostAlloc(&L->h_info, sizeof(int) * L->cap, cudaHostAllocMapped));
+    LM_CUDA_TRY(cudaHostAlloc(&L->h_done, sizeof(int) * L->cap, cudaHostAllocMapped));
+    std::memset(L->h_done, 0, sizeof(int) * L->cap);
+    L->feeder = std::thread(loop_feeder, s);
+    L->poller = std::thread(loop_poller, s);
+  }
   for (Lane* ln : s->lanes) ln->th = std::thread(lane_run, ln);
   for (Worker* w : s->workers) w->th = std::thread(worker_run, w);
   return LM_OK;
@@ -577,6 +877,9 @@ int lm_server_default_config(lm_server_config* c) {
   c->max_n = 4096;
   c->max_nrhs = 64;
   for (int b = 0; b < 4; ++b) c->nb[b] = 16;
+  c->ir_method = LM_IR_GEPP;
+  c->device_loop = 1;
+  c->loop_ctas = 16;
   return LM_OK;
 }
 
@@ -592,7 +895,9 @@ int lm_server_create(lm_server** out, int device, const lm_server_config* cfg) {
   if (c.large_workers < 1 || c.large_workers > 32 || c.batch_lanes < 1 || c.batch_lanes > 8 || c.small_max_n < 0 ||
       c.small_max_n > lm::BatchLimits::kMaxN || c.max_batch < 1 || c.max_n < 1 || c.max_nrhs < 1 ||
       c.max_nrhs > 64 || (c.small_precision != LM_PREC_FP64 && c.small_precision != LM_PREC_FP32_IR) ||
-      (c.large_precision != LM_PREC_FP64 && c.large_precision != LM_PREC_FP32_IR))
+      (c.large_precision != LM_PREC_FP64 && c.large_precision != LM_PREC_FP32_IR) ||
+      (c.ir_method != LM_IR_RBT && c.ir_method != LM_IR_GEPP) || (c.device_loop && c.loop_ctas < 1) ||
+      (c.device_loop && c.small_precision != LM_PREC_FP64))
     return LM_ERR_ARG;
   for (int b = 0; b < 4; ++b)
     if (c.nb[b] != 8 && c.nb[b] != 16 && c.nb[b] != 32) return LM_ERR_ARG;
@@ -758,6 +1063,10 @@ int lm_server_stats(lm_server* s, lm_server_stats_t* o) {
   for (Lane* ln : s->lanes) {
     batches += ln->batches;
     small += ln->solved;
+  }
+  if (s->loop) {
+    batches += s->loop->launches;
+    small += s->loop->solved;
   }
   o->micro_batches = batches;
   o->small_solved = small;

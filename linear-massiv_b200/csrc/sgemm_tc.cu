@@ -1,13 +1,17 @@
-// FP32-storage GEMM on the 5th-generation tensor cores (tcgen05, kind::tf32),
-// the trailing-matrix contraction of the low-precision factorisation used by
-// iterative refinement:  C = alpha * A * Bt^T + beta * C,  all FP32 row-major,
-// A m x k and Bt n x k (both K-major), products in TF32, accumulation in FP32.
+// Low-precision GEMM on the 5th-generation tensor cores (tcgen05), the
+// trailing-matrix contraction of the factorisation used by iterative
+// refinement:  C = alpha * A * Bt^T + beta * C,  C FP32 row-major, A m x k and
+// Bt n x k (both K-major), accumulation in FP32.  Operand modes:
+//   kTf32    FP32 storage, one kind::tf32 product;
+//   kTf32x3  FP32 high parts + FP32 remainders, three kind::tf32 products
+//            (hi*hi + hi*lo + lo*hi: close to FP32 accuracy);
+//   kBf16    BF16 storage, one kind::f16 product with BF16 operands.
 //
 // One CTA per SM, persistent over 128 x 128 output tiles:
-//   warp 0      TMA producer: A / Bt k-slices (32 floats = one 128-byte
-//               swizzle row) into the stage ring, and an L2 prefetch of each
-//               tile's C block as the tile starts;
-//   warp 1      MMA issuer (one thread): 4 x tcgen05.mma (K = 8) per slice
+//   warp 0      TMA producer: A / Bt k-slices (one 128-byte swizzle row: 32
+//               FP32 or 64 BF16 elements) into the stage ring, and an L2
+//               prefetch of each tile's C block as the tile starts;
+//   warp 1      MMA issuer (one thread): 4 x tcgen05.mma (32 bytes of K) per slice
 //               into a TMEM accumulator (two 128-column buffers, so the next
 //               tile's MMAs overlap this tile's epilogue); tcgen05.commit
 //               releases smem stages and hands accumulators to the epilogue;
@@ -23,17 +27,22 @@ namespace lm {
 
 namespace {
 
-constexpr int TBM = 128, TBN = 128, TBK = 32;  // tile M, N; k-slice in floats (128 B)
-constexpr int T_A_BYTES = TBM * TBK * 4;   // 16 KB
-constexpr int T_B_BYTES = TBN * TBK * 4;   // 16 KB
+enum : int { kTf32 = 0, kTf32x3 = 1, kBf16 = 2 };
+
+constexpr int TBM = 128, TBN = 128;        // tile M, N; a k-slice is one 128-byte swizzle row
+constexpr int T_A_BYTES = TBM * 128;       // 16 KB
+constexpr int T_B_BYTES = TBN * 128;       // 16 KB
 constexpr int T_C_BYTES = TBM * TBN * 4;   // 64 KB (4 boxes of 32 columns)
 constexpr int T_THREADS = 6 * 32;
 
-// SPLIT = 3xTF32: operands arrive as exactly-TF32 high parts and FP32
-// remainders; each k-step issues hi*hi + hi*lo + lo*hi, which restores close
-// to FP32 accuracy.  Stages hold 2 (plain) or 4 (split) operand tiles.
-template <bool SPLIT>
+// Per mode: elements per 128-byte k-slice (TBK), whether the operands come
+// as high parts + remainders (SPLIT: each k-step issues hi*hi + hi*lo + lo*hi),
+// and the operand stages (2 for split, 4 otherwise).  Every MMA reads 32
+// bytes of K (8 TF32 or 16 BF16 elements), four per slice.
+template <int MODE>
 struct TcCfg {
+  static constexpr bool SPLIT = MODE == kTf32x3;
+  static constexpr int TBK = MODE == kBf16 ? 64 : 32;
   static constexpr int STAGES = SPLIT ? 2 : 4;
   static constexpr int STAGE_BYTES = (T_A_BYTES + T_B_BYTES) * (SPLIT ? 2 : 1);
   static constexpr int SMEM = STAGES * STAGE_BYTES + T_C_BYTES + 1024 + 256;
@@ -67,6 +76,15 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t dtmem, uint64_t adesc, uint
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void tc_mma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                           uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
 }
@@ -120,8 +138,12 @@ __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t smem_addr) {
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
-// D f32, A/B tf32, both K-major, N = 128, M = 128.
+// Instruction descriptors: D f32 (bits 4-5 = 1), A and B format (bits 7-9,
+// 10-12: 2 = TF32 for kind::tf32, 1 = BF16 for kind::f16), both K-major,
+// N >> 3 (bits 17-22), M >> 4 (bits 24-28).
 constexpr uint32_t kIdescTF32 = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TBN >> 3) << 17) |
+                                ((uint32_t)(TBM >> 4) << 24);
+constexpr uint32_t kIdescBF16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) |
                                 ((uint32_t)(TBM >> 4) << 24);
 
 // byte offset of element (r, c) in a [128 rows][32 floats] 128B-swizzled box
@@ -129,13 +151,15 @@ __device__ __forceinline__ uint32_t cbox_off(int r, int c) {
   return (uint32_t)(r * 128 + ((((c >> 2) ^ (r & 7))) << 4) + ((c & 3) << 2));
 }
 
-template <bool SPLIT>
+template <int MODE>
 __global__ void __launch_bounds__(T_THREADS, 1)
     sgemm_tf32_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                       const __grid_constant__ CUtensorMap tmC, const __grid_constant__ CUtensorMap tmAl,
                       const __grid_constant__ CUtensorMap tmBl, SgemmArgs g) {
-  constexpr int TSTAGES = TcCfg<SPLIT>::STAGES;
-  constexpr int T_STAGE_BYTES = TcCfg<SPLIT>::STAGE_BYTES;
+  constexpr bool SPLIT = TcCfg<MODE>::SPLIT;
+  constexpr int TBK = TcCfg<MODE>::TBK;
+  constexpr int TSTAGES = TcCfg<MODE>::STAGES;
+  constexpr int T_STAGE_BYTES = TcCfg<MODE>::STAGE_BYTES;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* smem =
       reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -218,9 +242,13 @@ __global__ void __launch_bounds__(T_THREADS, 1)
           const uint32_t a0 = smem_u32(sA + s * T_STAGE_BYTES);
           const uint32_t b0 = a0 + T_A_BYTES;
 #pragma unroll
-          for (int kk = 0; kk < TBK / 8; ++kk) {
-            tc_mma_tf32(dt, sw128_kmajor_desc(a0 + kk * 32), sw128_kmajor_desc(b0 + kk * 32), kIdescTF32,
-                        (kb > 0 || kk > 0) ? 1u : 0u);
+          for (int kk = 0; kk < 4; ++kk) {  // four MMAs of 32 bytes of K per slice
+            if (MODE == kBf16)
+              tc_mma_f16(dt, sw128_kmajor_desc(a0 + kk * 32), sw128_kmajor_desc(b0 + kk * 32), kIdescBF16,
+                         (kb > 0 || kk > 0) ? 1u : 0u);
+            else
+              tc_mma_tf32(dt, sw128_kmajor_desc(a0 + kk * 32), sw128_kmajor_desc(b0 + kk * 32), kIdescTF32,
+                          (kb > 0 || kk > 0) ? 1u : 0u);
             if (SPLIT) {
               const uint32_t al = b0 + T_B_BYTES, bl = al + T_A_BYTES;
               tc_mma_tf32(dt, sw128_kmajor_desc(a0 + kk * 32), sw128_kmajor_desc(bl + kk * 32), kIdescTF32, 1u);
@@ -295,36 +323,33 @@ __global__ void __launch_bounds__(T_THREADS, 1)
 
 void count_launch(int n);
 
-int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
-               long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
-               const float* Btlo, int max_ctas, const int* gate) {
-  if (m <= 0 || n <= 0) return LM_OK;
-  if (k <= 0) return LM_ERR_ARG;
-  const bool split = Alo != nullptr && Btlo != nullptr;
+namespace {
+
+template <int MODE>
+int sgemm_launch(Ctx& ctx, int m, int n, int k, float alpha, const void* A, long long lda, const void* Bt,
+                 long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const void* Alo,
+                 const void* Btlo, int max_ctas, const int* gate) {
+  constexpr int TBK = TcCfg<MODE>::TBK;
+  constexpr int ES = MODE == kBf16 ? 2 : 4;  // operand element bytes
+  const CUtensorMapDataType dt = MODE == kBf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
   if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(Bt) | reinterpret_cast<uintptr_t>(C) |
        reinterpret_cast<uintptr_t>(Alo) | reinterpret_cast<uintptr_t>(Btlo)) & 15)
     return LM_ERR_UNSUPPORTED;
-  if ((lda | ldb | ldc) & 3) return LM_ERR_UNSUPPORTED;  // 16-byte row strides for TMA
-  static bool attr_set[2][kMaxDevices] = {};
+  if (((lda * ES) | (ldb * ES) | (ldc * 4)) & 15) return LM_ERR_UNSUPPORTED;  // 16-byte row strides for TMA
+  static bool attr_set[kMaxDevices] = {};
   const int dev = ctx_device(ctx);
-  if (!attr_set[split][dev]) {
-    if (split)
-      LM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tf32_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       TcCfg<true>::SMEM));
-    else
-      LM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tf32_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       TcCfg<false>::SMEM));
-    attr_set[split][dev] = true;
+  if (!attr_set[dev]) {
+    LM_CUDA_TRY(cudaFuncSetAttribute(sgemm_tf32_kernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     TcCfg<MODE>::SMEM));
+    attr_set[dev] = true;
   }
   CUtensorMap tA, tB, tC, tAl, tBl;
-  LM_TRY(make_tmap_2d(&tA, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, A, k, m, lda, TBK, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
-  LM_TRY(make_tmap_2d(&tB, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Bt, k, n, ldb, TBK, TBN, CU_TENSOR_MAP_SWIZZLE_128B));
+  LM_TRY(make_tmap_2d(&tA, dt, ES, A, k, m, lda, TBK, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
+  LM_TRY(make_tmap_2d(&tB, dt, ES, Bt, k, n, ldb, TBK, TBN, CU_TENSOR_MAP_SWIZZLE_128B));
   LM_TRY(make_tmap_2d(&tC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, C, n, m, ldc, 32, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
-  if (split) {
-    LM_TRY(make_tmap_2d(&tAl, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Alo, k, m, lda, TBK, TBM,
-                        CU_TENSOR_MAP_SWIZZLE_128B));
-    LM_TRY(make_tmap_2d(&tBl, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, Btlo, k, n, ldb, TBK, TBN,
-                        CU_TENSOR_MAP_SWIZZLE_128B));
+  if (TcCfg<MODE>::SPLIT) {
+    LM_TRY(make_tmap_2d(&tAl, dt, ES, Alo, k, m, lda, TBK, TBM, CU_TENSOR_MAP_SWIZZLE_128B));
+    LM_TRY(make_tmap_2d(&tBl, dt, ES, Btlo, k, n, ldb, TBK, TBN, CU_TENSOR_MAP_SWIZZLE_128B));
   } else {
     tAl = tA;
     tBl = tB;
@@ -340,7 +365,7 @@ int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long 
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid, 1, 1);
   cfg.blockDim = dim3(T_THREADS, 1, 1);
-  cfg.dynamicSmemBytes = split ? TcCfg<true>::SMEM : TcCfg<false>::SMEM;
+  cfg.dynamicSmemBytes = TcCfg<MODE>::SMEM;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeClusterDimension;  // explicit 1-CTA clusters for the shared::cluster forms
@@ -350,15 +375,34 @@ int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long 
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   {
-    Prof prof(ctx, kPhaseGemm, 2.0 * m * n * k * (split ? 3 : 1),
-              4.0 * ((double)m * k + (double)n * k) * (split ? 2 : 1) + 8.0 * m * n, st);
-    if (split)
-      LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, sgemm_tf32_kernel<true>, tA, tB, tC, tAl, tBl, g));
-    else
-      LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, sgemm_tf32_kernel<false>, tA, tB, tC, tAl, tBl, g));
+    const int products = TcCfg<MODE>::SPLIT ? 3 : 1;
+    Prof prof(ctx, kPhaseGemm, 2.0 * m * n * k * products,
+              (double)ES * ((double)m * k + (double)n * k) * (TcCfg<MODE>::SPLIT ? 2 : 1) + 8.0 * m * n, st);
+    LM_CUDA_TRY(cudaLaunchKernelEx(&cfg, sgemm_tf32_kernel<MODE>, tA, tB, tC, tAl, tBl, g));
   }
   count_launch(1);
   return LM_OK;
+}
+
+}  // namespace
+
+int sgemm_tf32(Ctx& ctx, int m, int n, int k, float alpha, const float* A, long long lda, const float* Bt,
+               long long ldb, float beta, float* C, long long ldc, cudaStream_t st, const float* Alo,
+               const float* Btlo, int max_ctas, const int* gate) {
+  if (m <= 0 || n <= 0) return LM_OK;
+  if (k <= 0) return LM_ERR_ARG;
+  if (Alo != nullptr && Btlo != nullptr)
+    return sgemm_launch<kTf32x3>(ctx, m, n, k, alpha, A, lda, Bt, ldb, beta, C, ldc, st, Alo, Btlo, max_ctas, gate);
+  return sgemm_launch<kTf32>(ctx, m, n, k, alpha, A, lda, Bt, ldb, beta, C, ldc, st, nullptr, nullptr, max_ctas,
+                             gate);
+}
+
+int sgemm_bf16(Ctx& ctx, int m, int n, int k, float alpha, const void* A, long long lda, const void* Bt,
+               long long ldb, float beta, float* C, long long ldc, cudaStream_t st, int max_ctas) {
+  if (m <= 0 || n <= 0) return LM_OK;
+  if (k <= 0) return LM_ERR_ARG;
+  return sgemm_launch<kBf16>(ctx, m, n, k, alpha, A, lda, Bt, ldb, beta, C, ldc, st, nullptr, nullptr, max_ctas,
+                             nullptr);
 }
 
 }  // namespace lm

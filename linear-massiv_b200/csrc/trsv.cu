@@ -159,14 +159,15 @@ __device__ __forceinline__ void load_row_share(T* out, const T* src, int c0, int
 // corr (inverse form only): per-block flags at stride 2; when given, the
 // correction step on the diagonal block runs only for blocks whose flag is
 // set.  The 16-column variant never takes the correction step.
-template <typename T, int RHS, bool EXACT>
+template <typename T, int RHS, bool EXACT, bool FWD>
 __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restrict__ LU, long long lda, int n,
-                                                             int nrhs, int forward, const T* __restrict__ Dinv,
+                                                             int nrhs, const T* __restrict__ Dinv,
                                                              T* X, long long ldx, int* sync, int* status,
                                                              int vec_ok, const int* corr, int unit_l) {
   constexpr int MAX_RHS = RHS;
   constexpr int BS = TrsvCfg<T>::BS, NT = TrsvCfg<T>::NT, VEC = TrsvCfg<T>::VEC, CP = BS / 4;
   constexpr int RPL = BS / 32;  // rows per lane of the one-warp substitution
+  constexpr bool forward = FWD;  // the direction is a compile-time constant
   static_assert(NT == 4 * BS, "four threads per row");
   __shared__ int tk_sh, prog_sh;
   // rows padded by one element: the four threads of a row read columns 4 q
@@ -224,12 +225,17 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
     load_row_share<T>(tv, LU + (long long)(r0 + r) * lda, j * BS, q, n, row_ok, vec_ok != 0);
     if (d >= known) {
       if (threadIdx.x == 0) {
+        // every waiting block polls the one progress word: a short sleep
+        // between polls keeps them from saturating its L2 slice, which the
+        // producing block's stores and instruction fetches also go through
         int p = ld_acquire(sync);
-        for (uint32_t it = 0; ok && p <= d; p = ld_acquire(sync))
+        for (uint32_t it = 0; ok && p <= d; p = ld_acquire(sync)) {
           if (++it > kSpinLimit) {
             atomicCAS(status, 0, LM_DEVERR_TIMEOUT);
             ok = false;
           }
+          __nanosleep(p + 1 < d ? 512 : 64);
+        }
         prog_sh = ok ? p : nb;  // on timeout, run to the end without waiting
       }
       __syncthreads();
@@ -264,70 +270,76 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
   __syncthreads();
   if constexpr (EXACT) {
     // warp 0: blocked column sweep in 32 dependent steps of RPL rows.  Step s:
-    // lane s solves its RPL x RPL diagonal tile exactly (sequentially, in
-    // registers), the RPL values go to every lane by shuffles, and the lanes
-    // on the unsolved side subtract tile (l, s) times them from their rows.
+    // every lane takes lane s's RPL partial results by shuffles and solves the
+    // RPL x RPL diagonal tile with them itself (the same values in every lane,
+    // so no lane branches off), then the lanes on the unsolved side subtract
+    // tile (l, s) times the solution from their rows.  Tile rows are 16-byte
+    // shared-memory loads.
     if (threadIdx.x < 32) {
       constexpr int TS = TrsvDiag<T>::TS;
+      static_assert(RPL * sizeof(T) == 16, "a tile row is one 16-byte load");
       const int l = threadIdx.x;
       T y[RPL][MAX_RHS];
 #pragma unroll
       for (int i = 0; i < RPL; ++i)
 #pragma unroll
         for (int h = 0; h < MAX_RHS; ++h) y[i][h] = ys[RPL * l + i][h];
-      T rd[RPL];
+      const uint32_t tile_base = smem_u32(diag.tile);
+      auto load_tile = [&](int row_lane, int col_lane, T (&t)[RPL][RPL]) {
+        const uint32_t a = tile_base + (uint32_t)((col_lane * 32 + row_lane) * TS * (int)sizeof(T));
 #pragma unroll
-      for (int i = 0; i < RPL; ++i) rd[i] = (forward && unit_l) ? T(1) : diag.rdiag[RPL * l + i];
-      // (nrhs is uniform across the warp, so the guarded shuffles are too)
+        for (int i = 0; i < RPL; ++i) {
+          if constexpr (sizeof(T) == 4) {
+            float4 v;
+            asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+                         : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                         : "r"(a + 16u * i));
+            t[i][0] = v.x, t[i][1] = v.y, t[i][2] = v.z, t[i][3] = v.w;
+          } else {
+            double2 v;
+            asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(a + 16u * i));
+            t[i][0] = v.x, t[i][1] = v.y;
+          }
+        }
+      };
 #pragma unroll 1
       for (int st = 0; st < 32; ++st) {
         const int sl = forward ? st : 31 - st;  // lane whose rows are solved now
-        // tile (l, sl): this lane's rows, the solved lane's columns
-        T tl[RPL][RPL];
-        const T* tp = diag.tile + (sl * 32 + l) * TS;
+        T tl[RPL][RPL], td[RPL][RPL], rdv[RPL];
+        load_tile(l, sl, tl);   // this lane's rows, the solved lane's columns
+        load_tile(sl, sl, td);  // the diagonal tile (the same address in every lane)
 #pragma unroll
-        for (int i = 0; i < RPL; ++i)
-#pragma unroll
-          for (int j = 0; j < RPL; ++j) tl[i][j] = tp[i * RPL + j];
-        if (l == sl) {
-          // the diagonal tile, solved in place: forward lower (unit, or
-          // scaled by the reciprocal diagonal), backward upper
-          if (forward) {
-#pragma unroll
-            for (int i = 0; i < RPL; ++i)
-#pragma unroll
-              for (int h = 0; h < MAX_RHS; ++h) {
-                T v = y[i][h];
-#pragma unroll
-                for (int j = 0; j < i; ++j) v = fma(-tl[i][j], y[j][h], v);
-                y[i][h] = unit_l ? v : v * rd[i];
-              }
-          } else {
-#pragma unroll
-            for (int i = RPL - 1; i >= 0; --i)
-#pragma unroll
-              for (int h = 0; h < MAX_RHS; ++h) {
-                T v = y[i][h];
-#pragma unroll
-                for (int j = i + 1; j < RPL; ++j) v = fma(-tl[i][j], y[j][h], v);
-                y[i][h] = v * rd[i];
-              }
-          }
-        }
+        for (int i = 0; i < RPL; ++i) rdv[i] = (forward && unit_l) ? T(1) : diag.rdiag[RPL * sl + i];
 #pragma unroll
         for (int h = 0; h < MAX_RHS; ++h)
           if (h < nrhs) {
             T xv[RPL];
 #pragma unroll
             for (int j = 0; j < RPL; ++j) xv[j] = __shfl_sync(0xffffffffu, y[j][h], sl);
-            if (forward ? l > sl : l < sl) {
+            if (forward) {
 #pragma unroll
               for (int i = 0; i < RPL; ++i) {
-                T v = y[i][h];
+                T v = xv[i];
 #pragma unroll
-                for (int j = 0; j < RPL; ++j) v = fma(-tl[i][j], xv[j], v);
-                y[i][h] = v;
+                for (int j = 0; j < i; ++j) v = fma(-td[i][j], xv[j], v);
+                xv[i] = unit_l ? v : v * rdv[i];
               }
+            } else {
+#pragma unroll
+              for (int i = RPL - 1; i >= 0; --i) {
+                T v = xv[i];
+#pragma unroll
+                for (int j = i + 1; j < RPL; ++j) v = fma(-td[i][j], xv[j], v);
+                xv[i] = v * rdv[i];
+              }
+            }
+            const bool below = forward ? l > sl : l < sl;
+#pragma unroll
+            for (int i = 0; i < RPL; ++i) {
+              T v = y[i][h];
+#pragma unroll
+              for (int j = 0; j < RPL; ++j) v = fma(-tl[i][j], xv[j], v);
+              y[i][h] = l == sl ? xv[i] : (below ? v : y[i][h]);
             }
           }
       }
@@ -467,15 +479,18 @@ int trsv_pass(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const
     int dev = 0;
     LM_CUDA_TRY(cudaGetDevice(&dev));
     if (!attr_set[dev]) {
-      LM_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<T, RHS, EXACT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      LM_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<T, RHS, EXACT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem));
+      LM_CUDA_TRY(cudaFuncSetAttribute(trsv_kernel<T, RHS, EXACT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem));
       attr_set[dev] = true;
     }
   }
   LM_CUDA_TRY(cudaMemsetAsync(sync, 0, sizeof(int) * 4, st));
-  trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 1, DinvL, X, ldx, sync, status, vec_ok, corr,
-                                                   unit_l);
-  trsv_kernel<T, RHS, EXACT><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, 0, DinvU, X, ldx, sync + 2, status, vec_ok,
-                                                   corr ? corr + 1 : nullptr, unit_l);
+  trsv_kernel<T, RHS, EXACT, true><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, DinvL, X, ldx, sync, status, vec_ok, corr,
+                                                         unit_l);
+  trsv_kernel<T, RHS, EXACT, false><<<nb, NT, smem, st>>>(LU, lda, n, nrhs, DinvU, X, ldx, sync + 2, status, vec_ok,
+                                                          corr ? corr + 1 : nullptr, unit_l);
   count_launch(2);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;
@@ -492,6 +507,8 @@ int trsv_lu(const T* LU, long long lda, int n, int nrhs, const T* DinvL, const T
   if (!exact && (reinterpret_cast<uintptr_t>(DinvL) % 16 || reinterpret_cast<uintptr_t>(DinvU) % 16))
     return LM_ERR_ARG;
   const int vec_ok = (reinterpret_cast<uintptr_t>(LU) % 16 == 0) && (lda % VEC == 0);
+  if (nrhs == 1 && exact)  // the refinement's common case: one column, fewer registers
+    return trsv_pass<T, 1, true>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, nullptr, vec_ok, ul);
   if (nrhs <= MAX_RHS) {
     if (exact)
       return trsv_pass<T, MAX_RHS, true>(LU, lda, n, nrhs, DinvL, DinvU, X, ldx, sync, status, st, nullptr, vec_ok, ul);

@@ -44,11 +44,14 @@ EXPORTS = [
     "lm_server_default_config", "lm_server_create", "lm_server_submit", "lm_server_test", "lm_server_wait",
     "lm_server_cancel", "lm_server_drain", "lm_server_stats", "lm_server_reset_stats", "lm_server_destroy",
     "lm_dgemv", "lm_matvec_host", "lm_dnorm_inf", "lm_norm_inf_host", "lm_dgetrf_nopiv", "lm_lu_nopivot_host",
-    "lm_cholesky_gaxpy_host", "lm_dtridiag_solve", "lm_tridiag_solve_host",
+    "lm_cholesky_gaxpy_host", "lm_dtridiag_solve", "lm_tridiag_solve_host", "lm_dgesv_ir_prec",
 ]
 
 IR_RBT = 0
 IR_GEPP = 1
+IR_PREC_TF32X3 = 0
+IR_PREC_TF32 = 1
+IR_PREC_BF16 = 2
 BATCH_GENERAL = 0
 BATCH_SPD = 1
 PREC_FP64 = 0
@@ -151,6 +154,7 @@ def _lib():
                 "lm_cholesky_gaxpy_host": ([vp, i, dp, dp, ip], i),
                 "lm_dtridiag_solve": ([vp, i, vp, vp, vp, vp], i),
                 "lm_tridiag_solve_host": ([vp, i, dp, dp, dp, dp], i),
+                "lm_dgesv_ir_prec": ([vp, i, i, vp, i, vp, i, vp, i, i, d, i, ip, dp, ip], i),
             }
             for name, (args, res) in sigs.items():
                 fn = getattr(L, name)
@@ -481,6 +485,25 @@ def luSolveIR(A, b, tol: float = 0.0, max_iter: int = 30, ctx: Context | None = 
 
 # ---- host-buffer entry points (what a pure FFI binding calls) -----------------
 
+def luSolveIRPrec(A, b, prec: int = IR_PREC_TF32X3, tol: float = 0.0, max_iter: int = 30,
+                  ctx: Context | None = None):
+    """Mixed-precision luSolve with the factor precision prec (IR_PREC_*):
+    (x, outer steps, backward error, status)."""
+    import torch
+
+    ctx = ctx or default_context(A.device.index or 0)
+    B, vec = _as_cols(b)
+    B = B.contiguous()
+    X = torch.empty_like(B)
+    it, be, info = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_int(0)
+    st = _lib().lm_dgesv_ir_prec(ctx.h, A.shape[0], B.shape[1], _ptr(A), A.stride(0), _ptr(B), B.stride(0), _ptr(X),
+                                 X.stride(0), int(prec), float(tol), int(max_iter), ctypes.byref(it), ctypes.byref(be),
+                                 ctypes.byref(info))
+    if st < 0 and st != LM_ERR_NOT_CONVERGED:
+        _check(st, "lm_dgesv_ir_prec")
+    return (X[:, 0] if vec else X), it.value, be.value, st
+
+
 def _np_ptr(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
@@ -657,7 +680,8 @@ class ServerConfig(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_size_t), ("large_workers", ctypes.c_int), ("batch_lanes", ctypes.c_int),
                 ("small_max_n", ctypes.c_int), ("small_precision", ctypes.c_int), ("large_precision", ctypes.c_int),
                 ("max_batch", ctypes.c_int), ("max_n", ctypes.c_int), ("max_nrhs", ctypes.c_int),
-                ("nb", ctypes.c_int * 4)]
+                ("nb", ctypes.c_int * 4), ("ir_method", ctypes.c_int), ("device_loop", ctypes.c_int),
+                ("loop_ctas", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):

@@ -87,6 +87,40 @@ def test_mix_matches_alone_and_fp64_accuracy(server):
     assert st["micro_batches"] >= 1 and st["small_solved"] >= 1
 
 
+def test_device_loop_matches_micro_batches():
+    """Small requests on the device-resident loop (the default) give the same
+    bits as the micro-batch lanes of the batch kernel, and the loop returns to
+    the host when idle and is relaunched by the next request."""
+    g = philox(97)
+    reqs = []
+    for _ in range(40):
+        n = int(g.integers(8, 257))
+        r = int(g.integers(1, 17))
+        spd = g.uniform() < 0.5
+        M = g.uniform(-1, 1, (n, n))
+        M = M @ M.T + n * np.eye(n) if spd else M
+        reqs.append((M, g.uniform(-1, 1, (n, r)), lmb200.BATCH_SPD if spd else lmb200.BATCH_GENERAL))
+    outs = {}
+    for loop in (1, 0):
+        s = lmb200.Server(0, max_n=256, max_nrhs=16, large_workers=1, batch_lanes=2, device_loop=loop)
+        try:
+            ids = [s.submit(A, B, k) for A, B, k in reqs[:20]]
+            time.sleep(0.05)  # long enough for an idle loop to return
+            ids += [s.submit(A, B, k) for A, B, k in reqs[20:]]
+            res = []
+            for (rid, X), (A, B, k) in zip(ids, reqs):
+                assert s.wait(rid, 60.0)[0] == 0
+                assert berr(A, X, B) <= TOL * A.shape[0]
+                res.append(X.copy())
+            outs[loop] = res
+            st = s.stats()
+            assert st["small_solved"] == 40 and st["micro_batches"] >= (2 if loop else 1)
+        finally:
+            s.close()
+    for a, b in zip(outs[1], outs[0]):
+        assert np.array_equal(a, b)
+
+
 def test_small_requests_overtake_a_large_one(server):
     g = philox(92)
     A = sigma_matrix(g, 1024, 1e3, False)
