@@ -73,6 +73,8 @@ def parse():
     p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
     p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
     p.add_argument("--kappa", type=float, default=1e6, help="ir: condition number of A (0 = uniform A)")
+    p.add_argument("--ir-method", choices=["gepp", "rbt"], default="gepp",
+                   help="ir: partial pivoting (default) or random butterflies without pivoting")
     p.add_argument("--prec", choices=["tf32x3", "tf32", "bf16"], default="tf32x3",
                    help="ir: precision of the factor's trailing updates (tf32 and bf16 are refined by GMRES-IR)")
     p.add_argument("--reflectors", type=int, default=0,
@@ -82,6 +84,9 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--cpu-full", action="store_true",
+                   help="cpu_baseline: one oracle solve at the full n on every host thread instead of the "
+                        "single-threaded n <= 2048 sample (minutes at n = 16384)")
     p.add_argument("--no-peak", action="store_true", help="skip the cuBLAS DGEMM peak measurement")
     p.add_argument("--k", type=int, default=0, help="gemm inner dimension (default n); k < n adds beta = 1")
     p.add_argument("--profile-steps", type=int, default=1,
@@ -110,7 +115,9 @@ def workload_name(a):
         upd = {"tf32x3": "3xTF32 tcgen05 updates, FP64 refinement",
                "tf32": "1xTF32 tcgen05 trailing updates, FP64 GMRES-IR",
                "bf16": "BF16 tcgen05 trailing updates, FP64 GMRES-IR"}[a.prec]
-        return f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, FP32 LU with partial pivoting + {upd}"
+        fac = ("FP32 LU with partial pivoting" if a.ir_method == "gepp" else
+               "random butterflies + FP32 LU without pivoting (partial pivoting if refinement stalls)")
+        return f"mixed-precision IR luSolve n={a.n} nrhs={a.nrhs}, {spec}, {fac} + {upd}"
     if a.workload == "lu":
         return f"luSolve FP64 n={a.n} nrhs={a.nrhs}, A uniform[-1,1]"
     if a.workload == "chol":
@@ -605,12 +612,25 @@ def cpu_baseline(a):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    ns = min(a.n, 2048)
+    full = a.cpu_full and a.workload in ("lu", "ir", "chol")
+    ns = a.n if full else min(a.n, 2048)
+    threads = (os.cpu_count() or 1) if full else 1
+    O.set_threads(threads)
     g = np.random.Generator(np.random.Philox(a.seed + 1))
     A = g.uniform(-1.0, 1.0, (ns, ns))
     b = g.uniform(-1.0, 1.0, ns)
     if a.workload == "chol":
         A = A @ A.T + ns * np.eye(ns)
+    if full:
+        # one solve of the full order; the oracle's trailing updates split
+        # their rows over the threads (bitwise the same result as one thread)
+        t0 = time.perf_counter()
+        {"lu": O.lu_solve_p, "ir": O.lu_solve_p, "chol": O.chol_solve_p}[a.workload](A, b)
+        dt = time.perf_counter() - t0
+        O.set_threads(1)
+        return {"value": 1.0 / dt, "unit": metric_name(a), "cores": threads, "kind": "port",
+                "sample": f"one oracle solve at the full n={ns} ({dt:.2f} s) with its trailing updates split over "
+                          f"{threads} host threads"}
     fn = {"lu": lambda: O.lu_solve_p(A, b), "ir": lambda: O.lu_solve_p(A, b), "chol": lambda: O.chol_solve_p(A, b),
           "gemm": lambda: O.matmul_p(A, A)}[a.workload]
     fn()
@@ -639,7 +659,7 @@ def run_reference(a, world, rank):
     import oracle as O
 
     threads = os.cpu_count() or 1
-    ns = min(a.n, 1024)
+    ns = min(a.n, 2048)
     g = np.random.Generator(np.random.Philox(a.seed + 1))
     A = g.uniform(-1.0, 1.0, (ns, ns))
     b = g.uniform(-1.0, 1.0, ns)
@@ -668,7 +688,9 @@ def run_reference(a, world, rank):
     line = {"impl": "reference", "metric": metric_name(a), "value": value, "unit": metric_name(a),
             "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 * dt / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded numpy Philox)", "config": {"workload": workload_name(a), "sample_n": ns},
+            "data": "synthetic (seeded numpy Philox, uniform[-1,1])",
+            "config": {"workload": workload_name(a), "n": a.n, "nrhs": a.nrhs, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (8 n^2 bytes per matrix)"},
             "cpu_baseline": {"value": value, "unit": metric_name(a), "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": value, "unit": metric_name(a), "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -711,6 +733,8 @@ def run_ours(a, world, rank, local):
 
     torch.cuda.set_device(local)
     ctx = lmb200.Context(local)
+    if a.workload == "ir":
+        ctx.set_ir_method(lmb200.IR_RBT if a.ir_method == "rbt" else lmb200.IR_GEPP)
     lib = lmb200.lib()
     n, nrhs = a.n, a.nrhs
     A_h, B_h = make_inputs(a, rank, torch, np)

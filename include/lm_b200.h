@@ -299,7 +299,7 @@ int lm_batch_tune_set(lm_ctx* ctx, const int* nb /* [2][4] */);
  * mixed-precision solve of lm_dgesv_ir (FP32 factor + FP64 refinement, for
  * general and SPD matrices alike, method ir_method) at a padded order (n
  * rounded up to a multiple of 64, 128 or 256, the system embedded with a
- * small identity block and zero right-hand-side rows, so that requests of
+ * diagonal block max_i |a_ii| I and zero right-hand-side rows, so that requests of
  * nearby orders replay the same captured CUDA graphs; the stopping test is
  * that of the original order), then FP64 LU (general) or FP64 Cholesky
  * (SPD) when refinement does not converge; with LM_PREC_FP64 FP64 LU or
@@ -319,8 +319,10 @@ typedef struct {
   int max_nrhs;         /* most right-hand sides (default 64, <= 64) */
   int nb[4];            /* batch-kernel panel width per size bucket (default 16) */
   int ir_method;        /* factorisation of the large mixed-precision solves: LM_IR_GEPP
-                           (default) or LM_IR_RBT (solved at the request's own order: the
-                           random butterflies would mix the padding into the system) */
+                           (default: FP32 partial pivoting, the same result for a request
+                           alone and in any mix) or LM_IR_RBT (the randomised factor
+                           without pivoting, redone with partial pivoting whenever its
+                           refinement stalls) */
   int device_loop;      /* 1 (default): small requests run on the device-resident loop, a
                            persistent kernel of loop_ctas CTAs that claims each posted
                            request from a ring in device memory as soon as its data has

@@ -412,6 +412,15 @@ int convert_d2s(float* dst, long long ldd, const double* src, long long lds, int
 
 namespace {
 
+// Normwise backward error of one column from its norms: a NaN in the
+// residual or in the solution (whose max-abs reductions return NaN) is never
+// converged, and a zero denominator counts only an exact zero residual.
+inline double backward_error(double rn, double xn, double den) {
+  if (rn != rn || xn != xn || den != den) return 1e300;
+  if (den > 0) return rn / den;
+  return rn > 0 ? 1e300 : 0.0;
+}
+
 // Refinement loop shared by both low-precision factorisations.  R (n x ldr
 // FP64), D (np x ldr FP32, np >= n) and nrm (2 + 3 * 64 words, nrm[0] and
 // nrm[1..] already hold ||A||_inf and ||B_c||_inf) are device scratch.
@@ -461,7 +470,7 @@ int refine(Ctx& c, int n, int np, int nrhs, const double* A, long long lda, cons
     for (int col = 0; col < nrhs; ++col) {
       const double rn = dbl(h[1 + 64 + col]), xn = dbl(h[1 + 128 + col]), bn = dbl(h[1 + col]);
       const double den = anorm * xn + bn;
-      const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
+      const double be = backward_error(rn, xn, den);
       worst = std::max(worst, (be != be) ? 1e300 : be);
     }
     ctx_ir_history(c).push_back(worst);
@@ -691,7 +700,7 @@ int refine_gmres(Ctx& c, int n, int nrhs, const double* A, long long lda, const 
     for (int col = 0; col < nrhs; ++col) {
       const double rn = dbl(h[1 + 64 + col]), xn = dbl(h[1 + 128 + col]), bn = dbl(h[1 + col]);
       const double den = anorm * xn + bn;
-      const double be = den > 0 ? rn / den : (rn > 0 ? 1.0 : 0.0);
+      const double be = backward_error(rn, xn, den);
       worst = std::max(worst, (be != be) ? 1e300 : be);
     }
     ctx_ir_history(c).push_back(worst);

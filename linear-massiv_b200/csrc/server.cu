@@ -67,17 +67,34 @@ int padded_order(int n) {
 
 // Diagonal of the padding: the system is embedded as [[A, 0], [0, c I]] with
 // B padded by zero rows, so the padded unknowns are exactly zero and the first
-// n rows of the solution are A's.  A small power of two keeps ||A_p||_inf =
-// ||A||_inf (the refinement's stopping test) for any A of norm >= c, and the
-// partial-pivoting search never prefers a padding row over a nonzero in A.
-constexpr double kPadDiag = 1.0 / (1 << 30);
+// n rows of the solution are A's.  c = max_i |a_ii| (1 if that is 0): never
+// above ||A||_inf, so ||A_p||_inf = ||A||_inf and the refinement's stopping
+// test is the original one, and on A's own scale, so the padded system is no
+// worse conditioned than A even when the randomised method mixes the padding
+// rows into it.
+__global__ void pad_diag_kernel(const double* A, int n, double* c) {
+  double m = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, fabs(A[(long long)i * n + i]));
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) *c = (m > 0.0 && m == m) ? m : 1.0;
+  }
+}
 
-__global__ void embed_kernel(double* Ap, int np, const double* A, int n, double c) {
+__global__ void embed_kernel(double* Ap, int np, const double* A, int n, const double* c) {
   const long long total = (long long)np * np;
+  const double cd = *c;
   for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
        e += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(e / np), j = (int)(e % np);
-    Ap[e] = (i < n && j < n) ? A[(long long)i * n + j] : (i == j ? c : 0.0);
+    Ap[e] = (i < n && j < n) ? A[(long long)i * n + j] : (i == j ? cd : 0.0);
   }
 }
 
@@ -187,6 +204,7 @@ struct Worker {
   // max_nrhs): a request of an order this worker has seen before replays the
   // solve's captured CUDA graphs instead of launching every kernel again
   double *Aw = nullptr, *Bw = nullptr, *Xw = nullptr;
+  double* cpad = nullptr;  // diagonal of the padding block (device)
 };
 
 // Device-resident request loop for the small requests: the feeder thread
@@ -454,13 +472,12 @@ int worker_solve(lm_server* s, Worker* w, Req* r) {
   if (s->cfg.large_precision == LM_PREC_FP32_IR) {
     int it = 0;
     double be = 0;
-    // solved at the bucket order in the worker's fixed buffers (graph replay);
-    // the randomised method mixes every row and column, so it would mix the
-    // padding in too: it solves at the request's own order
-    const int np = s->cfg.ir_method == LM_IR_GEPP ? padded_order(r->n) : r->n;
+    // solved at the bucket order in the worker's fixed buffers (graph replay)
+    const int np = padded_order(r->n);
     const long long tot = (long long)np * np;
-    embed_kernel<<<(int)std::min<long long>((tot + 255) / 256, 4096), 256, 0, st>>>(w->Aw, np, dA, r->n, kPadDiag);
-    lm::count_launch(1);
+    pad_diag_kernel<<<1, 256, 0, st>>>(dA, r->n, w->cpad);
+    embed_kernel<<<(int)std::min<long long>((tot + 255) / 256, 4096), 256, 0, st>>>(w->Aw, np, dA, r->n, w->cpad);
+    lm::count_launch(2);
     LM_CUDA_TRY(cudaGetLastError());
     LM_CUDA_TRY(cudaMemcpyAsync(w->Bw, dB, nr, cudaMemcpyDeviceToDevice, st));
     if (np > r->n)
@@ -734,6 +751,7 @@ void server_free(lm_server* s) {
     cudaFree(w->Aw);
     cudaFree(w->Bw);
     cudaFree(w->Xw);
+    cudaFree(w->cpad);
     delete w;
   }
   cudaFree(s->arena.base);
@@ -798,6 +816,7 @@ int server_init(lm_server* s) {
     LM_CUDA_TRY(cudaMalloc(&w->Aw, sizeof(double) * nn));
     LM_CUDA_TRY(cudaMalloc(&w->Bw, sizeof(double) * nr));
     LM_CUDA_TRY(cudaMalloc(&w->Xw, sizeof(double) * nr));
+    LM_CUDA_TRY(cudaMalloc(&w->cpad, 256));
     LM_TRY(prewarm(s, w));
   }
   size_t free_after = 0;

@@ -192,3 +192,25 @@ def test_ir_gepp_bitwise_repeatable(ctx):
     xs = [lmb200.luSolveIR(A, b, ctx=ctx)[0].cpu().numpy() for _ in range(3)]
     assert ctx.ir_last_method() == lmb200.IR_GEPP
     assert np.array_equal(xs[0], xs[1]) and np.array_equal(xs[1], xs[2])
+
+
+@pytest.mark.parametrize("where", ["matrix", "rhs"])
+def test_ir_never_reports_nan_as_converged(ctx, ir_method, where):
+    """A NaN in the data makes every iterate NaN; the stopping test must see
+    that as not converged (the max-abs reductions return NaN, and a NaN
+    denominator once read as a zero backward error)."""
+    g = philox(9700)
+    n = 300
+    A = gen_randsvd(g, n, 1e2, -1.0, 1.0)
+    b = g.uniform(-1, 1, n)
+    if where == "matrix":
+        A[17, 5] = np.nan
+    else:
+        b[3] = np.nan
+    x, iters, berr, st = lmb200.luSolveIR(dev(A), dev(b), ctx=ctx, max_iter=5)
+    assert st != 0
+    assert not (berr <= 1e-15 * n)
+    for prec in (lmb200.IR_PREC_TF32, lmb200.IR_PREC_BF16):
+        x, iters, berr, st = lmb200.luSolveIRPrec(dev(A), dev(b), prec=prec, ctx=ctx, max_iter=2)
+        assert st != 0
+    ctx.check()
