@@ -295,15 +295,17 @@ int lm_batch_tune_set(lm_ctx* ctx, const int* nb /* [2][4] */);
  * batch kernel (batch_lanes streams, each micro-batch taking every small
  * request queued when its lane frees up), larger ones each take
  * one of `large_workers` contexts (own stream; workspaces pre-grown at start-up
- * for max_n x max_nrhs): with large_precision LM_PREC_FP32_IR the
- * mixed-precision solve of lm_dgesv_ir (FP32 factor + FP64 refinement, for
- * general and SPD matrices alike, method ir_method) at a padded order (n
+ * for max_n x max_nrhs).  Every large request is solved at a padded order (n
  * rounded up to a multiple of 64, 128 or 256, the system embedded with a
- * diagonal block max_i |a_ii| I and zero right-hand-side rows, so that requests of
- * nearby orders replay the same captured CUDA graphs; the stopping test is
- * that of the original order), then FP64 LU (general) or FP64 Cholesky
- * (SPD) when refinement does not converge; with LM_PREC_FP64 FP64 LU or
- * Cholesky directly.  A, B (read) and X (written) are the
+ * diagonal block max_i |a_ii| I and zero right-hand-side rows), so that
+ * requests of nearby orders replay the same captured CUDA graphs: by FP64 LU
+ * (general, n <= lu_fp64_max_n) or FP64 Cholesky (SPD, n <= chol_fp64_max_n),
+ * and above those orders, with large_precision LM_PREC_FP32_IR, by the
+ * mixed-precision solve of lm_dgesv_ir (FP32 factor + FP64 refinement, for
+ * general and SPD matrices alike, method ir_method, stopping test of the
+ * original order), then FP64 LU or Cholesky at the original order when
+ * refinement does not converge; with LM_PREC_FP64 always FP64.  A, B (read)
+ * and X (written) are the
  * caller's host buffers (pinned for asynchronous copies) and must stay valid
  * until the request completes.  Status of a completed request: 0, LAPACK-style
  * info > 0, or < 0 on error / cancellation. */
@@ -332,6 +334,12 @@ typedef struct {
                            LM_PREC_FP64). */
   int loop_ctas;        /* CTAs of the device-resident loop (default 16, which leaves every GPC
                            room for the large solves' thread-block clusters) */
+  int lu_fp64_max_n;    /* general requests above small_max_n and up to this order are solved
+                           by FP64 LU at the bucket order instead of the mixed-precision solve
+                           (default 2048: below it both factorisations are bound by the same
+                           column chain, and FP64 needs no refinement) */
+  int chol_fp64_max_n;  /* SPD requests up to this order by FP64 Cholesky at the bucket order
+                           (default 4096) */
 } lm_server_config;
 typedef struct {
   long long completed, rejected, cancelled, failed, fp64_fallbacks;

@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(256) gemv_exact_kernel(int m, int n, const dou
   double acc = 0.0;
 #pragma unroll 8
   for (int j = l; j < n4; j += 4) acc = fma(ar[j], x[j], acc);
+  __syncwarp();
   // lane 0 of the quad gathers the four accumulators in the reference's order
   const double a1 = __shfl_down_sync(kFull, acc, 1, 4);
   const double a2 = __shfl_down_sync(kFull, acc, 2, 4);

@@ -68,6 +68,7 @@ static_assert(sizeof(Fixed) <= kFixed, "fixed scratch");
 template <typename T>
 __device__ __forceinline__ void block_argmax(T& v, int& i, Fixed* fx) {
   const int lane = tid_() & 31, warp = tid_() >> 5;
+  __syncwarp();  // a warp split by earlier branches would serialise the shuffles
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const T ov = __shfl_xor_sync(0xffffffffu, v, o);
@@ -78,6 +79,7 @@ __device__ __forceinline__ void block_argmax(T& v, int& i, Fixed* fx) {
   __syncthreads();
   T w = lane < kBT / 32 ? (T)fx->rv[lane] : T(-1);
   int wi = lane < kBT / 32 ? fx->ri[lane] : INT_MAX;
+  __syncwarp();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const T ov = __shfl_xor_sync(0xffffffffu, w, o);
@@ -93,11 +95,13 @@ __device__ __forceinline__ void block_argmax(T& v, int& i, Fixed* fx) {
 __device__ __forceinline__ double block_max(double v, Fixed* fx) {
   const int lane = tid_() & 31, warp = tid_() >> 5;
   if (v != v) v = DBL_MAX;
+  __syncwarp();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   if (lane == 0) fx->rv[warp] = v;
   __syncthreads();
   double w = lane < kBT / 32 ? fx->rv[lane] : 0.0;
+  __syncwarp();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) w = fmax(w, __shfl_xor_sync(0xffffffffu, w, o));
   __syncthreads();
@@ -373,6 +377,7 @@ __device__ void tri_solve(const TF* F, int n, int mode, TV* V, int r, TF* Tb) {
     __syncthreads();
     for (int h = warp; h < r; h += kBT / 32) {
       TV y = lane < bw ? V[(i0 + lane) * r + h] : TV(0);
+      __syncwarp();  // one converged warp for the column sweep's shuffles
       if (fwd) {
         for (int kk = 0; kk < bw; ++kk) {
           if (!unit && lane == kk) y = y / (TV)Tb[kk * LDT + kk];
@@ -496,6 +501,7 @@ __device__ int run_ir(const BatchItem& it, const BatchArgs& g, unsigned char* sm
     for (int i = warp; i < n; i += kBT / 32) {
       double s = 0.0;
       for (int k = lane; k < n; k += 32) s += fabs(A[(long long)i * n + k]);
+      __syncwarp();
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
       m = fmax(m, s);
@@ -533,6 +539,7 @@ __device__ int run_ir(const BatchItem& it, const BatchArgs& g, unsigned char* sm
         for (int h = 0; h < BatchLimits::kMaxRhs; ++h)
           if (h < r) s[h] = fma(a, Xd[k * r + h], s[h]);
       }
+      __syncwarp();
 #pragma unroll
       for (int h = 0; h < BatchLimits::kMaxRhs; ++h)
         if (h < r) {

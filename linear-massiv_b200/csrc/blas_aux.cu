@@ -356,6 +356,7 @@ __global__ void residual_kernel(int n, int nrhs, const double* __restrict__ A, l
     for (int r = 0; r < NR; ++r)
       if (r < nrhs) acc[r] = fma(a, X[(long long)j * ldx + r], acc[r]);
   }
+  __syncwarp();  // lanes leave the strided loop at different trip counts
 #pragma unroll
   for (int r = 0; r < NR; ++r)
 #pragma unroll

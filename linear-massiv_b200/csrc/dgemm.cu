@@ -216,6 +216,9 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB, CSM>::THREADS, MINB)
       const int s = it % STAGES;
       const uint32_t ph = (uint32_t)((it / STAGES) & 1);
       if (!mbar_wait(&full[s], ph, g.status)) return;
+      // lanes leave the poll independently: reconverge before the warp-wide
+      // mma.sync of this slice
+      __syncwarp();
       const uint32_t aBase = sA32 + s * Cfg::A_BYTES;
       const uint32_t bBase = sB32 + s * Cfg::B_BYTES;
 #pragma unroll
@@ -256,6 +259,7 @@ __global__ void __launch_bounds__(GemmCfg<BM, BN, MINB, CSM>::THREADS, MINB)
     const bool use_beta = g.beta != 0.0;
     if constexpr (CSM) {
       if (!mbar_wait(cfull, (uint32_t)(cj & 1), g.status)) return;
+      __syncwarp();
       const uint32_t sC32 = smem_u32(sC);
 #pragma unroll
       for (int mi = 0; mi < 4; ++mi)

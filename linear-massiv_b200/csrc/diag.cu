@@ -285,6 +285,7 @@ __device__ __noinline__ void lu32_warp(float* blk, int o, int w, int base, int* 
   for (int k = 0; k < 32; ++k) {
     const float piv = __shfl_sync(0xffffffffu, r[k], k);
     if (i == 0 && o + k < w && (piv == 0.f || piv != piv)) atomicCAS(status + 1, 0, base + o + k + 1);
+    __syncwarp();  // the rare branch above must not leave the warp split for the shuffles
     const float l = r[k] / piv;
     if (i > k) r[k] = l;
 #pragma unroll 32
@@ -386,6 +387,7 @@ __global__ void __launch_bounds__(512, 1)
     if (t < 32) {
       double m = 0.0;
       for (int j = t; j < DB; j += 32) m = fmax(m, colsum[j]);
+      __syncwarp();
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
       if (t == 0) colsum[0] = m;

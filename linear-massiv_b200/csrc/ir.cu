@@ -155,6 +155,7 @@ __global__ void sgemm_rhs_kernel(int m, int k, int nrhs, const float* __restrict
       for (int c = 0; c < 8; ++c)
         if (c0 + c < nrhs) acc[c] = fmaf(a, Y[(long long)kk * ldy + c0 + c], acc[c]);
     }
+    __syncwarp();
 #pragma unroll
     for (int c = 0; c < 8; ++c)
 #pragma unroll
@@ -183,6 +184,7 @@ __global__ void norm_inf_rows_kernel(const double* A, long long lda, int n, unsi
   if (row >= n) return;
   double s = 0.0;
   for (int j = lane; j < n; j += 32) s += fabs(A[(long long)row * lda + j]);
+  __syncwarp();
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
   if (lane == 0) atomicMax(out, (unsigned long long)__double_as_longlong(s));

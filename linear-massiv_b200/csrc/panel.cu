@@ -82,6 +82,10 @@ __device__ __forceinline__ unsigned long long msg_to_key(T m) {
 // Every lane receives the warp's best (key, row) in the pivot order: the
 // largest key, then the lowest row (rows are >= 0, or INT_MAX for none).
 __device__ __forceinline__ void warp_best(unsigned long long& key, int& row) {
+  // reconverge first: after the data-dependent branches and bounded spins of
+  // a column step a warp can arrive split, and every *_sync below would then
+  // serialise its halves
+  __syncwarp();
   const unsigned khi = (unsigned)(key >> 32), klo = (unsigned)key;
   const unsigned hi = __reduce_max_sync(0xffffffffu, khi);
   const unsigned lo = __reduce_max_sync(0xffffffffu, khi == hi ? klo : 0u);
@@ -372,6 +376,7 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
       bool fresh = lane < w && pr >= w;
       for (int jj = 0; jj < lane && jj < w; ++jj)
         if (hist[jj] == pr) fresh = false;
+      __syncwarp();
       const unsigned bal = __ballot_sync(0xffffffffu, fresh);
       if (lane < w) trow[lane] = lane;
       if (fresh) trow[w + __popc(bal & ((1u << lane) - 1u))] = pr;

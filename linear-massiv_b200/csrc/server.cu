@@ -12,11 +12,14 @@
 //     every queued small request that fits and runs them as ONE launch of the
 //     persistent batch kernel (batch.cu) on its own stream;
 //   larger requests each take a worker (own context, stream and pre-grown
-//     workspace): mixed-precision LU with FP64 refinement (lm_dgesv_ir) for
-//     general and SPD requests alike, solved at a padded bucket order so that
-//     the worker replays captured CUDA graphs for orders it has not seen, then
-//     FP64 LU (general) or FP64 Cholesky (SPD) when refinement does not
-//     converge or the FP32 factor breaks down.
+//     workspace) and are solved at a padded bucket order, so that the worker
+//     replays captured CUDA graphs for orders it has not seen: FP64 LU or
+//     Cholesky up to lu_fp64_max_n / chol_fp64_max_n (where the factorisation
+//     is bound by its column chain, the same in either precision, and FP64
+//     needs no refinement), above that mixed-precision LU with FP64
+//     refinement (lm_dgesv_ir) for general and SPD requests alike, then FP64
+//     LU (general) or FP64 Cholesky (SPD) when refinement does not converge
+//     or the FP32 factor breaks down.
 // Admission by HBM footprint: every admitted request holds one block of a
 // device arena (its A, B, X, factor and pivots); a request is admitted only
 // when its block can be carved from the free space (first fit, coalescing on
@@ -204,6 +207,7 @@ struct Worker {
   // max_nrhs): a request of an order this worker has seen before replays the
   // solve's captured CUDA graphs instead of launching every kernel again
   double *Aw = nullptr, *Bw = nullptr, *Xw = nullptr;
+  int* Pw = nullptr;       // pivots of the FP64 LU at the bucket order
   double* cpad = nullptr;  // diagonal of the padding block (device)
 };
 
@@ -467,42 +471,52 @@ int worker_solve(lm_server* s, Worker* w, Req* r) {
   const size_t nn = (size_t)r->n * r->n * 8, nr = (size_t)r->n * r->nrhs * 8;
   LM_CUDA_TRY(cudaMemcpyAsync(dA, r->A, nn, cudaMemcpyHostToDevice, st));
   LM_CUDA_TRY(cudaMemcpyAsync(dB, r->B, nr, cudaMemcpyHostToDevice, st));
+  const bool general = r->kind == LM_BATCH_GENERAL;
+  // Both methods run at the bucket order in the worker's fixed buffers, so a
+  // request of an order this worker has served before replays captured graphs.
+  const int np = padded_order(r->n);
+  const long long tot = (long long)np * np;
+  pad_diag_kernel<<<1, 256, 0, st>>>(dA, r->n, w->cpad);
+  embed_kernel<<<(int)std::min<long long>((tot + 255) / 256, 4096), 256, 0, st>>>(w->Aw, np, dA, r->n, w->cpad);
+  lm::count_launch(2);
+  LM_CUDA_TRY(cudaGetLastError());
+  LM_CUDA_TRY(cudaMemcpyAsync(w->Bw, dB, nr, cudaMemcpyDeviceToDevice, st));
+  if (np > r->n)
+    LM_CUDA_TRY(cudaMemsetAsync(w->Bw + (size_t)r->n * r->nrhs, 0, sizeof(double) * (size_t)(np - r->n) * r->nrhs, st));
   int info = 0, rc = LM_OK;
-  bool fp64 = true;
-  if (s->cfg.large_precision == LM_PREC_FP32_IR) {
-    int it = 0;
-    double be = 0;
-    // solved at the bucket order in the worker's fixed buffers (graph replay)
-    const int np = padded_order(r->n);
-    const long long tot = (long long)np * np;
-    pad_diag_kernel<<<1, 256, 0, st>>>(dA, r->n, w->cpad);
-    embed_kernel<<<(int)std::min<long long>((tot + 255) / 256, 4096), 256, 0, st>>>(w->Aw, np, dA, r->n, w->cpad);
-    lm::count_launch(2);
-    LM_CUDA_TRY(cudaGetLastError());
-    LM_CUDA_TRY(cudaMemcpyAsync(w->Bw, dB, nr, cudaMemcpyDeviceToDevice, st));
-    if (np > r->n)
-      LM_CUDA_TRY(cudaMemsetAsync(w->Bw + (size_t)r->n * r->nrhs, 0, sizeof(double) * (size_t)(np - r->n) * r->nrhs, st));
-    // the stopping test of the original order: 1e-15 n
-    rc = lm_dgesv_ir(w->ctx, np, r->nrhs, w->Aw, np, w->Bw, r->nrhs, w->Xw, r->nrhs, 1e-15 * r->n, 30, &it, &be,
-                     &info);
-    lm_ctx_ir_last_method(w->ctx, &r->ir_method);
-    if (rc == LM_OK) {
-      LM_CUDA_TRY(cudaMemcpyAsync(dX, w->Xw, nr, cudaMemcpyDeviceToDevice, st));
-      fp64 = false;
-      r->iters = it;
-    } else if (rc == LM_ERR_NOT_CONVERGED || rc > 0) {
-      r->fallback = true;
-      r->iters = -1;
-    } else {
-      return rc;
-    }
-  }
-  if (fp64) {
-    LM_CUDA_TRY(cudaMemcpyAsync(dX, dB, nr, cudaMemcpyDeviceToDevice, st));
-    rc = r->kind == LM_BATCH_GENERAL ? lm_dgesv(w->ctx, r->n, r->nrhs, dA, r->n, dP, dX, r->nrhs, &info)
-                                      : lm_dposv(w->ctx, r->n, r->nrhs, dA, r->n, dX, r->nrhs, &info);
+  const bool ir = s->cfg.large_precision == LM_PREC_FP32_IR &&
+                  r->n > (general ? s->cfg.lu_fp64_max_n : s->cfg.chol_fp64_max_n);
+  if (!ir) {
+    // FP64 LU or Cholesky of the embedded system, solved in place in Bw: the
+    // padding block is decoupled, so the first n rows are A's solution
+    rc = general ? lm_dgesv(w->ctx, np, r->nrhs, w->Aw, np, w->Pw, w->Bw, r->nrhs, &info)
+                 : lm_dposv(w->ctx, np, r->nrhs, w->Aw, np, w->Bw, r->nrhs, &info);
     if (rc < 0) return rc;
+    r->iters = 0;
+    LM_CUDA_TRY(cudaMemcpyAsync(r->X, w->Bw, nr, cudaMemcpyDeviceToHost, st));
+    LM_CUDA_TRY(cudaStreamSynchronize(st));
+    return info;
   }
+  int it = 0;
+  double be = 0;
+  // the stopping test of the original order: 1e-15 n
+  rc = lm_dgesv_ir(w->ctx, np, r->nrhs, w->Aw, np, w->Bw, r->nrhs, w->Xw, r->nrhs, 1e-15 * r->n, 30, &it, &be, &info);
+  lm_ctx_ir_last_method(w->ctx, &r->ir_method);
+  if (rc == LM_OK) {
+    r->iters = it;
+    LM_CUDA_TRY(cudaMemcpyAsync(r->X, w->Xw, nr, cudaMemcpyDeviceToHost, st));
+    LM_CUDA_TRY(cudaStreamSynchronize(st));
+    return LM_OK;
+  }
+  if (rc != LM_ERR_NOT_CONVERGED && rc <= 0) return rc;
+  // refinement did not converge (or the FP32 factor broke down): FP64 at the
+  // request's own order from the untouched arena copy
+  r->fallback = true;
+  r->iters = -1;
+  LM_CUDA_TRY(cudaMemcpyAsync(dX, dB, nr, cudaMemcpyDeviceToDevice, st));
+  rc = general ? lm_dgesv(w->ctx, r->n, r->nrhs, dA, r->n, dP, dX, r->nrhs, &info)
+               : lm_dposv(w->ctx, r->n, r->nrhs, dA, r->n, dX, r->nrhs, &info);
+  if (rc < 0) return rc;
   LM_CUDA_TRY(cudaMemcpyAsync(r->X, dX, nr, cudaMemcpyDeviceToHost, st));
   LM_CUDA_TRY(cudaStreamSynchronize(st));
   return info;
@@ -751,6 +765,7 @@ void server_free(lm_server* s) {
     cudaFree(w->Aw);
     cudaFree(w->Bw);
     cudaFree(w->Xw);
+    cudaFree(w->Pw);
     cudaFree(w->cpad);
     delete w;
   }
@@ -809,13 +824,14 @@ int server_init(lm_server* s) {
     w->s = s;
     s->workers.push_back(w);
     LM_TRY(lm_ctx_create(&w->ctx, s->device));
-    lm::ctx_set_graph_cache(w->ctx, 256);
+    lm::ctx_set_graph_cache(w->ctx, 1024);
     LM_TRY(lm_ctx_set_ir_method(w->ctx, s->cfg.ir_method));
     const size_t np = (size_t)padded_order(s->cfg.max_n);
     const size_t nn = np * np, nr = np * s->cfg.max_nrhs;
     LM_CUDA_TRY(cudaMalloc(&w->Aw, sizeof(double) * nn));
     LM_CUDA_TRY(cudaMalloc(&w->Bw, sizeof(double) * nr));
     LM_CUDA_TRY(cudaMalloc(&w->Xw, sizeof(double) * nr));
+    LM_CUDA_TRY(cudaMalloc(&w->Pw, sizeof(int) * np));
     LM_CUDA_TRY(cudaMalloc(&w->cpad, 256));
     LM_TRY(prewarm(s, w));
   }
@@ -899,6 +915,8 @@ int lm_server_default_config(lm_server_config* c) {
   c->ir_method = LM_IR_GEPP;
   c->device_loop = 1;
   c->loop_ctas = 16;
+  c->lu_fp64_max_n = 2048;
+  c->chol_fp64_max_n = 4096;
   return LM_OK;
 }
 
@@ -916,7 +934,7 @@ int lm_server_create(lm_server** out, int device, const lm_server_config* cfg) {
       c.max_nrhs > 64 || (c.small_precision != LM_PREC_FP64 && c.small_precision != LM_PREC_FP32_IR) ||
       (c.large_precision != LM_PREC_FP64 && c.large_precision != LM_PREC_FP32_IR) ||
       (c.ir_method != LM_IR_RBT && c.ir_method != LM_IR_GEPP) || (c.device_loop && c.loop_ctas < 1) ||
-      (c.device_loop && c.small_precision != LM_PREC_FP64))
+      (c.device_loop && c.small_precision != LM_PREC_FP64) || c.lu_fp64_max_n < 0 || c.chol_fp64_max_n < 0)
     return LM_ERR_ARG;
   for (int b = 0; b < 4; ++b)
     if (c.nb[b] != 8 && c.nb[b] != 16 && c.nb[b] != 32) return LM_ERR_ARG;

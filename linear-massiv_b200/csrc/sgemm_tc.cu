@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(T_THREADS, 1)
       if (ok && use_beta && !mbar_wait(c_full, (uint32_t)(lt & 1), g.status)) ok = false;
       if (!use_beta && leader) bulk_wait_read0();
       named_bar(1, 128);  // C block present (or free) for all epilogue warps
+      __syncwarp();       // converged for the warp-wide tcgen05.ld (.sync.aligned)
       tc_fence_after();
       if (ok) {
 #pragma unroll 1

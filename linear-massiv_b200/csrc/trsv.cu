@@ -258,7 +258,10 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
     // xj is double-buffered: the next write to this buffer comes after the
     // next iteration's barrier, which every thread reaches after this FMA.
   }
-  // y = rhs - T_b,dep x_dep  (the four lanes of a row are adjacent)
+  // y = rhs - T_b,dep x_dep  (the four lanes of a row are adjacent).  The
+  // warp is reconverged first: thread 0's bounded poll and the barriers
+  // leave it split, and a split warp serialises every shuffle that follows.
+  __syncwarp();
 #pragma unroll
   for (int h = 0; h < MAX_RHS; ++h) {
     acc[h] += __shfl_xor_sync(0xffffffffu, acc[h], 1);
@@ -302,6 +305,9 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
           }
         }
       };
+      // one converged warp for the whole sweep: entered split (after the
+      // divergent ys stores and the barrier), each step's shuffles cost 5x
+      __syncwarp();
 #pragma unroll 1
       for (int st = 0; st < 32; ++st) {
         const int sl = forward ? st : 31 - st;  // lane whose rows are solved now
@@ -311,8 +317,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
 #pragma unroll
         for (int i = 0; i < RPL; ++i) rdv[i] = (forward && unit_l) ? T(1) : diag.rdiag[RPL * sl + i];
 #pragma unroll
-        for (int h = 0; h < MAX_RHS; ++h)
-          if (h < nrhs) {
+        for (int h = 0; h < MAX_RHS; ++h) {  // columns past nrhs hold zeros: no branch on nrhs
             T xv[RPL];
 #pragma unroll
             for (int j = 0; j < RPL; ++j) xv[j] = __shfl_sync(0xffffffffu, y[j][h], sl);
@@ -356,6 +361,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
     // and a product with the explicit inverse alone loses accuracy by their
     // condition number
     auto inv_times_ys = [&](T (&out)[MAX_RHS]) {
+      __syncwarp();
 #pragma unroll
       for (int h = 0; h < MAX_RHS; ++h) out[h] = T(0);
 #pragma unroll
@@ -410,6 +416,7 @@ __global__ void __launch_bounds__(TrsvCfg<T>::NT) trsv_kernel(const T* __restric
       for (int h = 0; h < MAX_RHS; ++h)
         if (h < nrhs) rr[h] = fma(tb[e], xb[cc][h], rr[h]);
     }
+    __syncwarp();
 #pragma unroll
     for (int h = 0; h < MAX_RHS; ++h) {
       rr[h] += __shfl_xor_sync(0xffffffffu, rr[h], 1);

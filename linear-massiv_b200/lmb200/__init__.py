@@ -681,7 +681,7 @@ class ServerConfig(ctypes.Structure):
                 ("small_max_n", ctypes.c_int), ("small_precision", ctypes.c_int), ("large_precision", ctypes.c_int),
                 ("max_batch", ctypes.c_int), ("max_n", ctypes.c_int), ("max_nrhs", ctypes.c_int),
                 ("nb", ctypes.c_int * 4), ("ir_method", ctypes.c_int), ("device_loop", ctypes.c_int),
-                ("loop_ctas", ctypes.c_int)]
+                ("loop_ctas", ctypes.c_int), ("lu_fp64_max_n", ctypes.c_int), ("chol_fp64_max_n", ctypes.c_int)]
 
 
 class ServerStats(ctypes.Structure):

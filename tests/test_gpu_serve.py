@@ -1,8 +1,9 @@
 """Serving loop (continuous batching, HBM-budget admission) on the GPU.
 
-Requests mix small instances (micro-batched into the persistent batch kernel)
-and larger ones (mixed-precision LU + FP64 refinement for general and SPD
-systems, FP64 LU or Cholesky as the fallback).  Checked: every result reaches the normwise backward error
+Requests mix small instances (the device-resident loop or micro-batches of the
+persistent batch kernel) and larger ones (FP64 LU or Cholesky at the bucket
+order, or the mixed-precision LU + FP64 refinement for general and SPD systems
+with FP64 LU or Cholesky as the fallback).  Checked: every result reaches the normwise backward error
 1e-15 n; each result is the same alone and in the mix (bitwise: the
 per-request computation does not depend on what else runs); admission never
 exceeds the arena; small requests overtake a large one in flight; host-side
@@ -59,9 +60,13 @@ def make_requests(g, count, nmax):
     return reqs
 
 
-@pytest.fixture(scope="module")
-def server():
-    s = lmb200.Server(0, max_n=1024, max_nrhs=64, large_workers=3, batch_lanes=2, hbm_budget=512 << 20)
+@pytest.fixture(scope="module", params=["fp64", "ir"])
+def server(request):
+    """Larger requests by FP64 LU / Cholesky at the bucket order (the default up
+    to order 2048 / 4096), or all of them by the mixed-precision solve."""
+    limits = {} if request.param == "fp64" else {"lu_fp64_max_n": 0, "chol_fp64_max_n": 0}
+    s = lmb200.Server(0, max_n=1024, max_nrhs=64, large_workers=3, batch_lanes=2, hbm_budget=512 << 20, **limits)
+    s.route = request.param
     yield s
     s.close()
 
@@ -83,6 +88,7 @@ def test_mix_matches_alone_and_fp64_accuracy(server):
         assert np.array_equal(X, Xm), "result differs alone vs in the mix"
     st = server.stats()
     assert st["completed"] >= 96 and st["failed"] == 0
+    assert (st["ir_solves"] > 0) == (server.route == "ir")
     assert st["arena_peak_bytes"] <= st["arena_bytes"]
     assert st["micro_batches"] >= 1 and st["small_solved"] >= 1
 
