@@ -23,8 +23,9 @@
 //   NaN rule of the reference scan: if |a_jj| is NaN it stays the pivot; NaNs
 //   below it never win.
 //
-// potrf_block — Cholesky of one <=128 x 128 diagonal block in registers
-//   (rawCholColumnSIMDFrom, K.hs:2137-2195, for a diagonal panel).
+// potrf_block — Cholesky of one <=128 x 128 diagonal block in shared memory,
+//   by 32-column panels (rawCholColumnSIMDFrom, K.hs:2137-2195, for a
+//   diagonal panel).
 #include <climits>
 
 #include "common.cuh"
@@ -38,6 +39,7 @@ namespace {
 
 constexpr int kLeafThreads = 512;
 constexpr int kLeafRowsTimesW = 16384;  // rows per CTA * leaf width (128 KB of FP64)
+static_assert(kLeafThreads / 32 >= 16, "one pushing warp per CTA of the largest (16-CTA) cluster");
 
 template <typename T>
 __device__ __forceinline__ T absval(T x) {
@@ -148,15 +150,16 @@ __device__ __forceinline__ void pack16(const T* src, uint32_t (&w)[4]) {
 }
 
 // Push a message staged in this CTA's shared memory (`msg`) to the same
-// offset `slot` in every CTA of the cluster, completing on their `bar`.
+// offset `slot` in CTA d of the cluster, completing on its `bar`; one lane
+// per 16-byte chunk.
 template <typename T, int W>
-__device__ __forceinline__ void push_all(const T* msg, T* slot, uint64_t* bar, int C, int lane) {
+__device__ __forceinline__ void push_one(const T* msg, T* slot, uint64_t* bar, int d, int lane) {
   using M = LeafMsg<T, W>;
-  for (int it = lane; it < C * M::CHUNKS; it += 32) {
-    const int d = it / M::CHUNKS, ch = it % M::CHUNKS;
+  static_assert(M::CHUNKS <= 32, "one chunk per lane");
+  if (lane < M::CHUNKS) {
     uint32_t w4[4];
-    pack16<T>(msg + ch * M::PER_CHUNK, w4);
-    st_async_16(dsmem_map(slot, d) + ch * 16, dsmem_map(bar, d), w4[0], w4[1], w4[2], w4[3]);
+    pack16<T>(msg + lane * M::PER_CHUNK, w4);
+    st_async_16(dsmem_map(slot, d) + lane * 16, dsmem_map(bar, d), w4[0], w4[1], w4[2], w4[3]);
   }
 }
 
@@ -271,10 +274,13 @@ __global__ void __launch_bounds__(kLeafThreads, 1)
           outc[2] = T(0);
           outc[3] = T(0);
         }
-        __syncwarp();
-        push_all<T, W>(outc, cand + ((size_t)par * 16 + q) * M::N, &rbar[par], C, lane);
       }
     }
+    // the staged candidate goes out from C warps at once: warp d sends it to
+    // CTA d, one 16-byte chunk per lane (one warp sending all C copies took
+    // about 900 cycles per column)
+    __syncthreads();
+    if (warp < C) push_one<T, W>(outc, cand + ((size_t)par * 16 + q) * M::N, &rbar[par], warp, lane);
     // ---- wait for the C candidates ----
     if (!timed_out && !mbar_wait_spin(&rbar[par], (uint32_t)((j >> 1) & 1), status)) timed_out = true;
 
@@ -504,88 +510,154 @@ template int panel_leaf<double>(Ctx&, double*, long long, int, int, int, int, in
 template int panel_leaf<float>(Ctx&, float*, long long, int, int, int, int, int, int*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
-// Cholesky of one diagonal block (w <= 128), right-looking in registers.
+// Cholesky of one diagonal block (w <= 128), by 32-column panels in shared memory.
 // ---------------------------------------------------------------------------
 namespace {
 
-// Cholesky of the w x w block at A (w <= 128, lower triangle) in place.
-// Thread (ty, tx) of a 16 x 32 grid holds elements (ty + 16 a, tx + 32 b),
-// a < 8, b < 4, in registers.  Step k: the owner of a_kk publishes
-// 1 / sqrt(a_kk); the owners of column k form l_ik = a_ik / sqrt(a_kk) as
-// products with it and publish them; every thread subtracts l_ik l_jk from its lower elements
-// (i, j > k).  Two barriers per column, nothing re-read from memory.  A
-// non-positive (or NaN) pivot is recorded as base + k + 1 in status[1]; the
-// square root still runs, leaving the NaN the reference's arithmetic would.
+// Cholesky of the w x w block at A (w <= 128, lower triangle) in place, in
+// shared memory, right-looking by 32-column panels (padded to whole panels
+// with the identity).  Per panel c0:
+//   1. warp 0 factors the 32 x 32 diagonal block in registers: lane i holds
+//      row i; step k broadcasts a_kk, forms r = 1 / sqrt(a_kk), l_ik = a_ik r
+//      (l_kk = a_kk r) and subtracts l_ik l_jk from the lanes' later columns
+//      with one shuffle per column (steps unrolled at compile time so the row
+//      stays in registers: 256 threads leave room for it); r is kept for the
+//      panel solve;
+//   2. one thread per row below solves x = a L11^-T by the same products
+//      (x_k = (a_k - sum_{j<k} x_j l_kj) r_k);
+//   3. all threads subtract X X^T from the lower trailing block in 4 x 4
+//      register tiles.
+// A non-positive (or NaN) pivot is recorded as base + k + 1 in status[1]
+// (the first one: panels and steps run in order); the arithmetic continues,
+// leaving the NaN the reference's would.
+constexpr int kPbLd = 129;  // padded row stride of the shared copy (elements)
+constexpr int kPbXt = 96;   // row stride of the transposed panel X^T (elements)
+constexpr int kPbThreads = 256;
+
 template <typename T>
-__global__ void __launch_bounds__(512) potrf_block_kernel(T* A, long long lda, int w, int base, int* status) {
-  __shared__ T rk[2];
-  __shared__ T lcol[2][128];
-  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
-  T v[8][4];
+constexpr int potrf_block_smem() {
+  return (128 * kPbLd + 32 * kPbXt) * (int)sizeof(T);
+}
+
+// Step K of the one-warp 32 x 32 Cholesky (lane i holds row i in d), with
+// K a compile-time constant so that d stays in registers.
+template <typename T, int K>
+__device__ __forceinline__ void pb_diag_step(T (&d)[32], int lane, int& bad, T& myr) {
+  if constexpr (K < 32) {
+    const T dkk = __shfl_sync(0xffffffffu, d[K], K);
+    bad = (bad < 0 && !(dkk > T(0))) ? K : bad;  // the same in every lane
+    const T r = rsqrt(dkk);
+    const T lk = d[K] * r;
+    d[K] = lane >= K ? lk : d[K];
+    myr = lane == K ? r : myr;
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = ty + 16 * a, j = tx + 32 * b;
-      v[a][b] = (i < w && j <= i) ? A[(long long)i * lda + j] : (i == j ? T(1) : T(0));
+    for (int j = K + 1; j < 32; ++j) {
+      const T lj = __shfl_sync(0xffffffffu, lk, j);
+      d[j] = lane >= j ? fma(-lk, lj, d[j]) : d[j];
     }
+    pb_diag_step<T, K + 1>(d, lane, bad, myr);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) potrf_block_kernel(T* A, long long lda, int w, int base, int* status) {
+  extern __shared__ __align__(16) unsigned char pb_smem[];
+  T* S = reinterpret_cast<T*>(pb_smem);  // 128 x kPbLd, lower triangle
+  T* Xt = S + 128 * kPbLd;               // 32 x kPbXt: the solved panel, transposed
+  __shared__ T rdiag[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int np = (w + 31) >> 5;  // panels
+  const int wp = np << 5;        // padded order
+  for (int e = tid; e < wp * wp; e += kPbThreads) {
+    const int i = e / wp, j = e % wp;
+    T v = T(0);
+    if (j <= i) v = (i < w) ? A[(long long)i * lda + j] : (i == j ? T(1) : T(0));
+    S[i * kPbLd + j] = v;
+  }
+  __syncthreads();
 #pragma unroll 1
-  for (int k = 0; k < w; ++k) {
-    const int buf = k & 1;
-    const int ak = k >> 4, bk = k >> 5;
-    if (ty == (k & 15) && tx == (k & 31)) {
+  for (int p = 0; p < np; ++p) {
+    const int c0 = p << 5;
+    // ---- 1. diagonal block, one warp (selects, not branches: the warp
+    //         stays converged for its shuffles) ----
+    if (warp == 0) {
+      T d[32];
+      T* row = S + (c0 + lane) * kPbLd + c0;
 #pragma unroll
-      for (int a = 0; a < 8; ++a)
-        if (a == ak)
+      for (int j = 0; j < 32; ++j) d[j] = row[j];
+      int bad = -1;
+      T myr = T(0);
+      pb_diag_step<T, 0>(d, lane, bad, myr);
+      rdiag[lane] = myr;
 #pragma unroll
-          for (int b = 0; b < 4; ++b)
-            if (b == bk) {
-              const T d = v[a][b];
-              if (!(d > T(0))) atomicCAS(status + 1, 0, base + k + 1);
-              // 1 / sqrt(d) once, then sqrt(d) = d / sqrt(d) and every
-              // multiplier a product with it (within an ulp of the quotients)
-              const T r = rsqrt(d);
-              v[a][b] = d * r;
-              rk[buf] = r;
-            }
+      for (int j = 0; j < 32; ++j)
+        if (j <= lane) row[j] = d[j];
+      if (lane == 0 && bad >= 0 && c0 + bad < w) atomicCAS(status + 1, 0, base + c0 + bad + 1);
     }
     __syncthreads();
-    if (tx == (k & 31)) {
-      const T r = rk[buf];
+    const int m = wp - c0 - 32;  // rows below the diagonal block
+    if (m <= 0) break;
+    // ---- 2. panel solve, one thread per row: x = a L11^-T ----
+    if (tid < m) {
+      T* row = S + (c0 + 32 + tid) * kPbLd + c0;
+      const T* L = S + c0 * kPbLd + c0;
+      T a[32];
 #pragma unroll
-      for (int b = 0; b < 4; ++b)
-        if (b == bk)
+      for (int j = 0; j < 32; ++j) a[j] = row[j];
 #pragma unroll
-          for (int a = 0; a < 8; ++a) {
-            const int i = ty + 16 * a;
-            if (i > k) {
-              const T l = v[a][b] * r;
-              v[a][b] = l;
-              lcol[buf][i] = l;
-            }
-          }
-    }
-    __syncthreads();
+      for (int k = 0; k < 32; ++k) {
+        const T x = a[k] * rdiag[k];
+        a[k] = x;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
-      const int i = ty + 16 * a;
-      if (i > k) {
-        const T li = lcol[buf][i];
+        for (int j = k + 1; j < 32; ++j) a[j] = fma(-x, L[j * kPbLd + k], a[j]);
+      }
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
-          const int j = tx + 32 * b;
-          if (j > k && j <= i) v[a][b] = fma(-li, lcol[buf][j], v[a][b]);
-        }
+      for (int j = 0; j < 32; ++j) {
+        row[j] = a[j];
+        Xt[j * kPbXt + tid] = a[j];
       }
     }
-  }
+    __syncthreads();
+    // ---- 3. trailing update, 4 x 4 register tiles of the lower triangle ----
+    const int tt = m >> 2;                 // tiles per side
+    const int ntiles = tt * (tt + 1) / 2;  // tile (ti, tj), tj <= ti, at t = ti (ti + 1) / 2 + tj
+    for (int t = tid; t < ntiles; t += kPbThreads) {
+      int ti = (int)((sqrtf(8.0f * (float)t + 1.0f) - 1.0f) * 0.5f);
+      while (ti > 0 && ti * (ti + 1) / 2 > t) --ti;
+      while ((ti + 1) * (ti + 2) / 2 <= t) ++ti;
+      const int tj = t - ti * (ti + 1) / 2;
+      const int ri = 4 * ti, rj = 4 * tj;  // rows within the trailing block
+      const int i0 = c0 + 32 + ri, j0 = c0 + 32 + rj;
+      T acc[4][4];
 #pragma unroll
-  for (int a = 0; a < 8; ++a)
+      for (int u = 0; u < 4; ++u)
 #pragma unroll
-    for (int b = 0; b < 4; ++b) {
-      const int i = ty + 16 * a, j = tx + 32 * b;
-      if (i < w && j <= i) A[(long long)i * lda + j] = v[a][b];
+        for (int v = 0; v < 4; ++v) acc[u][v] = S[(i0 + u) * kPbLd + j0 + v];
+#pragma unroll 8
+      for (int k = 0; k < 32; ++k) {
+        T xi[4], xj[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          xi[u] = Xt[k * kPbXt + ri + u];
+          xj[u] = Xt[k * kPbXt + rj + u];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = fma(-xi[u], xj[v], acc[u][v]);
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+          if (j0 + v <= i0 + u) S[(i0 + u) * kPbLd + j0 + v] = acc[u][v];
     }
+    __syncthreads();
+  }
+  for (int e = tid; e < w * w; e += kPbThreads) {
+    const int i = e / w, j = e % w;
+    if (j <= i) A[(long long)i * lda + j] = S[i * kPbLd + j];
+  }
 }
 
 }  // namespace
@@ -594,7 +666,14 @@ template <typename T>
 int potrf_block(Ctx& c, T* A, long long lda, int w, int base, cudaStream_t st) {
   if (w <= 0) return LM_OK;
   if (w > 128) return LM_ERR_ARG;
-  potrf_block_kernel<T><<<1, 512, 0, st>>>(A, lda, w, base, ctx_status(c));
+  constexpr int smem = potrf_block_smem<T>();
+  static bool attr_set[kMaxDevices] = {};
+  const int dev = ctx_device(c);
+  if (!attr_set[dev]) {
+    LM_CUDA_TRY(cudaFuncSetAttribute(potrf_block_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr_set[dev] = true;
+  }
+  potrf_block_kernel<T><<<1, kPbThreads, smem, st>>>(A, lda, w, base, ctx_status(c));
   count_launch(1);
   LM_CUDA_TRY(cudaGetLastError());
   return LM_OK;
