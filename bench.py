@@ -69,6 +69,8 @@ def parse():
                    help="serve: pregenerated systems (each of its own order, log-uniform)")
     p.add_argument("--max-n", type=int, default=4096, help="serve: largest order")
     p.add_argument("--workers", type=int, default=8, help="serve: concurrent large solves")
+    p.add_argument("--lu-fp64-max-n", type=int, default=-1,
+                   help="serve: largest general order solved by FP64 LU (default: the server's)")
     p.add_argument("--count", type=int, default=10000, help="batch: number of instances")
     p.add_argument("--precision", choices=["fp64", "ir"], default="fp64", help="batch: FP64 or FP32 + FP64 IR")
     p.add_argument("--tune", action="store_true", help="batch: autotune the panel widths before timing")
@@ -99,7 +101,9 @@ def workload_name(a):
         return (f"serving loop, Poisson arrivals at {a.rate:g} req/s for {a.duration:g} s, n log-uniform in "
                 f"[16,{a.max_n}], nrhs in {{1,8,32}}, 70% general / 30% SPD, kappa log-uniform in [1e1,1e6] "
                 f"(sigma-spectrum, 8 reflectors per side; {a.pool} pregenerated systems of continuous order), "
-                f"mixed-precision IR with FP64 fallback at padded bucket orders, HBM-budget admission")
+                f"large requests at padded bucket orders: FP64 LU up to n="
+                f"{a.lu_fp64_max_n if a.lu_fp64_max_n >= 0 else 2048} and FP64 Cholesky (SPD), mixed-precision IR "
+                f"with FP64 fallback above; small ones on the device-resident loop; HBM-budget admission")
     if a.workload == "batch":
         return (f"batched solves, {a.count} instances in one persistent launch, n uniform in [8,256], nrhs uniform "
                 f"in [1,16], half SPD (B B^T + n I, Cholesky) half general (uniform[-1,1], LU), "
@@ -305,8 +309,9 @@ def run_serve(a, world, rank, local):
     g = np.random.Generator(np.random.Philox(a.seed + 99 + 7919 * rank))
     rhs = {r: torch.from_numpy(g.uniform(-1.0, 1.0, (a.max_n, r))).pin_memory() for r in (1, 8, 32)}
     free_b, _ = torch.cuda.mem_get_info()
+    route = {} if a.lu_fp64_max_n < 0 else {"lu_fp64_max_n": a.lu_fp64_max_n}
     srv = lmb200.Server(local, max_n=a.max_n, max_nrhs=32, large_workers=a.workers, batch_lanes=2,
-                        hbm_budget=int(min(free_b // 3, 48 << 30)))
+                        hbm_budget=int(min(free_b // 3, 48 << 30)), **route)
     # arrival schedule and request draws (seeded, fixed before the run)
     total = int(a.rate * a.duration)
     gaps = g.exponential(1.0 / a.rate, total)

@@ -229,6 +229,48 @@ __global__ void __launch_bounds__(128) perm_gather_kernel(const T* __restrict__ 
   }
 }
 
+// sigma of the swap list ipiv[0..n) (as perm_gather_kernel walks it), once
+// per factorisation: perm[i] = sigma(i); an out-of-range pivot row records
+// LM_DEVERR_BOUNDS and maps i to itself.
+__global__ void __launch_bounds__(128) perm_from_swaps_kernel(const int* __restrict__ ipiv, int n, int* perm,
+                                                              int* status) {
+  constexpr int CH = 4096;
+  __shared__ int sp[CH];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int r = i;
+  for (int c0 = ((n - 1) / CH) * CH; c0 >= 0; c0 -= CH) {
+    const int cnt = min(CH, n - c0);
+    __syncthreads();
+    for (int e = threadIdx.x; e < cnt; e += blockDim.x) sp[e] = __ldg(ipiv + c0 + e);
+    __syncthreads();
+#pragma unroll 8
+    for (int k = cnt - 1; k >= 0; --k) {
+      const int p = sp[k];
+      const int kk = c0 + k;
+      r = (r == kk) ? p : ((r == p) ? kk : r);
+    }
+  }
+  if (i < n) {
+    if (r < 0 || r >= n) {
+      atomicCAS(status, 0, LM_DEVERR_BOUNDS);
+      r = i;
+    }
+    perm[i] = r;
+  }
+}
+
+// W(i, :) = B(perm[i], :) for a narrow block (n x nrhs).
+template <typename T>
+__global__ void gather_rows_kernel(const T* __restrict__ B, long long ldb, int n, int nrhs,
+                                   const int* __restrict__ perm, T* W, long long ldw) {
+  const long long total = (long long)n * nrhs;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < total;
+       e += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(e / nrhs), c = (int)(e % nrhs);
+    W[(long long)i * ldw + c] = B[(long long)__ldg(perm + i) * ldb + c];
+  }
+}
+
 // op(Tri) X = B for one w x 32 column block of B per CTA (w <= 128).  The
 // triangle of op(Tri) is staged packed in shared memory (w(w+1)/2 entries,
 // so two CTAs fit per SM in FP64) together with the block.  Rows are solved
@@ -409,6 +451,25 @@ int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int c
   return LM_OK;
 }
 
+int perm_from_swaps(const int* ipiv, int n, int* perm, int* status, cudaStream_t st) {
+  if (n <= 0) return LM_OK;
+  perm_from_swaps_kernel<<<cdiv(n, 128), 128, 0, st>>>(ipiv, n, perm, status);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return LM_OK;
+}
+
+template <typename T>
+int laswp_perm(T* B, long long ldb, int n, int nrhs, const int* perm, T* W, cudaStream_t st) {
+  if (n <= 0 || nrhs <= 0) return LM_OK;
+  const long long total = (long long)n * nrhs;
+  gather_rows_kernel<T><<<(int)std::min<long long>((total + 255) / 256, 4096), 256, 0, st>>>(B, ldb, n, nrhs, perm,
+                                                                                            W, nrhs);
+  count_launch(1);
+  LM_CUDA_TRY(cudaGetLastError());
+  return copy2d<T>(B, ldb, W, nrhs, n, nrhs, st);
+}
+
 template <typename T>
 int laswp_narrow(T* B, long long ldb, int n, int nrhs, const int* ipiv, T* W, int* status, cudaStream_t st) {
   if (n <= 0 || nrhs <= 0) return LM_OK;
@@ -505,6 +566,8 @@ template int laswp<double>(double*, long long, int, const int*, int, int, int, i
 template int laswp<float>(float*, long long, int, const int*, int, int, int, int, int, int, int*, cudaStream_t, int*);
 template int laswp_narrow<double>(double*, long long, int, int, const int*, double*, int*, cudaStream_t);
 template int laswp_narrow<float>(float*, long long, int, int, const int*, float*, int*, cudaStream_t);
+template int laswp_perm<double>(double*, long long, int, int, const int*, double*, cudaStream_t);
+template int laswp_perm<float>(float*, long long, int, int, const int*, float*, cudaStream_t);
 template int trsm_left<double>(const double*, long long, int, bool, bool, bool, double*, long long, int,
                                cudaStream_t);
 template int trsm_left<float>(const float*, long long, int, bool, bool, bool, float*, long long, int,

@@ -110,6 +110,12 @@ int laswp(T* A, long long lda, int nrows, const int* ipiv, int k0, int k1, int c
 // parallel gather into W, n x nrhs scratch, then copied back).
 template <typename T>
 int laswp_narrow(T* B, long long ldb, int n, int nrhs, const int* ipiv, T* W, int* status, cudaStream_t st);
+// The composed row permutation of a swap list, once per factorisation
+// (perm[i] = sigma(i), the row laswp_narrow would bring to row i), and the
+// gather that applies it to a narrow block (W: n x nrhs scratch).
+int perm_from_swaps(const int* ipiv, int n, int* perm, int* status, cudaStream_t st);
+template <typename T>
+int laswp_perm(T* B, long long ldb, int n, int nrhs, const int* perm, T* W, cudaStream_t st);
 
 // In-place triangular solve with a w x w block (w <= 128) of Tri (ldt) on the
 // w x ncols block B (ldb):  op(Tri) X = B.

@@ -724,7 +724,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   const long long lda32 = (n + 31) / 32 * 32;
   const long long ldr = (nrhs + 7) / 8 * 8;
   const size_t a32_bytes = sizeof(float) * (size_t)n * lda32;
-  const size_t piv_bytes = sizeof(int) * (size_t)((n + 63) / 64 * 64);
+  const size_t piv_bytes = 2 * sizeof(int) * (size_t)((n + 63) / 64 * 64);  // ipiv, then its composed permutation
   const size_t r_bytes = sizeof(double) * (size_t)n * ldr;
   const size_t d_bytes = sizeof(float) * (size_t)n * ldr;
   const size_t nrm_bytes = sizeof(unsigned long long) * (size_t)(2 + 3 * 64);  // 16-byte multiple
@@ -744,6 +744,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   char* p = static_cast<char*>(ws);
   float* A32 = reinterpret_cast<float*>(p);
   int* ipiv = reinterpret_cast<int*>(p + a32_bytes);
+  int* perm = ipiv + (n + 63) / 64 * 64;
   double* R = reinterpret_cast<double*>(p + a32_bytes + piv_bytes);
   float* D = reinterpret_cast<float*>(p + a32_bytes + piv_bytes + r_bytes);
   unsigned long long* nrm = reinterpret_cast<unsigned long long*>(p + a32_bytes + piv_bytes + r_bytes + d_bytes);
@@ -768,10 +769,12 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
   // factor fl32(A)
   LM_TRY(run(gmres ? (prec == LM_IR_PREC_BF16 ? "factor_bf16" : "factor_tf32") : "factor", [&](cudaStream_t s) {
     LM_TRY(convert_d2s(A32, lda32, A, lda, n, n, s));
-    return sgetrf(c, n, A32, lda32, ipiv, s, prec);
+    LM_TRY(sgetrf(c, n, A32, lda32, ipiv, s, prec));
+    // the interchanges composed once; every correction then gathers with them
+    return perm_from_swaps(ipiv, n, perm, ctx_status(c), s);
   }));
   auto precond = [&](float* Dd, cudaStream_t s) {
-    LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
+    LM_TRY(laswp_perm<float>(Dd, ldr, n, nrhs, perm, Wg, s));
     return trsv_lu<float>(A32, lda32, n, nrhs, nullptr, nullptr, Dd, ldr, tsync, ctx_status(c), s, nullptr, true);
   };
   if (gmres)  // the host steers the Krylov steps: these run without graph capture
@@ -781,7 +784,7 @@ int dgesv_ir(Ctx& c, int n, int nrhs, const double* A, long long lda, const doub
                 [&](float* Dd, cudaStream_t s) {
                   {
                     Prof pp(c, kPhaseSwap, 0.0, 16.0 * n * nrhs, s);
-                    LM_TRY(laswp_narrow<float>(Dd, ldr, n, nrhs, ipiv, Wg, ctx_status(c), s));
+                    LM_TRY(laswp_perm<float>(Dd, ldr, n, nrhs, perm, Wg, s));
                   }
                   // diagonal blocks by substitution: with partial pivoting U's
                   // blocks carry the small pivots of an ill-conditioned A, and a

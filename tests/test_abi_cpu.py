@@ -85,3 +85,14 @@ def test_host_mirror_header_compiles():
                           "-I" + os.path.join(ROOT, "linear-massiv_b200", "host"), src],
                          capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
+
+
+def test_server_default_config_layout(lib):
+    """The ctypes mirror of lm_server_config reads the defaults the library
+    writes (a field out of order or missing would show up as garbage here)."""
+    c = lmb200.ServerConfig()
+    assert lib.lm_server_default_config(ctypes.byref(c)) == 0
+    assert (c.hbm_budget, c.large_workers, c.batch_lanes, c.small_max_n) == (0, 8, 2, 256)
+    assert (c.max_batch, c.max_n, c.max_nrhs, list(c.nb)) == (4096, 4096, 64, [16, 16, 16, 16])
+    assert (c.ir_method, c.device_loop, c.loop_ctas) == (lmb200.IR_GEPP, 1, 16)
+    assert (c.lu_fp64_max_n, c.chol_fp64_max_n) == (2048, 4096)
