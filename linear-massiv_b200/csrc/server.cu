@@ -250,7 +250,10 @@ struct lm_server {
   lm_server_config cfg{};
   std::mutex mu;
   std::condition_variable cv_done;
-  std::deque<Req*> pending;
+  // queued requests, one FIFO per class: dispatch takes from the fronts, so
+  // its cost does not grow with the length of the queue
+  std::deque<Req*> pend_small, pend_large;
+  size_t pending_count() const { return pend_small.size() + pend_large.size(); }
   std::unordered_map<long long, Req*> live;
   Arena arena;
   std::vector<Lane*> lanes;
@@ -307,14 +310,10 @@ void pump(lm_server* s) {
   if (s->loop) {
     DeviceLoop* L = s->loop;
     bool any = false;
-    for (auto it = s->pending.begin(); it != s->pending.end();) {
-      Req* r = *it;
-      if (!r->small) {
-        ++it;
-        continue;
-      }
+    while (!s->pend_small.empty()) {
+      Req* r = s->pend_small.front();
       if (L->in_ring + (int)L->to_post.size() >= L->cap || !admit(s, r)) break;
-      it = s->pending.erase(it);
+      s->pend_small.pop_front();
       L->to_post.push_back(r);
       any = true;
     }
@@ -324,16 +323,11 @@ void pump(lm_server* s) {
   for (Lane* ln : s->lanes) {
     if (ln->busy) continue;
     std::vector<Req*> take;
-    for (auto it = s->pending.begin(); it != s->pending.end() && (int)take.size() < s->cfg.max_batch;) {
-      Req* r = *it;
-      if (r->small && admit(s, r)) {
-        take.push_back(r);
-        it = s->pending.erase(it);
-      } else if (r->small) {
-        break;  // arena full: the rest waits for releases
-      } else {
-        ++it;
-      }
+    while (!s->pend_small.empty() && (int)take.size() < s->cfg.max_batch) {
+      Req* r = s->pend_small.front();
+      if (!admit(s, r)) break;  // arena full: the rest waits for releases
+      s->pend_small.pop_front();
+      take.push_back(r);
     }
     if (take.empty()) break;
     ln->jobs = std::move(take);
@@ -341,20 +335,16 @@ void pump(lm_server* s) {
     ln->cv.notify_one();
   }
   // large requests: arrival order among themselves
-  for (auto it = s->pending.begin(); it != s->pending.end();) {
-    Req* r = *it;
-    if (r->small) {
-      ++it;
-      continue;
-    }
+  while (!s->pend_large.empty()) {
     Worker* w = nullptr;
     for (Worker* x : s->workers)
       if (!x->busy) {
         w = x;
         break;
       }
+    Req* r = s->pend_large.front();
     if (!w || !admit(s, r)) break;
-    it = s->pending.erase(it);
+    s->pend_large.pop_front();
     w->job = r;
     w->busy = true;
     w->cv.notify_one();
@@ -703,13 +693,15 @@ void server_stop(lm_server* s) {
   {
     std::unique_lock<std::mutex> lk(s->mu);
     // queued requests that never started are cancelled; admitted ones finish
-    for (Req* r : s->pending) {
-      r->cancelled = true;
-      r->done = true;
-      r->status = LM_ERR_ARG;
-      ++s->cancelled;
+    for (std::deque<Req*>* q : {&s->pend_small, &s->pend_large}) {
+      for (Req* r : *q) {
+        r->cancelled = true;
+        r->done = true;
+        r->status = LM_ERR_ARG;
+        ++s->cancelled;
+      }
+      q->clear();
     }
-    s->pending.clear();
     s->cv_done.wait(lk, [&] { return s->inflight == 0; });
     s->stopping = true;
     for (Lane* ln : s->lanes) ln->cv.notify_all();
@@ -986,8 +978,8 @@ int lm_server_submit(lm_server* s, int n, int nrhs, int kind, const double* A, c
   r->t_submit = now_s();
   if (s->t_first == 0) s->t_first = r->t_submit;
   s->live[r->id] = r;
-  s->pending.push_back(r);
-  s->queue_peak = std::max(s->queue_peak, s->pending.size());
+  (r->small ? s->pend_small : s->pend_large).push_back(r);
+  s->queue_peak = std::max(s->queue_peak, s->pending_count());
   pump(s);
   *id = r->id;
   return LM_OK;
@@ -1034,9 +1026,10 @@ int lm_server_cancel(lm_server* s, long long id) {
   auto it = s->live.find(id);
   if (it == s->live.end()) return LM_ERR_ARG;
   Req* r = it->second;
-  auto q = std::find(s->pending.begin(), s->pending.end(), r);
-  if (q == s->pending.end()) return LM_ERR_UNSUPPORTED;  // already admitted (or done)
-  s->pending.erase(q);
+  std::deque<Req*>& pq = r->small ? s->pend_small : s->pend_large;
+  auto q = std::find(pq.begin(), pq.end(), r);
+  if (q == pq.end()) return LM_ERR_UNSUPPORTED;  // already admitted (or done)
+  pq.erase(q);
   r->cancelled = true;
   r->done = true;
   r->status = LM_ERR_ARG;
@@ -1048,7 +1041,7 @@ int lm_server_cancel(lm_server* s, long long id) {
 int lm_server_drain(lm_server* s, double timeout_s) {
   if (!s) return LM_ERR_ARG;
   std::unique_lock<std::mutex> lk(s->mu);
-  const auto pred = [&] { return s->pending.empty() && s->inflight == 0; };
+  const auto pred = [&] { return s->pending_count() == 0 && s->inflight == 0; };
   if (timeout_s > 0) {
     if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) return LM_ERR_TIMEOUT;
   } else {
@@ -1074,7 +1067,7 @@ int lm_server_stats(lm_server* s, lm_server_stats_t* o) {
   o->arena_bytes = s->arena.size;
   o->arena_peak_bytes = s->arena.peak;
   o->fixed_bytes = s->fixed_bytes;
-  o->pending = (long long)s->pending.size();
+  o->pending = (long long)s->pending_count();
   o->inflight = s->inflight;
   std::vector<double> v = s->lat_ms;
   if (!v.empty()) {
