@@ -230,8 +230,10 @@ __global__ void __launch_bounds__(128) perm_gather_kernel(const T* __restrict__ 
 }
 
 // sigma of the swap list ipiv[0..n) (as perm_gather_kernel walks it), once
-// per factorisation: perm[i] = sigma(i); an out-of-range pivot row records
-// LM_DEVERR_BOUNDS and maps i to itself.
+// per factorisation: perm[i] = sigma(i), so that every later application of
+// the interchanges to a right-hand side (applyPivotsForward, LU.hs:493-507)
+// is a plain gather; an out-of-range pivot row records LM_DEVERR_BOUNDS and
+// maps i to itself.
 __global__ void __launch_bounds__(128) perm_from_swaps_kernel(const int* __restrict__ ipiv, int n, int* perm,
                                                               int* status) {
   constexpr int CH = 4096;
